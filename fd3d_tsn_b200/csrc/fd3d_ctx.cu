@@ -1,0 +1,787 @@
+// fd3d_ctx.cu -- C ABI of the single-model B200 path (include/fd3d_gpu.h).
+//
+// Owns the device state of one forward model, enqueues the eleven launches of a
+// time step on the context's stream, captures chunks of steps in a CUDA graph,
+// and drains the device history ring into the reference's result files.
+#include <cuda_runtime.h>
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+#include "../../include/fd3d_gpu.h"
+#include "fd3d_common.cuh"
+#include "fd3d_kernels.cuh"
+#include "fd3d_opt.cuh"
+#include "fd3d_host.h"
+
+using namespace fd3d;
+
+#define CK(x)                                                                                  \
+    do {                                                                                       \
+        cudaError_t e_ = (x);                                                                  \
+        if (e_ != cudaSuccess) {                                                               \
+            std::fprintf(stderr, "fd3d: %s failed: %s (%s:%d)\n", #x, cudaGetErrorString(e_),  \
+                         __FILE__, __LINE__);                                                  \
+            return FD3D_ERR_CUDA;                                                              \
+        }                                                                                      \
+    } while (0)
+
+namespace fd3d {
+
+int validate_params(const fd3d_params* p) {
+    if (!p) return FD3D_ERR_ARG;
+    if (p->nabc < 3 || p->nfs != 2) return FD3D_ERR_ARG;
+    if (p->nxt < 2 * p->nabc + 4 || p->nyt < p->nabc + 4 || p->nzt < p->nabc + p->nfs + 4) return FD3D_ERR_ARG;
+    if (!(p->dh > 0) || !(p->dt > 0)) return FD3D_ERR_ARG;
+    if (p->law != FD3D_LAW_SW && p->law != FD3D_LAW_FVW) return FD3D_ERR_ARG;
+    if (p->precision != FD3D_PREC_F32 && p->precision != FD3D_PREC_F64) return FD3D_ERR_ARG;
+    if (p->nstations < 0 || p->nstations > FD3D_MAX_STATIONS) return FD3D_ERR_ARG;
+    for (int s = 0; s < p->nstations; ++s)
+        if (p->staX[s] < 1 || p->staX[s] > p->nxt || p->staY[s] < 1 || p->staY[s] > p->nyt || p->staZ[s] < 1 ||
+            p->staZ[s] > p->nzt)
+            return FD3D_ERR_ARG;
+    if (p->history_stride < 0 || p->history_capacity < 0) return FD3D_ERR_ARG;
+    if (p->vp_max > 0 && p->vp_max * p->dt / p->dh > 0.25) return FD3D_ERR_CFL;  // fd3d_init.f90:274-278
+    return FD3D_OK;
+}
+
+Grid make_grid(const fd3d_params& p) {
+    Grid g;
+    g.nxt = p.nxt; g.nyt = p.nyt; g.nzt = p.nzt; g.nabc = p.nabc; g.nfs = p.nfs;
+    g.off = (32 - (p.nabc % 32)) % 32;
+    g.px = ((p.nxt + g.off + 31) / 32) * 32;
+    g.plane = (long long)g.px * p.nyt;
+    g.n3 = g.plane * p.nzt + 64;
+    return g;
+}
+
+// init_pml (fd3d_deriv.f90:1319-1493): strip boxes and damping profiles, in T.
+template <class T>
+void make_pml(const fd3d_params& p, PmlDesc& D, std::vector<T>& prof) {
+    const int nxt = p.nxt, nyt = p.nyt, nzt = p.nzt, nabc = p.nabc, nfs = p.nfs;
+    const int bx[4][6] = {{2, nabc, nabc + 1, nyt - 1, nabc + 1, nzt - nfs},
+                          {nxt - nabc + 1, nxt - 1, nabc + 1, nyt - 1, nabc + 1, nzt - nfs},
+                          {2, nxt - 1, 2, nabc, nabc + 1, nzt - nfs},
+                          {2, nxt - 1, 2, nyt - 1, 2, nabc}};
+    long long base = 0;
+    prof.clear();
+    D.cum[0] = 0;
+    std::vector<std::vector<T>> ox(4), oxS(4), oy(4), oyS(4), oz(4), ozS(4);
+    for (int s = 0; s < 4; ++s) {
+        Strip& S = D.s[s];
+        S.nxb = bx[s][0]; S.nxe = bx[s][1]; S.nyb = bx[s][2]; S.nye = bx[s][3]; S.nzb = bx[s][4]; S.nze = bx[s][5];
+        S.ni = S.nxe - S.nxb + 1; S.nk = S.nze - S.nzb + 1; S.nj1 = S.nye - S.nyb + 2;
+        S.jend_uw = (s == 2) ? S.nye : S.nye + 1;
+        S.ncells = (long long)S.ni * S.nj1 * S.nk;
+        S.base = base;
+        base += S.ncells;
+        D.cum[s + 1] = D.cum[s] + (long long)S.ni * (S.jend_uw - S.nyb + 1) * S.nk;
+        ox[s].assign(S.ni, (T)0); oxS[s].assign(S.ni, (T)0);
+        oy[s].assign(S.nj1, (T)0); oyS[s].assign(S.nj1, (T)0);
+        oz[s].assign(S.nk, (T)0); ozS[s].assign(S.nk, (T)0);
+    }
+    const T dt = (T)p.dt, dh = (T)p.dh;
+    const T omegaM = (T)p.pml_fact * (T)p.pml_vp / ((T)2 * dh * (T)(nabc - 1));
+    const int n = nabc - 1;
+    std::vector<T> om(n), omR(n), omM(n), omRM(n);
+    for (int i = 1; i <= n; ++i) {
+        T r = (T)i / (T)n, rM = ((T)i - (T)0.5) / (T)n;
+        om[i - 1] = (T)0.5 * dt * omegaM * ((r * r) * (r * r));
+        omR[nabc - i - 1] = om[i - 1];
+        omM[i - 1] = (T)0.5 * dt * omegaM * ((rM * rM) * (rM * rM));
+        omRM[nabc - i - 1] = omM[i - 1];
+    }
+    for (int i = 1; i <= n; ++i) {  // 1-based reference index i -> 0-based i-1
+        ox[0][i - 1] = omR[i - 1];  oxS[0][i - 1] = omRM[i - 1];
+        ox[1][i - 1] = omM[i - 1];  oxS[1][i - 1] = om[i - 1];
+        oy[2][i - 1] = omR[i - 1];  ox[2][i - 1] = omR[i - 1];  ox[2][nxt - i - 2] = omM[i - 1];
+        oyS[2][i - 1] = omRM[i - 1]; oxS[2][i - 1] = omRM[i - 1]; oxS[2][nxt - i - 2] = om[i - 1];
+        oz[3][i - 1] = omR[i - 1];  ox[3][i - 1] = omR[i - 1];  ox[3][nxt - i - 2] = omM[i - 1];
+        oy[3][i - 1] = omR[i - 1];
+        ozS[3][i - 1] = omRM[i - 1]; oxS[3][i - 1] = omRM[i - 1]; oxS[3][nxt - i - 2] = om[i - 1];
+        oyS[3][i - 1] = omRM[i - 1];
+    }
+    for (int s = 0; s < 4; ++s) {
+        Strip& S = D.s[s];
+        auto put = [&](const std::vector<T>& v) { int o = (int)prof.size(); prof.insert(prof.end(), v.begin(), v.end()); return o; };
+        S.ox_off = put(ox[s]); S.oxS_off = put(oxS[s]);
+        S.oy_off = put(oy[s]); S.oyS_off = put(oyS[s]);
+        S.oz_off = put(oz[s]); S.ozS_off = put(ozS[s]);
+    }
+}
+
+template <class T>
+StepConst<T> make_const(const fd3d_params& p) {
+    StepConst<T> c;
+    c.dt = (T)p.dt; c.dh = (T)p.dh;
+    c.dth = c.dt / c.dh;
+    c.dth2 = (T)0.5 * c.dt / c.dh;
+    c.dht = c.dh / c.dt;
+    c.damp_s = (T)p.damp_s;
+    c.c1 = (T)9 / (T)8;
+    c.c2 = (T)-1 / (T)24;
+    c.dtA = p.dt;
+    c.dhA = (double)c.dh;
+    c.dthA = c.dtA / c.dhA;
+    return c;
+}
+
+struct CtxBase {
+    fd3d_params p;
+    Grid g;
+    cudaStream_t st = nullptr;
+    int law = 0;
+    int nf = 4;            // history planes per record
+    int steps_done = 0;    // host mirror of the device counter
+    int rec_written = 0;   // history records already written to files
+    bool medium_ok = false, fault_ok = false;
+    int* it_dev = nullptr;
+    int* status = nullptr;
+    int hist_cap = 0;
+    void* ring = nullptr;
+    void* seis = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    float last_ms = 0.f;
+    bool profiling = false;
+    std::vector<cudaEvent_t> kev;   // 2 per kernel id
+    float ktimes[FD3D_NKERNELS] = {0};
+    int klaunch[FD3D_NKERNELS] = {0};
+    cudaGraphExec_t gexec = nullptr;
+    int gsteps = 0;
+    int opt = 1;            // use the tiled interior kernels
+    virtual ~CtxBase() {}
+    virtual int alloc() = 0;
+    virtual int upload_medium(const void*, const void*, const void*, int) = 0;
+    virtual int upload_medium_layers(const double*, const double*, const double*) = 0;
+    virtual int upload_fault(const fd3d_fault*) = 0;
+    virtual int reset() = 0;
+    virtual int enqueue_step() = 0;
+    virtual int fetch_field(int, void*, int) = 0;
+    virtual int fetch_plane(int, double*) = 0;
+    virtual size_t elem() const = 0;
+};
+
+template <class T>
+struct Ctx : CtxBase {
+    Fields<T> f{};
+    Fault<T> q{};
+    FvwScalars fs{};
+    StepConst<T> c{};
+    PmlDesc D{};
+    PmlAux<T> X{};
+    std::vector<void*> allocs;
+    T* fieldpool = nullptr;
+    std::vector<double> psiX0, psiZ0;  // initial FVW state, restored by reset
+    size_t elem() const override { return sizeof(T); }
+
+    template <class U> int dalloc(U** ptr, size_t n) {
+        void* v = nullptr;
+        CK(cudaMalloc(&v, std::max<size_t>(n, 1) * sizeof(U)));
+        CK(cudaMemsetAsync(v, 0, std::max<size_t>(n, 1) * sizeof(U), st));
+        allocs.push_back(v);
+        *ptr = (U*)v;
+        return 0;
+    }
+
+    ~Ctx() override {
+        if (gexec) cudaGraphExecDestroy(gexec);
+        for (void* v : allocs) cudaFree(v);
+        for (auto e : kev) cudaEventDestroy(e);
+        if (ev0) cudaEventDestroy(ev0);
+        if (ev1) cudaEventDestroy(ev1);
+        if (st) cudaStreamDestroy(st);
+    }
+
+    int alloc() override {
+        CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+        CK(cudaEventCreate(&ev0));
+        CK(cudaEventCreate(&ev1));
+        kev.resize(2 * FD3D_NKERNELS);
+        for (auto& e : kev) CK(cudaEventCreate(&e));
+        g = make_grid(p);
+        c = make_const<T>(p);
+        law = p.law;
+        nf = (law == FD3D_LAW_FVW) ? 5 : 4;
+        // 12 arrays of the 3-D grid in one pool
+        if (dalloc(&fieldpool, (size_t)g.n3 * 12)) return FD3D_ERR_NOMEM;
+        T* b = fieldpool;
+        T** outs[9] = {&f.u, &f.v, &f.w, &f.xx, &f.yy, &f.zz, &f.xy, &f.yz, &f.xz};
+        for (int a = 0; a < 9; ++a) *outs[a] = b + (size_t)a * g.n3;
+        f.lam = b + 9 * (size_t)g.n3;
+        f.mu = b + 10 * (size_t)g.n3;
+        f.d = b + 11 * (size_t)g.n3;
+        const size_t n2 = (size_t)p.nxt * p.nzt;
+        T** tp[] = {&q.tx, &q.tz, &q.txt, &q.tzt, &q.RFx, &q.RFz, &q.avdx, &q.avdz, &q.v1t, &q.au1, &q.av1, &q.aw1,
+                    &q.uZ, &q.wX, &q.tabsX, &q.tabsZ, &q.T0X, &q.T0Z, &q.T0Xb, &q.Dc, &q.peakX, &q.dynX, &q.DcX, &q.peakZ,
+                    &q.dynZ, &q.DcZ, &q.coh, &q.aX, &q.bX, &q.vwX, &q.fwX, &q.aZ, &q.bZ, &q.vwZ, &q.fwZ,
+                    &q.schangeX, &q.schangeZ};
+        for (T** a : tp) if (dalloc(a, n2)) return FD3D_ERR_NOMEM;
+        double** dp[] = {&q.psiX, &q.psiZ, &q.distX, &q.distZ, &q.slipX, &q.slipZ, &q.ruptime, &q.rise, &q.sliptime};
+        for (double** a : dp) if (dalloc(a, n2)) return FD3D_ERR_NOMEM;
+        std::vector<T> prof;
+        make_pml<T>(p, D, prof);
+        long long ncell = 0;
+        for (int s = 0; s < 4; ++s) ncell += D.s[s].ncells;
+        T* pool = nullptr;
+        if (dalloc(&pool, (size_t)ncell * AX_N)) return FD3D_ERR_NOMEM;
+        for (int a = 0; a < AX_N; ++a) X.a[a] = pool + (size_t)a * ncell;
+        T* dprof = nullptr;
+        if (dalloc(&dprof, prof.size())) return FD3D_ERR_NOMEM;
+        CK(cudaMemcpyAsync(dprof, prof.data(), prof.size() * sizeof(T), cudaMemcpyHostToDevice, st));
+        X.prof = dprof;
+        if (dalloc(&it_dev, 1)) return FD3D_ERR_NOMEM;
+        if (dalloc(&status, 1)) return FD3D_ERR_NOMEM;
+        const int stride = std::max(1, p.history_stride);
+        p.history_stride = stride;
+        const long long plane = (long long)(p.nxt - 2 * p.nabc) * (p.nzt - p.nfs - p.nabc);
+        int cap = p.history_capacity;
+        if (cap <= 0) {
+            // default: a ring of ~256 MB, at least 8 and at most 4096 records
+            long long rec = plane * nf * (long long)sizeof(T);
+            cap = (int)std::min<long long>(4096, std::max<long long>(8, (256ll << 20) / std::max<long long>(rec, 1)));
+        }
+        hist_cap = cap;
+        T* r = nullptr;
+        if (dalloc(&r, (size_t)cap * nf * plane)) return FD3D_ERR_NOMEM;
+        ring = r;
+        T* sg = nullptr;
+        if (dalloc(&sg, (size_t)cap * std::max(1, p.nstations) * 3)) return FD3D_ERR_NOMEM;
+        seis = sg;
+        CK(cudaStreamSynchronize(st));
+        return FD3D_OK;
+    }
+
+    int upload_medium(const void* l, const void* m, const void* d, int rk) override {
+        if (rk != 4 && rk != 8) return FD3D_ERR_ARG;
+        const size_t n = (size_t)p.nxt * p.nyt * p.nzt;
+        const void* src[3] = {l, m, d};
+        T* dst[3] = {(T*)f.lam, (T*)f.mu, (T*)f.d};
+        if ((size_t)rk == sizeof(T)) {
+            // same element type: one pitched copy per array straight into the padded rows
+            for (int a = 0; a < 3; ++a) {
+                if (!src[a]) return FD3D_ERR_ARG;
+                CK(cudaMemcpy2DAsync(dst[a] + g.off, (size_t)g.px * sizeof(T), src[a], (size_t)p.nxt * sizeof(T),
+                                     (size_t)p.nxt * sizeof(T), (size_t)p.nyt * p.nzt, cudaMemcpyHostToDevice, st));
+            }
+            CK(cudaStreamSynchronize(st));
+            medium_ok = true;
+            return FD3D_OK;
+        }
+        std::vector<T> row((size_t)g.px * p.nyt * 16);
+        for (int a = 0; a < 3; ++a) {
+            if (!src[a]) return FD3D_ERR_ARG;
+            // pack k-slabs into the padded layout on the host, one copy per slab
+            const int kb = 16;
+            for (int k0 = 0; k0 < p.nzt; k0 += kb) {
+                const int nk = std::min(kb, p.nzt - k0);
+                std::fill(row.begin(), row.end(), (T)0);
+                for (int kk = 0; kk < nk; ++kk)
+                    for (int j = 0; j < p.nyt; ++j) {
+                        const size_t so = (size_t)p.nxt * ((size_t)j + (size_t)p.nyt * (k0 + kk));
+                        T* o = row.data() + (size_t)g.px * ((size_t)j + (size_t)p.nyt * kk) + g.off;
+                        if (rk == 8) { const double* s = (const double*)src[a] + so; for (int i = 0; i < p.nxt; ++i) o[i] = (T)s[i]; }
+                        else         { const float* s = (const float*)src[a] + so;  for (int i = 0; i < p.nxt; ++i) o[i] = (T)s[i]; }
+                    }
+                CK(cudaMemcpyAsync(dst[a] + (size_t)g.plane * k0, row.data(), (size_t)g.plane * nk * sizeof(T),
+                                   cudaMemcpyHostToDevice, st));
+                CK(cudaStreamSynchronize(st));
+            }
+        }
+        (void)n;
+        medium_ok = true;
+        return FD3D_OK;
+    }
+
+    int upload_medium_layers(const double* l, const double* m, const double* d) override {
+        if (!l || !m || !d) return FD3D_ERR_ARG;
+        std::vector<T> slab((size_t)g.plane);
+        T* dst[3] = {(T*)f.lam, (T*)f.mu, (T*)f.d};
+        const double* src[3] = {l, m, d};
+        for (int a = 0; a < 3; ++a)
+            for (int k = 0; k < p.nzt; ++k) {
+                std::fill(slab.begin(), slab.end(), (T)0);
+                const T v = (T)src[a][k];
+                for (int j = 0; j < p.nyt; ++j)
+                    for (int i = 0; i < p.nxt; ++i) slab[(size_t)g.px * j + g.off + i] = v;
+                CK(cudaMemcpyAsync(dst[a] + (size_t)g.plane * k, slab.data(), (size_t)g.plane * sizeof(T),
+                                   cudaMemcpyHostToDevice, st));
+                CK(cudaStreamSynchronize(st));
+            }
+        medium_ok = true;
+        return FD3D_OK;
+    }
+
+    int up2(T* dst, const std::vector<T>& v) {
+        CK(cudaMemcpyAsync(dst, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, st));
+        return 0;
+    }
+    int up2d(double* dst, const std::vector<double>& v) {
+        CK(cudaMemcpyAsync(dst, v.data(), v.size() * sizeof(double), cudaMemcpyHostToDevice, st));
+        return 0;
+    }
+
+    // friction arrays + interp_fric (fd3d_deriv.f90:3150-3190)
+    int upload_fault(const fd3d_fault* fl) override {
+        if (!fl) return FD3D_ERR_ARG;
+        const int nxt = p.nxt, nzt = p.nzt;
+        const size_t n2 = (size_t)nxt * nzt;
+        auto cp = [&](const double* s, double dflt) {
+            std::vector<T> v(n2);
+            for (size_t k = 0; k < n2; ++k) v[k] = (T)(s ? s[k] : dflt);
+            return v;
+        };
+        if (!fl->striniX || !fl->Dc) return FD3D_ERR_ARG;
+        std::vector<T> sX = cp(fl->striniX, 0), sZ = cp(fl->striniZ, 0), Dc = cp(fl->Dc, 0);
+        std::vector<T> zero(n2, (T)0);
+        std::vector<T> pkX = zero, dyX = zero, DcX = zero, T0X = zero;
+        std::vector<T> pkZ = zero, dyZ = zero, DcZ = zero, T0Z = sZ, coh = zero;
+        auto I2 = [&](int i, int k) { return (size_t)(i - 1) + (size_t)nxt * (k - 1); };
+        int rc = 0;
+        if (law == FD3D_LAW_FVW) {
+            if (!fl->a || !fl->b || !fl->psi || !fl->vw || !fl->aX || !fl->bX || !fl->psiX || !fl->vwX) return FD3D_ERR_ARG;
+            rc |= up2(q.aZ, cp(fl->a, 0)); rc |= up2(q.bZ, cp(fl->b, 0)); rc |= up2(q.vwZ, cp(fl->vw, 0));
+            rc |= up2(q.aX, cp(fl->aX, 0)); rc |= up2(q.bX, cp(fl->bX, 0)); rc |= up2(q.vwX, cp(fl->vwX, 0));
+            rc |= up2(q.fwZ, cp(fl->fwZ, fl->fw)); rc |= up2(q.fwX, cp(fl->fwX, fl->fw));
+            psiZ0.assign(fl->psi, fl->psi + n2);
+            psiX0.assign(fl->psiX, fl->psiX + n2);
+            fs.Sn = fl->Sn; fs.v0 = fl->v0; fs.f0 = fl->f0; fs.fw = fl->fw; fs.uini = fl->uini; fs.wini = fl->wini;
+            fs.nucleation = fl->nucleation;
+            fs.hx0 = fl->hx0; fs.hz0 = fl->hz0; fs.perturb = fl->perturb; fs.RR2 = fl->RR2; fs.TT2 = fl->TT2;
+            fs.strinixI = fl->strinixI;
+        } else {
+            if (!fl->peak_xz || !fl->dyn_xz) return FD3D_ERR_ARG;
+            pkZ = cp(fl->peak_xz, 0); dyZ = cp(fl->dyn_xz, 0); DcZ = Dc; coh = cp(fl->coh, 0);
+            fs = FvwScalars{};
+        }
+        for (int i = 2; i <= nxt - 1; ++i)
+            for (int k = 2; k <= nzt - 1; ++k) {
+                if (law != FD3D_LAW_FVW) {
+                    pkX[I2(i, k)] = (pkZ[I2(i, k)] + pkZ[I2(i - 1, k)] + pkZ[I2(i, k - 1)] + pkZ[I2(i - 1, k - 1)]) / (T)4;
+                    dyX[I2(i, k)] = (dyZ[I2(i, k)] + dyZ[I2(i - 1, k)] + dyZ[I2(i, k - 1)] + dyZ[I2(i - 1, k - 1)]) / (T)4;
+                    DcX[I2(i, k)] = (DcZ[I2(i, k)] + DcZ[I2(i - 1, k)] + DcZ[I2(i, k - 1)] + DcZ[I2(i - 1, k - 1)]) / (T)4;
+                }
+                T0X[I2(i, k)] = (sX[I2(i, k)] + sX[I2(i - 1, k)] + sX[I2(i, k - 1)] + sX[I2(i - 1, k - 1)]) / (T)4;
+            }
+        rc |= up2(q.Dc, Dc); rc |= up2(q.T0X, T0X); rc |= up2(q.T0Xb, T0X); rc |= up2(q.T0Z, T0Z);
+        rc |= up2(q.peakX, pkX); rc |= up2(q.dynX, dyX); rc |= up2(q.DcX, DcX);
+        rc |= up2(q.peakZ, pkZ); rc |= up2(q.dynZ, dyZ); rc |= up2(q.DcZ, DcZ); rc |= up2(q.coh, coh);
+        if (rc) return FD3D_ERR_CUDA;
+        CK(cudaStreamSynchronize(st));
+        fault_ok = true;
+        return reset_state(false);
+    }
+
+    // zeroing of fd3d_theo.f90:59-88 and of the PML aux (fd3d_deriv.f90:1342-1410)
+    int reset_state(bool keep_psi) {
+        (void)keep_psi;
+        CK(cudaMemsetAsync(fieldpool, 0, (size_t)g.n3 * 9 * sizeof(T), st));
+        const size_t n2 = (size_t)p.nxt * p.nzt;
+        T* zt[] = {q.tx, q.tz, q.txt, q.tzt, q.RFx, q.RFz, q.avdx, q.avdz, q.v1t, q.au1, q.av1, q.aw1, q.uZ, q.wX,
+                   q.schangeX, q.schangeZ};
+        for (T* a : zt) CK(cudaMemsetAsync(a, 0, n2 * sizeof(T), st));
+        double* zd[] = {q.distX, q.distZ, q.slipX, q.slipZ, q.rise};
+        for (double* a : zd) CK(cudaMemsetAsync(a, 0, n2 * sizeof(double), st));
+        std::vector<double> big(n2, 1.e4);
+        CK(cudaMemcpyAsync(q.ruptime, big.data(), n2 * sizeof(double), cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(q.sliptime, big.data(), n2 * sizeof(double), cudaMemcpyHostToDevice, st));
+        std::vector<T> t0(n2, law == FD3D_LAW_FVW ? (T)1 : (T)0);
+        CK(cudaMemcpyAsync(q.tabsX, t0.data(), n2 * sizeof(T), cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(q.tabsZ, t0.data(), n2 * sizeof(T), cudaMemcpyHostToDevice, st));
+        // initial state variable and prestress (the nucleation ramp rewrites T0X)
+        CK(cudaMemcpyAsync(q.T0X, q.T0Xb, n2 * sizeof(T), cudaMemcpyDeviceToDevice, st));
+        if (law == FD3D_LAW_FVW) {
+            CK(cudaMemcpyAsync(q.psiZ, psiZ0.data(), n2 * sizeof(double), cudaMemcpyHostToDevice, st));
+            CK(cudaMemcpyAsync(q.psiX, psiX0.data(), n2 * sizeof(double), cudaMemcpyHostToDevice, st));
+        }
+        long long ncell = 0;
+        for (int s = 0; s < 4; ++s) ncell += D.s[s].ncells;
+        CK(cudaMemsetAsync(X.a[0], 0, (size_t)ncell * AX_N * sizeof(T), st));
+        CK(cudaMemsetAsync(it_dev, 0, sizeof(int), st));
+        CK(cudaMemsetAsync(status, 0, sizeof(int), st));
+        CK(cudaStreamSynchronize(st));
+        steps_done = 0;
+        rec_written = 0;
+        return FD3D_OK;
+    }
+
+    int reset() override {
+        if (!fault_ok) return FD3D_ERR_STATE;
+        return reset_state(false);
+    }
+
+    void kbeg(int id) { if (profiling) cudaEventRecord(kev[2 * id], st); }
+    void kend(int id) {
+        if (!profiling) return;
+        cudaEventRecord(kev[2 * id + 1], st);
+        cudaEventSynchronize(kev[2 * id + 1]);
+        float ms = 0;
+        cudaEventElapsedTime(&ms, kev[2 * id], kev[2 * id + 1]);
+        ktimes[id] += ms;
+        klaunch[id] += 1;
+    }
+
+    int enqueue_step() override {
+        const int nxT = p.nxt - 2 * p.nabc;
+        const int nyI = p.nyt - 2 - p.nabc;
+        const int nzT = g.ks() - p.nabc;
+        const dim3 b2(32, 8);
+        // velocity half-step
+        kbeg(0);
+        if (opt) launch_vel_interior_opt<T>(g, f, c, st);
+        else {
+            const int kch = 4;
+            k_vel_interior<T><<<dim3((nxT + 31) / 32, (nyI + 7) / 8, (nzT + kch - 1) / kch), b2, 0, st>>>(g, f, c, kch);
+        }
+        kend(0);
+        kbeg(1);
+        k_vel_fault<T><<<dim3((std::max(nxT, p.nxt) + 31) / 32, (nzT + 7) / 8), b2, 0, st>>>(g, f, q, c, law, fs, it_dev, status);
+        kend(1);
+        const long long npml = D.cum[4];
+        kbeg(2);
+        k_vel_pml<T><<<(unsigned)((npml + 255) / 256), 256, 0, st>>>(g, f, D, X, c);
+        kend(2);
+        kbeg(3);
+        k_vel_fs<T><<<dim3((p.nxt + 31) / 32, (p.nyt + 7) / 8), b2, 0, st>>>(g, f);
+        kend(3);
+        // stress half-step
+        kbeg(4);
+        if (opt) launch_str_interior_opt<T>(g, f, c, st);
+        else {
+            const int kch = 4;
+            k_str_interior<T><<<dim3((nxT + 31) / 32, (nyI + 7) / 8, (nzT + kch - 1) / kch), b2, 0, st>>>(g, f, c, kch);
+        }
+        kend(4);
+        kbeg(5);
+        k_str_fault<T><<<dim3((nxT + 31) / 32, (nzT + 7) / 8), b2, 0, st>>>(g, f, q, c);
+        kend(5);
+        kbeg(6);
+        k_str_pml<T><<<(unsigned)((npml + 255) / 256), 256, 0, st>>>(g, f, D, X, c);
+        kend(6);
+        // fault boundary condition
+        kbeg(7);
+        k_str_fs<T><<<dim3((p.nxt + 31) / 32, (p.nyt + 7) / 8), b2, 0, st>>>(g, f);
+        k_traction<T><<<dim3((nxT + 31) / 32, (nzT + 7) / 8), b2, 0, st>>>(g, f, q, c);
+        k_friction<T><<<dim3((nxT + 31) / 32, (nzT + 7) / 8), b2, 0, st>>>(g, f, q, c, law, fs, it_dev);
+        HistDesc h;
+        h.ring = ring; h.cap = hist_cap; h.stride = p.history_stride; h.nf = nf; h.nst = p.nstations;
+        for (int s = 0; s < p.nstations; ++s) { h.sta[3 * s] = p.staX[s]; h.sta[3 * s + 1] = p.staY[s]; h.sta[3 * s + 2] = p.staZ[s]; }
+        h.seis = seis;
+        k_output<T><<<dim3((nxT + 31) / 32, (nzT + 7) / 8), b2, 0, st>>>(g, f, q, law, it_dev, h, status);
+        if (law == FD3D_LAW_FVW && fs.nucleation) {
+            const int ni = (p.nxt - p.nabc) - (p.nabc - 1) + 1, nk = g.ks() - (p.nabc - 1) + 1;
+            k_nucleation<T><<<dim3((ni + 31) / 32, (nk + 7) / 8), b2, 0, st>>>(g, q, c, fs, it_dev);
+        }
+        kend(7);
+        return FD3D_OK;
+    }
+
+    int fetch_field(int which, void* host, int rk) override {
+        if (rk != 4 && rk != 8) return FD3D_ERR_ARG;
+        const T* src;
+        switch (which) {
+            case FD3D_FIELD_U: src = f.u; break;   case FD3D_FIELD_V: src = f.v; break;
+            case FD3D_FIELD_W: src = f.w; break;   case FD3D_FIELD_XX: src = f.xx; break;
+            case FD3D_FIELD_YY: src = f.yy; break; case FD3D_FIELD_ZZ: src = f.zz; break;
+            case FD3D_FIELD_XY: src = f.xy; break; case FD3D_FIELD_YZ: src = f.yz; break;
+            case FD3D_FIELD_XZ: src = f.xz; break;
+            default: return FD3D_ERR_ARG;
+        }
+        std::vector<T> slab((size_t)g.plane);
+        for (int k = 0; k < p.nzt; ++k) {
+            CK(cudaMemcpyAsync(slab.data(), src + (size_t)g.plane * k, (size_t)g.plane * sizeof(T), cudaMemcpyDeviceToHost, st));
+            CK(cudaStreamSynchronize(st));
+            for (int j = 0; j < p.nyt; ++j) {
+                const size_t o = (size_t)p.nxt * ((size_t)j + (size_t)p.nyt * k);
+                const T* s = slab.data() + (size_t)g.px * j + g.off;
+                if (rk == 8) { double* d = (double*)host + o; for (int i = 0; i < p.nxt; ++i) d[i] = (double)s[i]; }
+                else         { float* d = (float*)host + o;  for (int i = 0; i < p.nxt; ++i) d[i] = (float)s[i]; }
+            }
+        }
+        return FD3D_OK;
+    }
+
+    int fetch_plane(int which, double* host) override {
+        const size_t n2 = (size_t)p.nxt * p.nzt;
+        const T* ts = nullptr;
+        const double* ds = nullptr;
+        switch (which) {
+            case FD3D_PLANE_TX: ts = q.tx; break;            case FD3D_PLANE_TZ: ts = q.tz; break;
+            case FD3D_PLANE_SLIPX: ds = q.slipX; break;      case FD3D_PLANE_SLIPZ: ds = q.slipZ; break;
+            case FD3D_PLANE_RUPTIME: ds = q.ruptime; break;  case FD3D_PLANE_RISE: ds = q.rise; break;
+            case FD3D_PLANE_SLIPTIME: ds = q.sliptime; break;
+            case FD3D_PLANE_DISTX: ds = q.distX; break;      case FD3D_PLANE_DISTZ: ds = q.distZ; break;
+            case FD3D_PLANE_PSIX: ds = q.psiX; break;        case FD3D_PLANE_PSIZ: ds = q.psiZ; break;
+            case FD3D_PLANE_T0X: ts = q.T0X; break;          case FD3D_PLANE_T0Z: ts = q.T0Z; break;
+            case FD3D_PLANE_SCHANGEX: ts = q.schangeX; break; case FD3D_PLANE_SCHANGEZ: ts = q.schangeZ; break;
+            default: return FD3D_ERR_ARG;
+        }
+        if (ds) {
+            CK(cudaMemcpyAsync(host, ds, n2 * sizeof(double), cudaMemcpyDeviceToHost, st));
+            CK(cudaStreamSynchronize(st));
+        } else {
+            std::vector<T> v(n2);
+            CK(cudaMemcpyAsync(v.data(), ts, n2 * sizeof(T), cudaMemcpyDeviceToHost, st));
+            CK(cudaStreamSynchronize(st));
+            for (size_t k = 0; k < n2; ++k) host[k] = (double)v[k];
+        }
+        return FD3D_OK;
+    }
+};
+
+}  // namespace fd3d
+
+struct fd3d_ctx {
+    CtxBase* impl;
+};
+
+extern "C" {
+
+const char* fd3d_version(void) { return "fd3d-b200 0.1 (sm_100a)"; }
+
+const char* fd3d_status_string(int s) {
+    switch (s) {
+        case FD3D_OK: return "ok";
+        case FD3D_ERR_ARG: return "bad argument";
+        case FD3D_ERR_CFL: return "CFL > 0.25: simulation would be numerically unstable";
+        case FD3D_ERR_CUDA: return "CUDA runtime error";
+        case FD3D_ERR_NOMEM: return "out of device memory / HBM budget";
+        case FD3D_ERR_NEWTON: return "FVW Newton solve did not converge";
+        case FD3D_ERR_NONFINITE: return "non-finite value on the fault plane";
+        case FD3D_ERR_STATE: return "call out of order";
+        case FD3D_ERR_IO: return "file I/O error";
+        case FD3D_ERR_NODEV: return "no CUDA device";
+        case FD3D_ERR_BUSY: return "no free slot";
+        default: return "unknown status";
+    }
+}
+
+int fd3d_device_count(int* count) {
+    if (!count) return FD3D_ERR_ARG;
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess) { cudaGetLastError(); *count = 0; return FD3D_OK; }
+    *count = n;
+    return FD3D_OK;
+}
+
+int fd3d_set_device(int dev) {
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess) { cudaGetLastError(); return FD3D_ERR_NODEV; }
+    if (dev < 0 || dev >= n) return FD3D_ERR_ARG;
+    CK(cudaSetDevice(dev));
+    return FD3D_OK;
+}
+
+int fd3d_ctx_create(const fd3d_params* p, fd3d_ctx** out) {
+    if (!out) return FD3D_ERR_ARG;
+    *out = nullptr;
+    int rc = validate_params(p);
+    if (rc) return rc;
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) { cudaGetLastError(); return FD3D_ERR_NODEV; }
+    CtxBase* c = (p->precision == FD3D_PREC_F64) ? (CtxBase*)new Ctx<double>() : (CtxBase*)new Ctx<float>();
+    c->p = *p;
+    const char* e = std::getenv("FD3D_NAIVE_INTERIOR");
+    if (e && e[0] == '1') c->opt = 0;
+    rc = c->alloc();
+    if (rc) {
+        delete c;
+        return rc == FD3D_ERR_CUDA ? FD3D_ERR_NOMEM : rc;
+    }
+    *out = new fd3d_ctx{c};
+    return FD3D_OK;
+}
+
+int fd3d_ctx_destroy(fd3d_ctx* ctx) {
+    if (!ctx) return FD3D_ERR_ARG;
+    if (ctx->impl->st) cudaStreamSynchronize(ctx->impl->st);
+    delete ctx->impl;
+    delete ctx;
+    return FD3D_OK;
+}
+
+int fd3d_upload_medium(fd3d_ctx* ctx, const void* l, const void* m, const void* d, int rk) {
+    if (!ctx) return FD3D_ERR_ARG;
+    return ctx->impl->upload_medium(l, m, d, rk);
+}
+
+int fd3d_upload_medium_layers(fd3d_ctx* ctx, const double* l, const double* m, const double* d) {
+    if (!ctx) return FD3D_ERR_ARG;
+    return ctx->impl->upload_medium_layers(l, m, d);
+}
+
+int fd3d_upload_fault(fd3d_ctx* ctx, const fd3d_fault* f) {
+    if (!ctx) return FD3D_ERR_ARG;
+    return ctx->impl->upload_fault(f);
+}
+
+int fd3d_reset(fd3d_ctx* ctx) {
+    if (!ctx) return FD3D_ERR_ARG;
+    return ctx->impl->reset();
+}
+
+static int build_graph(CtxBase* c, int nsteps) {
+    if (c->gexec) { cudaGraphExecDestroy(c->gexec); c->gexec = nullptr; }
+    cudaGraph_t gr;
+    CK(cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal));
+    for (int s = 0; s < nsteps; ++s) c->enqueue_step();
+    CK(cudaStreamEndCapture(c->st, &gr));
+    cudaError_t e = cudaGraphInstantiate(&c->gexec, gr, 0);
+    cudaGraphDestroy(gr);
+    if (e != cudaSuccess) { c->gexec = nullptr; return FD3D_ERR_CUDA; }
+    c->gsteps = nsteps;
+    return FD3D_OK;
+}
+
+int fd3d_run(fd3d_ctx* ctx, int nsteps) {
+    if (!ctx || nsteps < 0) return FD3D_ERR_ARG;
+    CtxBase* c = ctx->impl;
+    if (!c->medium_ok || !c->fault_ok) return FD3D_ERR_STATE;
+    CK(cudaEventRecord(c->ev0, c->st));
+    int left = nsteps;
+    const int chunk = 16;
+    if (!c->profiling && left >= chunk) {
+        if (!c->gexec || c->gsteps != chunk) {
+            int rc = build_graph(c, chunk);
+            if (rc) return rc;
+        }
+        while (left >= chunk) {
+            CK(cudaGraphLaunch(c->gexec, c->st));
+            left -= chunk;
+        }
+    }
+    for (int s = 0; s < left; ++s) c->enqueue_step();
+    CK(cudaGetLastError());
+    CK(cudaEventRecord(c->ev1, c->st));
+    c->steps_done += nsteps;
+    return FD3D_OK;
+}
+
+int fd3d_sync(fd3d_ctx* ctx) {
+    if (!ctx) return FD3D_ERR_ARG;
+    CtxBase* c = ctx->impl;
+    CK(cudaStreamSynchronize(c->st));
+    CK(cudaEventElapsedTime(&c->last_ms, c->ev0, c->ev1));
+    int st = 0;
+    CK(cudaMemcpy(&st, c->status, sizeof(int), cudaMemcpyDeviceToHost));
+    if (st & ST_NONFINITE) return FD3D_ERR_NONFINITE;
+    if (st & ST_NEWTON) return FD3D_ERR_NEWTON;
+    return FD3D_OK;
+}
+
+int fd3d_steps_done(fd3d_ctx* ctx, int* it) {
+    if (!ctx || !it) return FD3D_ERR_ARG;
+    *it = ctx->impl->steps_done;
+    return FD3D_OK;
+}
+
+int fd3d_last_run_ms(fd3d_ctx* ctx, float* ms) {
+    if (!ctx || !ms) return FD3D_ERR_ARG;
+    *ms = ctx->impl->last_ms;
+    return FD3D_OK;
+}
+
+int fd3d_set_profiling(fd3d_ctx* ctx, int on) {
+    if (!ctx) return FD3D_ERR_ARG;
+    CtxBase* c = ctx->impl;
+    c->profiling = on != 0;
+    for (int k = 0; k < FD3D_NKERNELS; ++k) { c->ktimes[k] = 0; c->klaunch[k] = 0; }
+    return FD3D_OK;
+}
+
+int fd3d_kernel_times(fd3d_ctx* ctx, float* ms, int* launches) {
+    if (!ctx || !ms) return FD3D_ERR_ARG;
+    CtxBase* c = ctx->impl;
+    for (int k = 0; k < FD3D_NKERNELS; ++k) {
+        ms[k] = c->ktimes[k];
+        if (launches) launches[k] = c->klaunch[k];
+    }
+    return FD3D_OK;
+}
+
+int fd3d_history_records(fd3d_ctx* ctx, int* nrec) {
+    if (!ctx || !nrec) return FD3D_ERR_ARG;
+    CtxBase* c = ctx->impl;
+    *nrec = c->steps_done / c->p.history_stride;
+    return FD3D_OK;
+}
+
+int fd3d_fetch_history(fd3d_ctx* ctx, int field, int rec0, int nrec, void* host, int rk) {
+    if (!ctx || !host || nrec < 0 || rec0 < 0 || (rk != 4 && rk != 8)) return FD3D_ERR_ARG;
+    CtxBase* c = ctx->impl;
+    if (field < 0 || field >= c->nf) return FD3D_ERR_ARG;
+    const int have = c->steps_done / c->p.history_stride;
+    if (rec0 + nrec > have || rec0 < have - c->hist_cap) return FD3D_ERR_ARG;  // overwritten or not yet made
+    CK(cudaStreamSynchronize(c->st));
+    const size_t plane = (size_t)(c->p.nxt - 2 * c->p.nabc) * (c->p.nzt - c->p.nfs - c->p.nabc);
+    const size_t es = c->elem();
+    std::vector<char> buf(plane * es);
+    for (int r = 0; r < nrec; ++r) {
+        const size_t slot = (size_t)((rec0 + r) % c->hist_cap);
+        const char* src = (const char*)c->ring + (slot * c->nf + field) * plane * es;
+        CK(cudaMemcpy(buf.data(), src, plane * es, cudaMemcpyDeviceToHost));
+        for (size_t k = 0; k < plane; ++k) {
+            double v = es == 4 ? (double)((float*)buf.data())[k] : ((double*)buf.data())[k];
+            if (rk == 8) ((double*)host)[(size_t)r * plane + k] = v;
+            else ((float*)host)[(size_t)r * plane + k] = (float)v;
+        }
+    }
+    return FD3D_OK;
+}
+
+int fd3d_fetch_stations(fd3d_ctx* ctx, int rec0, int nrec, double* host) {
+    if (!ctx || !host || nrec < 0 || rec0 < 0) return FD3D_ERR_ARG;
+    CtxBase* c = ctx->impl;
+    const int have = c->steps_done / c->p.history_stride;
+    if (rec0 + nrec > have || rec0 < have - c->hist_cap) return FD3D_ERR_ARG;
+    CK(cudaStreamSynchronize(c->st));
+    const int ns = c->p.nstations;
+    const size_t es = c->elem();
+    std::vector<char> buf((size_t)3 * std::max(ns, 1) * es);
+    for (int r = 0; r < nrec; ++r) {
+        const size_t slot = (size_t)((rec0 + r) % c->hist_cap);
+        CK(cudaMemcpy(buf.data(), (const char*)c->seis + slot * 3 * ns * es, 3 * ns * es, cudaMemcpyDeviceToHost));
+        for (int q = 0; q < 3 * ns; ++q)
+            host[(size_t)r * 3 * ns + q] = es == 4 ? (double)((float*)buf.data())[q] : ((double*)buf.data())[q];
+    }
+    return FD3D_OK;
+}
+
+int fd3d_fetch_field(fd3d_ctx* ctx, int field, void* host, int rk) {
+    if (!ctx || !host) return FD3D_ERR_ARG;
+    CK(cudaStreamSynchronize(ctx->impl->st));
+    return ctx->impl->fetch_field(field, host, rk);
+}
+
+int fd3d_fetch_plane(fd3d_ctx* ctx, int plane, double* host) {
+    if (!ctx || !host) return FD3D_ERR_ARG;
+    CK(cudaStreamSynchronize(ctx->impl->st));
+    return ctx->impl->fetch_plane(plane, host);
+}
+
+int fd3d_fetch_final(fd3d_ctx* ctx, double* slipX, double* slipZ, double* ruptime, double* rise, double* sliptime) {
+    if (!ctx) return FD3D_ERR_ARG;
+    int rc = 0;
+    CtxBase* c = ctx->impl;
+    const size_t n2 = (size_t)c->p.nxt * c->p.nzt;
+    if (slipX) rc |= fd3d_fetch_plane(ctx, FD3D_PLANE_SLIPX, slipX);
+    if (slipZ) rc |= fd3d_fetch_plane(ctx, FD3D_PLANE_SLIPZ, slipZ);
+    std::vector<double> rt(n2);
+    rc |= fd3d_fetch_plane(ctx, FD3D_PLANE_RUPTIME, rt.data());
+    if (ruptime) std::memcpy(ruptime, rt.data(), n2 * sizeof(double));
+    if (rise) {  // rise = rise - ruptime (fd3d_theo.f90:658)
+        rc |= fd3d_fetch_plane(ctx, FD3D_PLANE_RISE, rise);
+        for (size_t k = 0; k < n2; ++k) rise[k] = rise[k] - rt[k];
+    }
+    if (sliptime) rc |= fd3d_fetch_plane(ctx, FD3D_PLANE_SLIPTIME, sliptime);
+    return rc ? FD3D_ERR_CUDA : FD3D_OK;
+}
+
+int fd3d_write_results(fd3d_ctx* ctx, const char* dir, int rk) {
+    if (!ctx || !dir || (rk != 4 && rk != 8)) return FD3D_ERR_ARG;
+    return fd3d::write_results(ctx, ctx->impl->p, ctx->impl->nf, ctx->impl->rec_written, dir, rk);
+}
+
+}  // extern "C"

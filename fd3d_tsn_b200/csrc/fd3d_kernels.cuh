@@ -1,0 +1,643 @@
+// fd3d_kernels.cuh -- sm_100a kernels of one FD3D_TSN time step (templated on the
+// field type T: float for the production build, double for the FP64 build).
+//
+// The step is eight launches, each a set of reference regions whose write sets are
+// disjoint and which read nothing another thread of the same launch writes:
+//   1 vel_interior  uxx1/vyy1/wzz1 (fd3d_deriv.f90:50-193)
+//   2 vel_fault     uxx0a/vyy0a/wzz0a at j=nyt-1 + v mirror (fd3d_deriv.f90:198-508),
+//                   tasu1/tasw1 at j=nyt (fd3d_deriv.f90:1109-1234)
+//   3 vel_pml       pml_uvw, 4 strips (fd3d_deriv.f90:1927-2299)
+//   4 vel_fs        fuvw (fd3d_deriv.f90:1018-1062)
+//   5 str_interior  dstres (fd3d_deriv.f90:513-622)
+//   6 str_fault     sxx/sxy0/sxz0/syz0 at j=nyt-1 + xy/yz mirror, sxz1, tasii
+//                   (fd3d_deriv.f90:677-1012,1239-1314)
+//   7 str_pml       pml_xyz (fd3d_deriv.f90:2304-2992)
+//   8 str_fs        fres (fd3d_deriv.f90:1067-1104)
+// followed by the fault boundary condition (fd3d_theo.f90:233-542) in three plane
+// launches: traction, friction (|T| + friction law + slip), output planes.
+//
+// Operation order inside every expression follows the reference so that, with
+// contraction of multiply-add switched off (--fmad=false), the FP32 and FP64
+// builds reproduce the CPU restatement's arithmetic exactly for slip weakening.
+#pragma once
+#include "fd3d_common.cuh"
+
+namespace fd3d {
+
+// ---------------------------------------------------------------- velocity
+// Interior 4th-order velocity: one thread per (i,j), marching a chunk of k.
+template <class T>
+__global__ void __launch_bounds__(256) k_vel_interior(Grid g, Fields<T> f, StepConst<T> c, int kchunk) {
+    const int i = g.nabc + 1 + blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = g.nabc + 1 + blockIdx.y * blockDim.y + threadIdx.y;
+    if (i > g.nxt - g.nabc || j > g.nyt - 2) return;
+    const int kb = g.nabc + 1 + blockIdx.z * kchunk;
+    const int ke = min(kb + kchunk - 1, g.ks());
+    const long long sy = g.px, sz = g.plane;
+    const T c1 = c.c1, c2 = c.c2;
+    const T* __restrict__ xx = f.xx; const T* __restrict__ yy = f.yy; const T* __restrict__ zz = f.zz;
+    const T* __restrict__ xy = f.xy; const T* __restrict__ yz = f.yz; const T* __restrict__ xz = f.xz;
+    for (int k = kb; k <= ke; ++k) {
+        const long long p = g.at(i, j, k);
+        const T r = c.dth / f.d[p];
+        f.u[p] = f.u[p] + r * (c1 * (xx[p] - xx[p - 1]) + c2 * (xx[p + 1] - xx[p - 2]) +
+                               c1 * (xy[p] - xy[p - sy]) + c2 * (xy[p + sy] - xy[p - 2 * sy]) +
+                               c1 * (xz[p] - xz[p - sz]) + c2 * (xz[p + sz] - xz[p - 2 * sz]));
+        f.v[p] = f.v[p] + r * (c1 * (xy[p + 1] - xy[p]) + c2 * (xy[p + 2] - xy[p - 1]) +
+                               c1 * (yy[p + sy] - yy[p]) + c2 * (yy[p + 2 * sy] - yy[p - sy]) +
+                               c1 * (yz[p] - yz[p - sz]) + c2 * (yz[p + sz] - yz[p - 2 * sz]));
+        f.w[p] = f.w[p] + r * (c1 * (xz[p + 1] - xz[p]) + c2 * (xz[p + 2] - xz[p - 1]) +
+                               c1 * (yz[p] - yz[p - sy]) + c2 * (yz[p + sy] - yz[p - 2 * sy]) +
+                               c1 * (zz[p + sz] - zz[p]) + c2 * (zz[p + 2 * sz] - zz[p - sz]));
+    }
+}
+
+// FVW Newton solve of one node (fd3d_deriv.f90:1148-1161), FP64, bounded.
+__device__ __forceinline__ double fvw_newton(double vtilde, double cdelta, double uw, double psi, double a,
+                                             double v0, int* status) {
+    const double e = v0 * exp(-psi / a);
+    double ferr = 10.0;
+    int it = 0;
+    while (fabs(ferr) > 1e-10) {
+        ++it;
+        const double fwv = vtilde + cdelta * uw + sinh(uw) * e;
+        const double dfw = cdelta + cosh(uw) * e;
+        ferr = fwv / dfw;
+        uw = uw - ferr;
+        if (it > FD3D_NEWTON_MAXIT) { atomicOr(status, ST_NEWTON); break; }
+    }
+    return uw;
+}
+
+// Band j=nyt-1 (2nd order + damping, v mirror) and split-node fault velocity at j=nyt.
+template <class T>
+__global__ void k_vel_fault(Grid g, Fields<T> f, Fault<T> q, StepConst<T> c, int law, FvwScalars s,
+                            int* it_dev, int* status) {
+    const int ii = blockIdx.x * blockDim.x + threadIdx.x;
+    const int kk = blockIdx.y * blockDim.y + threadIdx.y;
+    if (ii == 0 && kk == 0) atomicAdd(it_dev, 1);  // step counter read by the fault BC launches
+    const int ks = g.ks();
+    const long long sy = g.px, sz = g.plane;
+    // ghost row k=ks+1: v(:,nyt,ks+1) = v(:,nyt-1,ks+1)  (bnd2d mirror, fd3d_deriv.f90:225-232)
+    if (kk == 0 && ii < g.nxt) {
+        const long long p = g.at(ii + 1, g.nyt - 1, ks + 1);
+        f.v[p + sy] = f.v[p];
+    }
+    const int i = g.nabc + 1 + ii, k = g.nabc + 1 + kk;
+    if (i > g.nxt - g.nabc || k > ks) return;
+    const int n2 = g.at2(i, k);
+    {   // uxx0a / vyy0a / wzz0a  (fd3d_deriv.f90:284-508)
+        const long long p = g.at(i, g.nyt - 1, k);
+        const T r = c.dth / f.d[p];
+        const T pdx = (f.xx[p] - f.xx[p - 1]) + (f.xy[p] - f.xy[p - sy]) + (f.xz[p] - f.xz[p - sz]);
+        const T au = pdx - q.au1[n2];
+        f.u[p] = f.u[p] + r * (pdx + c.damp_s * au);
+        q.au1[n2] = pdx;
+        const T pdy = (f.xy[p + 1] - f.xy[p]) + (f.yy[p + sy] - f.yy[p]) + (f.yz[p] - f.yz[p - sz]);
+        const T av = pdy - q.av1[n2];
+        const T vn = f.v[p] + r * (pdy + c.damp_s * av);
+        f.v[p] = vn;
+        f.v[p + sy] = vn;  // mirror into the fault plane
+        q.av1[n2] = pdy;
+        const T pdz = (f.xz[p + 1] - f.xz[p]) + (f.yz[p] - f.yz[p - sy]) + (f.zz[p + sz] - f.zz[p]);
+        const T aw = pdz - q.aw1[n2];
+        f.w[p] = f.w[p] + r * (pdz + c.damp_s * aw);
+        q.aw1[n2] = pdz;
+    }
+    const long long pf = g.at(i, g.nyt, k);
+    if (law == 0) {  // tasu1/tasw1 slip weakening
+        const T r = c.dth / f.d[pf];
+        f.u[pf] = f.u[pf] + r * (T)2 * (q.tx[n2] + q.RFx[n2]);
+        f.w[pf] = f.w[pf] + r * ((T)2 * (q.tz[n2] + q.RFz[n2]));
+        return;
+    }
+    // FVW (fd3d_deriv.f90:1141-1162, 1204-1226), FP64
+    const double d = (double)f.d[pf];
+    const double rr = c.dthA / d;
+    {
+        const double u = (double)f.u[pf];
+        const double a = (double)q.aX[n2];
+        const double s1 = 2.0 * (fabs((double)q.wX[n2]) + fabs(s.wini)), s2 = 2.0 * (fabs(u) + fabs(s.uini));
+        const double sr = sqrt(s1 * s1 + s2 * s2);
+        const double cdelta = 2.0 * rr * s.Sn * a;
+        double uw = asinh(exp(q.psiX[n2] / a) * sr / (2.0 * s.v0));
+        const double rfz = ((double)q.RFz[n2] + (double)q.RFz[g.at2(i - 1, k)] + (double)q.RFz[g.at2(i, k - 1)] +
+                            (double)q.RFz[g.at2(i - 1, k - 1)]) / 4.0;
+        const double q1 = (double)q.wX[n2] + 2.0 * rr * (rfz - (double)q.T0Z[n2]);
+        const double q2 = u + 2.0 * rr * ((double)q.RFx[n2] - (double)q.T0X[n2]);
+        const double vt = -sqrt(q1 * q1 + q2 * q2);
+        uw = fvw_newton(vt, cdelta, uw, q.psiX[n2], a, s.v0, status);
+        f.u[pf] = (T)(((double)q.tx[n2] + (double)q.T0X[n2]) * (-sinh(uw)) * s.v0 * exp(-q.psiX[n2] / a) /
+                      (double)q.tabsX[n2] + s.uini);
+    }
+    {
+        const double w = (double)f.w[pf];
+        const double a = (double)q.aZ[n2];
+        const double s1 = 2.0 * (w - s.wini), s2 = 2.0 * ((double)q.uZ[n2] - s.uini);
+        const double sr = sqrt(s1 * s1 + s2 * s2);
+        const double cdelta = 2.0 * rr * s.Sn * a;
+        double uw = asinh(exp(q.psiZ[n2] / a) * sr / (2.0 * s.v0));
+        const int e1 = g.at2(i + 1, k), e2 = g.at2(i, k + 1), e3 = g.at2(i + 1, k + 1);
+        const double rfx = ((double)q.RFx[n2] + (double)q.RFx[e1] + (double)q.RFx[e2] + (double)q.RFx[e3]) / 4.0;
+        const double t0x = ((double)q.T0X[n2] + (double)q.T0X[e1] + (double)q.T0X[e2] + (double)q.T0X[e3]) / 4.0;
+        const double q1 = w + 2.0 * rr * ((double)q.RFz[n2] - (double)q.T0Z[n2]);
+        const double q2 = (double)q.uZ[n2] + 2.0 * rr * (rfx - t0x);
+        const double vt = -sqrt(q1 * q1 + q2 * q2);
+        uw = fvw_newton(vt, cdelta, uw, q.psiZ[n2], a, s.v0, status);
+        f.w[pf] = (T)(((double)q.tz[n2] + (double)q.T0Z[n2]) * (-sinh(uw) * s.v0 * exp(-q.psiZ[n2] / a)) /
+                      (double)q.tabsZ[n2] + s.wini);
+    }
+}
+
+struct PmlDesc {
+    Strip s[4];
+    long long cum[5];  // cumulative thread counts (u/w range) over the strips
+};
+
+template <class T>
+struct PmlAux {
+    T* a[AX_N];         // each pool covers all 4 strips (Strip::base offsets)
+    const T* prof;      // damping profiles
+};
+
+// locate strip and (i,j,k) of compact thread index t (u/w loop range of every strip)
+__device__ __forceinline__ bool pml_locate(const PmlDesc& D, long long t, int& s, int& i, int& j, int& k,
+                                           long long& qa) {
+    if (t >= D.cum[4]) return false;
+    s = (t >= D.cum[1]) + (t >= D.cum[2]) + (t >= D.cum[3]);
+    const Strip& S = D.s[s];
+    long long r = t - D.cum[s];
+    const int nj = S.jend_uw - S.nyb + 1;
+    const int i2 = (int)(r % S.ni); r /= S.ni;
+    const int j2 = (int)(r % nj);
+    const int k2 = (int)(r / nj);
+    i = S.nxb + i2; j = S.nyb + j2; k = S.nzb + k2;
+    qa = S.base + i2 + (long long)S.ni * (j2 + (long long)S.nj1 * k2);
+    return true;
+}
+
+// pml_uvw: split-field PML velocity in the 4 strips (fd3d_deriv.f90:1927-2218)
+template <class T>
+__global__ void __launch_bounds__(256) k_vel_pml(Grid g, Fields<T> f, PmlDesc D, PmlAux<T> X, StepConst<T> c) {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    int s, i, j, k;
+    long long qa;
+    if (!pml_locate(D, t, s, i, j, k, qa)) return;
+    const Strip& S = D.s[s];
+    const int i2 = i - S.nxb, j2 = j - S.nyb, k2 = k - S.nzb;
+    const T ox = X.prof[S.ox_off + i2], oxS = X.prof[S.oxS_off + i2];
+    const T oy = X.prof[S.oy_off + j2], oz = X.prof[S.oz_off + k2];
+    const long long p = g.at(i, j, k), sy = g.px, sz = g.plane;
+    const T d = f.d[p], dt = c.dt, dh = c.dh;
+    T pt, a0, a1, a2;
+    a0 = X.a[AX_U0][qa]; a1 = X.a[AX_U1][qa]; a2 = X.a[AX_U2][qa];
+    pt = (a0 * ((T)1 - ox) + (dt / d) * (f.xx[p] - f.xx[p - 1]) / dh);        a0 = pt / ((T)1 + ox);
+    pt = (a1 * ((T)1 - oy) + (dt / d) * (f.xy[p] - f.xy[p - sy]) / dh);       a1 = pt / ((T)1 + oy);
+    pt = (a2 * ((T)1 - oz) + (dt / d) * (f.xz[p] - f.xz[p - sz]) / dh);       a2 = pt / ((T)1 + oz);
+    X.a[AX_U0][qa] = a0; X.a[AX_U1][qa] = a1; X.a[AX_U2][qa] = a2;
+    f.u[p] = a0 + a1 + a2;
+    if (j <= S.nye) {
+        if (j == g.nyt - 1) f.v[p + sy] = f.v[p];  // bnd2d mirror of the value before this update
+        a0 = X.a[AX_V0][qa]; a1 = X.a[AX_V1][qa]; a2 = X.a[AX_V2][qa];
+        pt = a0 * ((T)1 - oxS) + (dt / d) * (f.xy[p + 1] - f.xy[p]) / dh;     a0 = pt / ((T)1 + oxS);
+        pt = a1 * ((T)1 - oy) + (dt / d) * (f.yy[p + sy] - f.yy[p]) / dh;     a1 = pt / ((T)1 + oy);
+        pt = a2 * ((T)1 - oz) + (dt / d) * (f.yz[p] - f.yz[p - sz]) / dh;     a2 = pt / ((T)1 + oz);
+        X.a[AX_V0][qa] = a0; X.a[AX_V1][qa] = a1; X.a[AX_V2][qa] = a2;
+        f.v[p] = a0 + a1 + a2;
+    }
+    a0 = X.a[AX_W0][qa]; a1 = X.a[AX_W1][qa]; a2 = X.a[AX_W2][qa];
+    pt = a0 * ((T)1 - oxS) + (dt / d) * (f.xz[p + 1] - f.xz[p]) / dh;         a0 = pt / ((T)1 + oxS);
+    pt = a1 * ((T)1 - oy) + (dt / d) * (f.yz[p] - f.yz[p - sy]) / dh;         a1 = pt / ((T)1 + oy);
+    pt = a2 * ((T)1 - oz) + (dt / d) * (f.zz[p + sz] - f.zz[p]) / dh;         a2 = pt / ((T)1 + oz);
+    X.a[AX_W0][qa] = a0; X.a[AX_W1][qa] = a1; X.a[AX_W2][qa] = a2;
+    f.w[p] = a0 + a1 + a2;
+}
+
+// fuvw at the ghost row k=ks+1 (fd3d_deriv.f90:1018-1062).  w needs u and v of the
+// ghost row at (i+1,j) and (i,j-1); they are recomputed with the same formula
+// (identical operands and order), so no second launch is needed.
+template <class T>
+__global__ void k_vel_fs(Grid g, Fields<T> f) {
+    const int i = 1 + blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = 1 + blockIdx.y * blockDim.y + threadIdx.y;
+    if (i > g.nxt || j > g.nyt) return;
+    const int n = g.ks();
+    const long long sy = g.px, sz = g.plane;
+    auto ug = [&](int ii, int jj) -> T {  // loop 1: j=1..nyt, i=2..nxt-1
+        const long long p = g.at(ii, jj, n);
+        return f.u[p] - (f.w[p] - f.w[p - 1]);
+    };
+    auto vg = [&](int ii, int jj) -> T {  // loop 2: j=2..nyt-1, i=2..nxt-1; else existing value
+        const long long p = g.at(ii, jj, n);
+        if (jj >= 2 && jj <= g.nyt - 1 && ii >= 2 && ii <= g.nxt - 1) return f.v[p] - (f.w[p + sy] - f.w[p]);
+        return f.v[p + sz];
+    };
+    T un = (T)0, vn = (T)0, wn = (T)0;
+    const bool du = (i >= 2 && i <= g.nxt - 1);
+    const bool dv = (j >= 2 && j <= g.nyt - 1 && du);
+    const bool dw = (j >= 2 && i >= 2 && i <= g.nxt - 2);
+    if (du) un = ug(i, j);
+    if (dv) vn = vg(i, j);
+    if (dw) {
+        const long long p = g.at(i, j, n);
+        const T xl = f.lam[p + sz], xm = f.mu[p + sz];
+        const T a = (T)2 * xl, b = xl + (T)2 * xm;
+        const T u_i1 = ug(i + 1, j);
+        const T u_i = du ? un : f.u[p + sz];
+        const T v_j = vg(i, j);
+        const T v_jm = vg(i, j - 1);
+        wn = +(f.w[p - sz] - (a / b) * (f.u[p + 1] - f.u[p] + u_i1 - u_i + f.v[p] - f.v[p - sy] + v_j - v_jm));
+    }
+    // The ghost-row values read above (v at j=1 and j=nyt) are never written by this
+    // launch, so the writes below cannot race with them.
+    const long long pg = g.at(i, j, n + 1);
+    if (du) f.u[pg] = un;
+    if (dv) f.v[pg] = vn;
+    if (dw) f.w[pg] = wn;
+}
+
+// ---------------------------------------------------------------- stress
+template <class T>
+__global__ void __launch_bounds__(256) k_str_interior(Grid g, Fields<T> f, StepConst<T> c, int kchunk) {
+    const int i = g.nabc + 1 + blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = g.nabc + 1 + blockIdx.y * blockDim.y + threadIdx.y;
+    if (i > g.nxt - g.nabc || j > g.nyt - 2) return;
+    const int kb = g.nabc + 1 + blockIdx.z * kchunk;
+    const int ke = min(kb + kchunk - 1, g.ks());
+    const long long sy = g.px, sz = g.plane;
+    const T c1 = c.c1, c2 = c.c2, dth = c.dth;
+    const T* __restrict__ u = f.u; const T* __restrict__ v = f.v; const T* __restrict__ w = f.w;
+    const T* __restrict__ mu = f.mu;
+    for (int k = kb; k <= ke; ++k) {
+        const long long p = g.at(i, j, k);
+        const T xl = f.lam[p], xm = mu[p];
+        const T a = xl + (T)2 * xm, b = xl;
+        const T dxu1 = c1 * (u[p + 1] - u[p]), dxu2 = c2 * (u[p + 2] - u[p - 1]);
+        const T dyv1 = c1 * (v[p] - v[p - sy]), dyv2 = c2 * (v[p + sy] - v[p - 2 * sy]);
+        const T dzw1 = c1 * (w[p] - w[p - sz]), dzw2 = c2 * (w[p + sz] - w[p - 2 * sz]);
+        f.xx[p] = f.xx[p] + dth * a * (dxu1 + dxu2) + dth * b * (dyv1 + dyv2 + dzw1 + dzw2);
+        f.yy[p] = f.yy[p] + dth * a * (dyv1 + dyv2) + dth * b * (dxu1 + dxu2 + dzw1 + dzw2);
+        f.zz[p] = f.zz[p] + dth * a * (dzw1 + dzw2) + dth * b * (dxu1 + dxu2 + dyv1 + dyv2);
+        T xmu = (T)0.5 * (xm + mu[p + sy]);
+        f.xy[p] = f.xy[p] + dth * xmu * (c1 * (u[p + sy] - u[p]) + c2 * (u[p + 2 * sy] - u[p - sy]) +
+                                         c1 * (v[p] - v[p - 1]) + c2 * (v[p + 1] - v[p - 2]));
+        xmu = (T)0.5 * (xm + mu[p + sz]);
+        f.xz[p] = f.xz[p] + dth * xmu * (c1 * (u[p + sz] - u[p]) + c2 * (u[p + 2 * sz] - u[p - sz]) +
+                                         c1 * (w[p] - w[p - 1]) + c2 * (w[p + 1] - w[p - 2]));
+        xmu = (T)0.5 * (xm + mu[p + 1 + sy + sz]);
+        f.yz[p] = f.yz[p] + dth * xmu * (c1 * (v[p + sz] - v[p]) + c2 * (v[p + 2 * sz] - v[p - sz]) +
+                                         c1 * (w[p + sy] - w[p]) + c2 * (w[p + 2 * sy] - w[p - sy]));
+    }
+}
+
+// Band j=nyt-1 stresses (2nd order) + xy/yz mirror; sxz1 and tasii at j=nyt.
+template <class T>
+__global__ void k_str_fault(Grid g, Fields<T> f, Fault<T> q, StepConst<T> c) {
+    const int i = g.nabc + 1 + blockIdx.x * blockDim.x + threadIdx.x;
+    const int k = g.nabc + 1 + blockIdx.y * blockDim.y + threadIdx.y;
+    if (i > g.nxt - g.nabc || k > g.ks()) return;
+    const long long sy = g.px, sz = g.plane;
+    const T dth = c.dth, dth2 = c.dth2, c1 = c.c1, c2 = c.c2;
+    {   // sxx, sxy0, sxz0, syz0 at j=nyt-1 (fd3d_deriv.f90:818-1012)
+        const long long p = g.at(i, g.nyt - 1, k);
+        const T xl = f.lam[p], xm = f.mu[p];
+        const T a = xl + (T)2 * xm, b = xl;
+        const T up = f.u[p], vp = f.v[p], wp = f.w[p];
+        const T ux = f.u[p + 1], vy = f.v[p - sy], wz = f.w[p - sz];
+        f.xx[p] = f.xx[p] + dth * a * (ux - up) + dth * b * (vp - vy + wp - wz);
+        f.yy[p] = f.yy[p] + dth * a * (vp - vy) + dth * b * (ux - up + wp - wz);
+        f.zz[p] = f.zz[p] + dth * a * (wp - wz) + dth * b * (ux - up + vp - vy);
+        T xmu = xm + f.mu[p + sy];
+        const T xyn = f.xy[p] + dth2 * xmu * (f.u[p + sy] - up + vp - f.v[p - 1]);
+        f.xy[p] = xyn; f.xy[p + sy] = xyn;
+        xmu = xm + f.mu[p + sz];
+        f.xz[p] = f.xz[p] + dth2 * xmu * (f.u[p + sz] - up + wp - f.w[p - 1]);
+        xmu = xm + f.mu[p + 1 + sy + sz];
+        const T yzn = f.yz[p] + dth2 * xmu * (f.v[p + sz] - vp + f.w[p + sy] - wp);
+        f.yz[p] = yzn; f.yz[p + sy] = yzn;
+    }
+    {   // sxz1 (tasxz) and tasii at j=nyt (fd3d_deriv.f90:677-722, 1263-1314)
+        const long long p = g.at(i, g.nyt, k);
+        const T* u = f.u; const T* w = f.w;
+        T xmu = f.mu[p] + f.mu[p + sz];
+        f.xz[p] = f.xz[p] + dth2 * xmu * (c1 * (u[p + sz] - u[p]) + c2 * (u[p + 2 * sz] - u[p - sz]) +
+                                          c1 * (w[p] - w[p - 1]) + c2 * (w[p + 1] - w[p - 2]));
+        const T xl = f.lam[p], xm = f.mu[p];
+        const T a = xl + (T)2 * xm, b = xl;
+        const T diff1 = c1 * (u[p + 1] - u[p]) + c2 * (u[p + 2] - u[p - 1]);
+        const T diff3 = c1 * (w[p] - w[p - sz]) + c2 * (w[p + sz] - w[p - 2 * sz]);
+        const T vb = f.v[p - sy];
+        const T v1t = vb - b * (diff1 + diff3) / ((T)2 * a);
+        q.v1t[g.at2(i, k)] = v1t;
+        const T dv = v1t - vb;
+        f.xx[p] = f.xx[p] + dth * a * (diff1) + dth * b * ((T)2 * dv + diff3);
+        f.yy[p] = f.yy[p] + dth * a * (T)2 * dv + dth * b * (diff1 + diff3);
+        f.zz[p] = f.zz[p] + dth * a * (diff3) + dth * b * (diff1 + (T)2 * dv);
+    }
+}
+
+// pml_xyz in the 4 strips (fd3d_deriv.f90:2304-2992)
+template <class T>
+__global__ void __launch_bounds__(256) k_str_pml(Grid g, Fields<T> f, PmlDesc D, PmlAux<T> X, StepConst<T> c) {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    int s, i, j, k;
+    long long qa;
+    if (!pml_locate(D, t, s, i, j, k, qa)) return;
+    const Strip& S = D.s[s];
+    const int i2 = i - S.nxb, j2 = j - S.nyb, k2 = k - S.nzb;
+    const T ox = X.prof[S.ox_off + i2], oxS = X.prof[S.oxS_off + i2];
+    const T oy = X.prof[S.oy_off + j2], oyS = X.prof[S.oyS_off + j2];
+    const T oz = X.prof[S.oz_off + k2], ozS = X.prof[S.ozS_off + k2];
+    const T oyxy = (s >= 2) ? oyS : oy;  // xy, yz: omegayS in strips 3,4
+    const T ozxz = (s == 3) ? ozS : oz;  // xz, yz: omegazS in strip 4
+    const bool top = (s <= 2) && (k == S.nze);  // xz/yz aux zeroed at the top row, strips 1-3
+    const long long p = g.at(i, j, k), sy = g.px, sz = g.plane;
+    const T dt = c.dt, dh = c.dh;
+    const T xl = f.lam[p], xm = f.mu[p];
+    const T a = xl + (T)2 * xm, b = xl;
+    const T diff1 = f.u[p + 1] - f.u[p];
+    const T diff2 = f.v[p] - f.v[p - sy];
+    const T diff3 = f.w[p] - f.w[p - sz];
+    T pt, a0, a1, a2;
+    a0 = X.a[AX_XX0][qa]; a1 = X.a[AX_XX1][qa]; a2 = X.a[AX_XX2][qa];
+    pt = a0 * ((T)1 - oxS) + dt * a * diff1 / dh; a0 = pt / ((T)1 + oxS);
+    pt = a1 * ((T)1 - oy) + dt * b * diff2 / dh;  a1 = pt / ((T)1 + oy);
+    pt = a2 * ((T)1 - oz) + dt * b * diff3 / dh;  a2 = pt / ((T)1 + oz);
+    X.a[AX_XX0][qa] = a0; X.a[AX_XX1][qa] = a1; X.a[AX_XX2][qa] = a2;
+    f.xx[p] = a0 + a1 + a2;
+    a0 = X.a[AX_YY0][qa]; a1 = X.a[AX_YY1][qa]; a2 = X.a[AX_YY2][qa];
+    pt = a0 * ((T)1 - oxS) + dt * b * diff1 / dh; a0 = pt / ((T)1 + oxS);
+    pt = a1 * ((T)1 - oy) + dt * a * diff2 / dh;  a1 = pt / ((T)1 + oy);
+    pt = a2 * ((T)1 - oz) + dt * b * diff3 / dh;  a2 = pt / ((T)1 + oz);
+    X.a[AX_YY0][qa] = a0; X.a[AX_YY1][qa] = a1; X.a[AX_YY2][qa] = a2;
+    f.yy[p] = a0 + a1 + a2;
+    a0 = X.a[AX_ZZ0][qa]; a1 = X.a[AX_ZZ1][qa]; a2 = X.a[AX_ZZ2][qa];
+    pt = a0 * ((T)1 - oxS) + dt * b * diff1 / dh; a0 = pt / ((T)1 + oxS);
+    pt = a1 * ((T)1 - oy) + dt * b * diff2 / dh;  a1 = pt / ((T)1 + oy);
+    pt = a2 * ((T)1 - oz) + dt * a * diff3 / dh;  a2 = pt / ((T)1 + oz);
+    X.a[AX_ZZ0][qa] = a0; X.a[AX_ZZ1][qa] = a1; X.a[AX_ZZ2][qa] = a2;
+    f.zz[p] = a0 + a1 + a2;
+    {   // xz (j up to jend_uw)
+        const T xmu = (xm + f.mu[p + sz]) / (T)2;
+        a0 = X.a[AX_XZ0][qa]; a1 = X.a[AX_XZ1][qa];
+        pt = a0 * ((T)1 - ozxz) + dt * xmu * (f.u[p + sz] - f.u[p]) / dh; a0 = pt / ((T)1 + ozxz);
+        pt = a1 * ((T)1 - ox) + dt * xmu * (f.w[p] - f.w[p - 1]) / dh;    a1 = pt / ((T)1 + ox);
+        f.xz[p] = a0 + a1;
+        if (top) { a0 = (T)0; a1 = (T)0; }
+        X.a[AX_XZ0][qa] = a0; X.a[AX_XZ1][qa] = a1;
+    }
+    if (j <= S.nye) {
+        if (j == g.nyt - 1) { f.xy[p + sy] = f.xy[p]; f.yz[p + sy] = f.yz[p]; }  // strbnd mirror
+        T xmu = (xm + f.mu[p + sy]) / (T)2;
+        a0 = X.a[AX_XY0][qa]; a1 = X.a[AX_XY1][qa];
+        pt = a0 * ((T)1 - oyxy) + dt * xmu * (f.u[p + sy] - f.u[p]) / dh; a0 = pt / ((T)1 + oyxy);
+        pt = a1 * ((T)1 - ox) + dt * xmu * (f.v[p] - f.v[p - 1]) / dh;    a1 = pt / ((T)1 + ox);
+        X.a[AX_XY0][qa] = a0; X.a[AX_XY1][qa] = a1;
+        f.xy[p] = a0 + a1;
+        xmu = (xm + f.mu[p + 1 + sy + sz]) / (T)2;
+        a0 = X.a[AX_YZ0][qa]; a1 = X.a[AX_YZ1][qa];
+        pt = a0 * ((T)1 - ozxz) + dt * xmu * (f.v[p + sz] - f.v[p]) / dh; a0 = pt / ((T)1 + ozxz);
+        pt = a1 * ((T)1 - oyxy) + dt * xmu * (f.w[p + sy] - f.w[p]) / dh; a1 = pt / ((T)1 + oyxy);
+        f.yz[p] = a0 + a1;
+        if (top) { a0 = (T)0; a1 = (T)0; }
+        X.a[AX_YZ0][qa] = a0; X.a[AX_YZ1][qa] = a1;
+    }
+}
+
+// fres (fd3d_deriv.f90:1067-1104)
+template <class T>
+__global__ void k_str_fs(Grid g, Fields<T> f) {
+    const int i = 1 + blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = 1 + blockIdx.y * blockDim.y + threadIdx.y;
+    if (i > g.nxt || j > g.nyt) return;
+    const long long p = g.at(i, j, g.ks()), sz = g.plane;
+    f.zz[p + sz] = -f.zz[p];
+    f.zz[p + 2 * sz] = -f.zz[p - sz];
+    f.xz[p + sz] = -f.xz[p - sz];
+    f.xz[p + 2 * sz] = -f.xz[p - 2 * sz];
+    f.yz[p + sz] = -f.yz[p - sz];
+    f.yz[p + 2 * sz] = -f.yz[p - 2 * sz];
+    f.xz[p] = (T)0;
+    f.yz[p] = (T)0;
+}
+
+// ---------------------------------------------------------------- fault BC
+// trial traction, damping, RF (fd3d_theo.f90:233-308, non-FSPACE)
+template <class T>
+__global__ void k_traction(Grid g, Fields<T> f, Fault<T> q, StepConst<T> c) {
+    const int i = g.nabc + 1 + blockIdx.x * blockDim.x + threadIdx.x;
+    const int k = g.nabc + 1 + blockIdx.y * blockDim.y + threadIdx.y;
+    const int ks = g.ks();
+    if (i > g.nxt - g.nabc || k > ks) return;
+    const long long sy = g.px, sz = g.plane;
+    const long long p = g.at(i, g.nyt, k);
+    const int n2 = g.at2(i, k);
+    const T c1 = c.c1, c2 = c.c2, dht = c.dht, ds = c.damp_s;
+    const T* xx = f.xx; const T* xz = f.xz; const T* zz = f.zz;
+    T pdz;
+    if (k < ks)
+        pdz = (c1 * (xz[p + 1] - xz[p]) + c2 * (xz[p + 2] - xz[p - 1])) / (T)2 +
+              (c1 * (zz[p + sz] - zz[p]) + c2 * (zz[p + 2 * sz] - zz[p - sz])) / (T)2 - f.yz[p - sy];
+    else
+        pdz = ((xz[p + 1 - sz] - xz[p - sz]) / ((T)2 * (T)4) + (zz[p + sz] - zz[p]) / ((T)2 * (T)2) -
+               f.yz[p - sy - sz] / (T)4);
+    T av = ds * (pdz - q.avdz[n2]);
+    T rf = pdz + av;
+    q.RFz[n2] = rf;
+    T tzv;
+    if (k < ks) tzv = -rf - (T)0.5 * f.d[p] * dht * f.w[p];
+    else        tzv = -rf - (T)0.5 * f.d[p] * dht * f.w[p] / (T)2;
+    q.tzt[n2] = tzv;
+    q.avdz[n2] = pdz;
+    const T pdx = (c1 * (xx[p] - xx[p - 1]) + c2 * (xx[p + 1] - xx[p - 2])) / (T)2 +
+                  (c1 * (xz[p] - xz[p - sz]) + c2 * (xz[p + sz] - xz[p - 2 * sz])) / (T)2 - f.xy[p - sy];
+    av = ds * (pdx - q.avdx[n2]);
+    rf = pdx + av;
+    q.RFx[n2] = rf;
+    const T txv = -rf - (T)0.5 * f.d[p] * dht * f.u[p];
+    q.txt[n2] = txv;
+    q.avdx[n2] = pdx;
+    // ghost row nzt-1 (fd3d_theo.f90:304-307); with nfs=2: nzt-1 = ks+1, nzt-2 = ks, nzt-3 = ks-1
+    if (k == ks) q.txt[g.at2(i, ks + 1)] = +txv;
+    if (k == ks - 1) q.tzt[g.at2(i, ks + 1)] = -tzv;
+}
+
+// |T| at staggered nodes, friction law, slip, rupture time (fd3d_theo.f90:313-410)
+template <class T>
+__global__ void k_friction(Grid g, Fields<T> f, Fault<T> q, StepConst<T> c, int law, FvwScalars s,
+                           const int* it_dev) {
+    const int i = g.nabc + 1 + blockIdx.x * blockDim.x + threadIdx.x;
+    const int k = g.nabc + 1 + blockIdx.y * blockDim.y + threadIdx.y;
+    if (i > g.nxt - g.nabc || k > g.ks()) return;
+    const double time = (double)(*it_dev) * c.dtA;
+    const double dtA = c.dtA, rup = 1.e-3;
+    const long long sy = g.px, sz = g.plane;
+    (void)sy;
+    const int n2 = g.at2(i, k);
+    const int e1 = g.at2(i + 1, k), e2 = g.at2(i, k + 1), e3 = g.at2(i + 1, k + 1);
+    const int w1i = g.at2(i - 1, k), w2i = g.at2(i, k - 1), w3i = g.at2(i - 1, k - 1);
+    const T* txt = q.txt; const T* tzt = q.tzt; const T* T0X = q.T0X; const T* T0Z = q.T0Z;
+    T tint = (txt[n2] + T0X[n2] + txt[e1] + T0X[e1] + txt[e2] + T0X[e2] + txt[e3] + T0X[e3]) / (T)4;
+    const T szv = tzt[n2] + T0Z[n2];
+    const T tabsZ = sqrt(tint * tint + szv * szv);
+    tint = (tzt[n2] + T0Z[n2] + tzt[w1i] + T0Z[w1i] + tzt[w2i] + T0Z[w2i] + tzt[w3i] + T0Z[w3i]) / (T)4;
+    const T sxv = txt[n2] + T0X[n2];
+    const T tabsX = sqrt(sxv * sxv + tint * tint);
+    q.tabsZ[n2] = tabsZ;
+    q.tabsX[n2] = tabsX;
+    const long long p = g.at(i, g.nyt, k);
+    const T U = f.u[p], W = f.w[p];
+    // Z nodes (fd3d_theo.f90:326-373)
+    {
+        const T uZ = (U + f.u[p + 1] + f.u[p + sz] + f.u[p + 1 + sz]) / (T)4;
+        q.uZ[n2] = uZ;
+        const T u1out = -sqrt(W * W + uZ * uZ);
+        T tzn = tzt[n2];
+        if (law == 1) {
+            const double a = (double)q.aZ[n2];
+            const double s1 = 2.0 * (fabs((double)W) + fabs(s.wini)), s2 = 2.0 * (fabs((double)uZ) + fabs(s.uini));
+            const double sr = sqrt(s1 * s1 + s2 * s2);
+            const double flv = s.f0 - ((double)q.bZ[n2] - a) * log(sr / s.v0);
+            const double fw = (double)q.fwZ[n2];
+            const double fss = fw + (flv - fw) / pow(1.0 + pow(sr / (double)q.vwZ[n2], 8.0), 1.0 / 8.0);
+            const double psiss = a * (log(sinh(fss / a)) + log(2.0 * s.v0 / sr));
+            const double psi = (q.psiZ[n2] - psiss) * exp(-sr * dtA / (double)q.Dc[n2]) + psiss;
+            q.psiZ[n2] = psi;
+            const double fric = s.Sn * a * asinh(sr * exp(psi / a) / (2.0 * s.v0));
+            q.distZ[n2] = q.distZ[n2] - 2.0 * (double)u1out * dtA;
+            q.schangeZ[n2] = (T)fric;
+            if (fabs(2.0 * (double)u1out) > rup) {
+                if (q.ruptime[n2] != 1.e4) q.rise[n2] = time;
+                if (q.ruptime[n2] == 1.e4) q.ruptime[n2] = time;
+            }
+        } else {
+            const double dz = q.distZ[n2], dcz = (double)q.DcZ[n2];
+            double fric;
+            if (dz <= dcz) fric = (double)q.peakZ[n2] * (1.0 - dz / dcz) + (double)q.dynZ[n2] * dz / dcz + (double)q.coh[n2];
+            else           fric = (double)q.dynZ[n2] + (double)q.coh[n2];
+            if ((double)tabsZ >= fric) {
+                q.distZ[n2] = dz - 2.0 * (double)u1out * dtA;
+                tzn = (T)(((double)tzn + (double)T0Z[n2]) * fric / (double)tabsZ - (double)T0Z[n2]);
+                if (-2.0 * (double)u1out > rup) {
+                    if (q.ruptime[n2] != 1.e4) q.rise[n2] = time;
+                    if (q.ruptime[n2] == 1.e4) q.ruptime[n2] = time;
+                }
+            }
+        }
+        q.tz[n2] = tzn;
+        q.slipZ[n2] = q.slipZ[n2] - 2.0 * (double)W * dtA;
+        q.slipX[n2] = q.slipX[n2] - 2.0 * (double)uZ * dtA;
+        if (q.sliptime[n2] == 1.e4 && q.distZ[n2] > (double)q.Dc[n2]) q.sliptime[n2] = time;
+    }
+    // X nodes (fd3d_theo.f90:375-410)
+    {
+        const T wX = (W + f.w[p - 1] + f.w[p - sz] + f.w[p - 1 - sz]) / (T)4;
+        q.wX[n2] = wX;
+        const T u1out = -sqrt(wX * wX + U * U);
+        T txn = txt[n2];
+        if (law == 1) {
+            const double a = (double)q.aX[n2];
+            const double s1 = 2.0 * (fabs((double)wX) + fabs(s.wini)), s2 = 2.0 * (fabs((double)U) + fabs(s.uini));
+            const double sr = sqrt(s1 * s1 + s2 * s2);
+            const double flv = s.f0 - ((double)q.bX[n2] - a) * log(sr / s.v0);
+            const double fw = (double)q.fwX[n2];
+            const double fss = fw + (flv - fw) / pow(1.0 + pow(sr / (double)q.vwX[n2], 8.0), 1.0 / 8.0);
+            const double psiss = a * (log(sinh(fss / a)) + log(2.0 * s.v0 / sr));
+            const double psi = (q.psiX[n2] - psiss) * exp(-sr * dtA / (double)q.Dc[n2]) + psiss;
+            q.psiX[n2] = psi;
+            const double fric = s.Sn * a * asinh(sr * exp(psi / a) / (2.0 * s.v0));
+            q.distX[n2] = q.distX[n2] - 2.0 * (double)u1out * dtA;
+            q.schangeX[n2] = (T)fric;
+        } else {
+            const double dx = q.distX[n2], dcx = (double)q.DcX[n2];
+            double fric;
+            if (dx <= (double)q.Dc[n2]) fric = (double)q.peakX[n2] * (1.0 - dx / dcx) + (double)q.dynX[n2] * dx / dcx + (double)q.coh[n2];
+            else                        fric = (double)q.dynX[n2] + (double)q.coh[n2];
+            if ((double)tabsX >= fric) {
+                q.distX[n2] = dx - 2.0 * (double)u1out * dtA;
+                txn = (T)(((double)txn + (double)T0X[n2]) * fric / (double)tabsX - (double)T0X[n2]);
+            }
+        }
+        q.tx[n2] = txn;
+    }
+}
+
+struct HistDesc {
+    void* ring;         // [cap][nf][nzT][nxT] of T
+    int cap, stride, nf;
+    int nst;
+    int sta[3 * 10];    // station (i,j,k)
+    void* seis;         // [cap][nst*3] of T
+};
+
+// output planes, stations, history ring (fd3d_theo.f90:413-467); non-finite check
+template <class T>
+__global__ void k_output(Grid g, Fields<T> f, Fault<T> q, int law, const int* it_dev, HistDesc h, int* status) {
+    const int ii = blockIdx.x * blockDim.x + threadIdx.x;
+    const int kk = blockIdx.y * blockDim.y + threadIdx.y;
+    const int it = *it_dev;
+    const bool rec = (it % h.stride) == 0;
+    const long long slot = (long long)((it / h.stride - 1) % h.cap);
+    const int nxT = g.nxt - 2 * g.nabc, nzT = g.ks() - g.nabc;
+    if (rec && ii < h.nst && kk == 0) {
+        const long long p = g.at(h.sta[3 * ii], h.sta[3 * ii + 1], h.sta[3 * ii + 2]);
+        T* sp = (T*)h.seis + slot * (3 * h.nst) + 3 * ii;
+        sp[0] = f.u[p]; sp[1] = f.v[p]; sp[2] = f.w[p];
+    }
+    if (ii >= nxT || kk >= nzT) return;
+    const int i = g.nabc + 1 + ii, k = g.nabc + 1 + kk;
+    const bool top = (k == g.ks());
+    const long long p = g.at(i, g.nyt, k), sz = g.plane;
+    const int n2 = g.at2(i, k), e1 = g.at2(i + 1, k), e2 = g.at2(i, k + 1), e3 = g.at2(i + 1, k + 1);
+    const T U = f.u[p], U2 = f.u[p + 1], W = f.w[p];
+    T srx, srz, scx, scz;
+    srz = (T)-2 * W;
+    if (!top) {
+        const T U3 = f.u[p + sz], U4 = f.u[p + 1 + sz];
+        srx = ((T)-2 * U - (T)2 * U2 - (T)2 * U3 - (T)2 * U4) / (T)4;
+        if (law == 0) {
+            scz = q.tz[n2] + q.T0Z[n2];
+            scx = (q.tx[n2] + q.T0X[n2] + q.tx[e1] + q.T0X[e1] + q.tx[e2] + q.T0X[e2] + q.tx[e3] + q.T0X[e3]) / (T)4;
+        }
+    } else {
+        if (law == 1) {
+            srx = ((T)-2 * U - (T)2 * U2) / (T)4;
+        } else {
+            scz = q.tz[n2] + q.T0Z[n2];
+            scx = (q.tx[n2] + q.T0X[n2] + q.tx[e1] + q.T0X[e1]) / (T)2;
+            srx = ((T)-2 * U - (T)2 * U2) / (T)2;
+        }
+    }
+    if (law == 1) { scx = q.schangeX[n2]; scz = q.schangeZ[n2]; }
+    else { q.schangeX[n2] = scx; q.schangeZ[n2] = scz; }
+    if (!(isfinite((double)srx) && isfinite((double)srz) && isfinite((double)scx) && isfinite((double)scz)))
+        atomicOr(status, ST_NONFINITE);
+    if (rec) {
+        const long long plane = (long long)nxT * nzT;
+        T* r = (T*)h.ring + slot * h.nf * plane + (long long)kk * nxT + ii;
+        r[0] = srx;
+        r[plane] = srz;
+        r[2 * plane] = scx;
+        r[3 * plane] = scz;
+        if (h.nf > 4) r[4 * plane] = (T)q.psiZ[n2];
+    }
+}
+
+// TPV103/104 smooth nucleation of T0X (fd3d_theo.f90:487-542)
+template <class T>
+__global__ void k_nucleation(Grid g, Fault<T> q, StepConst<T> c, FvwScalars s, const int* it_dev) {
+    const int i = g.nabc - 1 + blockIdx.x * blockDim.x + threadIdx.x;
+    const int k = g.nabc - 1 + blockIdx.y * blockDim.y + threadIdx.y;
+    if (i > g.nxt - g.nabc || k > g.ks()) return;
+    const double time = (double)(*it_dev) * c.dtA;
+    const double th = time - c.dtA / 2.0;
+    if (!(th <= s.TT2)) return;
+    const double GT = (th < s.TT2) ? exp((th - s.TT2) * (th - s.TT2) / (th * (th - 2.0 * s.TT2))) : 1.0;
+    const double hx = (double)i * c.dhA, hz = (double)k * c.dhA;
+    const double rr = (hx - s.hx0) * (hx - s.hx0) + (hz - s.hz0) * (hz - s.hz0);
+    const double FXZ = (rr < s.RR2 - c.dhA) ? exp(rr / (rr - s.RR2 - c.dhA)) : 0.0;
+    const double base = s.nucleation == 2 ? (double)q.T0Xb[g.at2(i, k)] : s.strinixI;
+    q.T0X[g.at2(i, k)] = (T)(base + s.perturb * FXZ * GT);
+}
+
+}  // namespace fd3d

@@ -1,0 +1,156 @@
+// fd3d_opt.cuh -- tiled interior sweeps (the bulk of every time step).
+//
+// One CTA owns a 32 x 8 (x,y) column of the interior box and marches a chunk of z.
+// Per z-plane the CTA stages the x/y neighbourhood of the fields it differentiates
+// in shared memory (one coalesced load per element, halos included) and keeps the
+// z-neighbours of its own column in a 4-deep register queue, so each field element
+// is read from HBM once per sweep.  The arithmetic and its order are those of
+// k_vel_interior / k_str_interior (uxx1/vyy1/wzz1 and dstres of fd3d_deriv.f90).
+#pragma once
+#include "fd3d_common.cuh"
+
+namespace fd3d {
+
+constexpr int TX = 32, TY = 8, NT = TX * TY;
+
+// load an (H x W) window starting at (i0-ox, j0-oy) of plane k into s (row stride W)
+template <class T, int H, int W>
+__device__ __forceinline__ void stage(T* __restrict__ s, const T* __restrict__ a, const Grid& g, int i0, int j0,
+                                      int ox, int oy, int k, int tid) {
+    const long long base = g.at(1, 1, k);
+#pragma unroll
+    for (int e = tid; e < H * W; e += NT) {
+        const int r = e / W, cc = e - r * W;
+        const int gi = i0 - ox + cc, gj = j0 - oy + r;
+        T v = (T)0;
+        if (gi <= g.nxt && gj <= g.nyt) v = a[base + (gi - 1) + (long long)g.px * (gj - 1)];
+        s[e] = v;
+    }
+}
+
+template <class T>
+__global__ void __launch_bounds__(NT) k_vel_interior_tiled(Grid g, Fields<T> f, StepConst<T> c, int kchunk) {
+    __shared__ T s_xx[TY][36];
+    __shared__ T s_xy[TY + 3][36];
+    __shared__ T s_yy[TY + 3][TX];
+    __shared__ T s_xz[TY][36];
+    __shared__ T s_yz[TY + 3][TX];
+    const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
+    const int i0 = g.nabc + 1 + blockIdx.x * TX, j0 = g.nabc + 1 + blockIdx.y * TY;
+    const int i = i0 + tx, j = j0 + ty;
+    const bool act = (i <= g.nxt - g.nabc) && (j <= g.nyt - 2);
+    const int kb = g.nabc + 1 + blockIdx.z * kchunk;
+    const int ke = min(kb + kchunk - 1, g.ks());
+    const int ic = min(i, g.nxt), jc = min(j, g.nyt);
+    const long long sz = g.plane;
+    const long long pc = g.at(ic, jc, kb);
+    const T* __restrict__ zz = f.zz; const T* __restrict__ xz = f.xz; const T* __restrict__ yz = f.yz;
+    // z queues of the own column: zz(k-1..k+2), xz(k-2..k+1), yz(k-2..k+1)
+    T zq0, zq1 = zz[pc - sz], zq2 = zz[pc], zq3 = zz[pc + sz];
+    T xq0, xq1 = xz[pc - 2 * sz], xq2 = xz[pc - sz], xq3 = xz[pc];
+    T yq0, yq1 = yz[pc - 2 * sz], yq2 = yz[pc - sz], yq3 = yz[pc];
+    const T c1 = c.c1, c2 = c.c2, dth = c.dth;
+    for (int k = kb; k <= ke; ++k) {
+        const long long pk = pc + (long long)(k - kb) * sz;
+        __syncthreads();
+        stage<T, TY, 36>(&s_xx[0][0], f.xx, g, i0, j0, 2, 0, k, tid);
+        stage<T, TY + 3, 36>(&s_xy[0][0], f.xy, g, i0, j0, 1, 2, k, tid);
+        stage<T, TY + 3, TX>(&s_yy[0][0], f.yy, g, i0, j0, 0, 1, k, tid);
+        stage<T, TY, 36>(&s_xz[0][0], f.xz, g, i0, j0, 1, 0, k, tid);
+        stage<T, TY + 3, TX>(&s_yz[0][0], f.yz, g, i0, j0, 0, 2, k, tid);
+        zq0 = zq1; zq1 = zq2; zq2 = zq3; zq3 = zz[pk + 2 * sz];
+        xq0 = xq1; xq1 = xq2; xq2 = xq3; xq3 = xz[pk + sz];
+        yq0 = yq1; yq1 = yq2; yq2 = yq3; yq3 = yz[pk + sz];
+        __syncthreads();
+        if (!act) continue;
+        const T r = dth / f.d[pk];
+        f.u[pk] = f.u[pk] + r * (c1 * (s_xx[ty][tx + 2] - s_xx[ty][tx + 1]) + c2 * (s_xx[ty][tx + 3] - s_xx[ty][tx]) +
+                                 c1 * (s_xy[ty + 2][tx + 1] - s_xy[ty + 1][tx + 1]) + c2 * (s_xy[ty + 3][tx + 1] - s_xy[ty][tx + 1]) +
+                                 c1 * (xq2 - xq1) + c2 * (xq3 - xq0));
+        f.v[pk] = f.v[pk] + r * (c1 * (s_xy[ty + 2][tx + 2] - s_xy[ty + 2][tx + 1]) + c2 * (s_xy[ty + 2][tx + 3] - s_xy[ty + 2][tx]) +
+                                 c1 * (s_yy[ty + 2][tx] - s_yy[ty + 1][tx]) + c2 * (s_yy[ty + 3][tx] - s_yy[ty][tx]) +
+                                 c1 * (yq2 - yq1) + c2 * (yq3 - yq0));
+        f.w[pk] = f.w[pk] + r * (c1 * (s_xz[ty][tx + 2] - s_xz[ty][tx + 1]) + c2 * (s_xz[ty][tx + 3] - s_xz[ty][tx]) +
+                                 c1 * (s_yz[ty + 2][tx] - s_yz[ty + 1][tx]) + c2 * (s_yz[ty + 3][tx] - s_yz[ty][tx]) +
+                                 c1 * (zq2 - zq1) + c2 * (zq3 - zq0));
+    }
+}
+
+template <class T>
+__global__ void __launch_bounds__(NT) k_str_interior_tiled(Grid g, Fields<T> f, StepConst<T> c, int kchunk) {
+    // u, v, w of plane k with a 2-cell halo on every side: rows j0-2..j0+9, cols i0-2..i0+33
+    __shared__ T s_u[TY + 4][36];
+    __shared__ T s_v[TY + 4][36];
+    __shared__ T s_w[TY + 4][36];
+    const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
+    const int i0 = g.nabc + 1 + blockIdx.x * TX, j0 = g.nabc + 1 + blockIdx.y * TY;
+    const int i = i0 + tx, j = j0 + ty;
+    const bool act = (i <= g.nxt - g.nabc) && (j <= g.nyt - 2);
+    const int kb = g.nabc + 1 + blockIdx.z * kchunk;
+    const int ke = min(kb + kchunk - 1, g.ks());
+    const int ic = min(i, g.nxt), jc = min(j, g.nyt);
+    const long long sy = g.px, sz = g.plane;
+    const long long pc = g.at(ic, jc, kb);
+    const T* __restrict__ u = f.u; const T* __restrict__ v = f.v; const T* __restrict__ w = f.w;
+    const T* __restrict__ mu = f.mu;
+    // z queues: u(k-1..k+2), v(k-1..k+2), w(k-2..k+1), mu(k..k+1)
+    T uq0, uq1 = u[pc - sz], uq2 = u[pc], uq3 = u[pc + sz];
+    T vq0, vq1 = v[pc - sz], vq2 = v[pc], vq3 = v[pc + sz];
+    T wq0, wq1 = w[pc - 2 * sz], wq2 = w[pc - sz], wq3 = w[pc];
+    T mq0, mq1 = mu[pc];
+    const T c1 = c.c1, c2 = c.c2, dth = c.dth;
+    const int X = tx + 2, Y = ty + 2;
+    for (int k = kb; k <= ke; ++k) {
+        const long long pk = pc + (long long)(k - kb) * sz;
+        __syncthreads();
+        stage<T, TY + 4, 36>(&s_u[0][0], u, g, i0, j0, 2, 2, k, tid);
+        stage<T, TY + 4, 36>(&s_v[0][0], v, g, i0, j0, 2, 2, k, tid);
+        stage<T, TY + 4, 36>(&s_w[0][0], w, g, i0, j0, 2, 2, k, tid);
+        uq0 = uq1; uq1 = uq2; uq2 = uq3; uq3 = u[pk + 2 * sz];
+        vq0 = vq1; vq1 = vq2; vq2 = vq3; vq3 = v[pk + 2 * sz];
+        wq0 = wq1; wq1 = wq2; wq2 = wq3; wq3 = w[pk + sz];
+        mq0 = mq1; mq1 = mu[pk + sz];
+        __syncthreads();
+        if (!act) continue;
+        const T xl = f.lam[pk], xm = mq0;
+        const T a = xl + (T)2 * xm, b = xl;
+        const T dxu1 = c1 * (s_u[Y][X + 1] - s_u[Y][X]), dxu2 = c2 * (s_u[Y][X + 2] - s_u[Y][X - 1]);
+        const T dyv1 = c1 * (s_v[Y][X] - s_v[Y - 1][X]), dyv2 = c2 * (s_v[Y + 1][X] - s_v[Y - 2][X]);
+        const T dzw1 = c1 * (wq2 - wq1), dzw2 = c2 * (wq3 - wq0);
+        f.xx[pk] = f.xx[pk] + dth * a * (dxu1 + dxu2) + dth * b * (dyv1 + dyv2 + dzw1 + dzw2);
+        f.yy[pk] = f.yy[pk] + dth * a * (dyv1 + dyv2) + dth * b * (dxu1 + dxu2 + dzw1 + dzw2);
+        f.zz[pk] = f.zz[pk] + dth * a * (dzw1 + dzw2) + dth * b * (dxu1 + dxu2 + dyv1 + dyv2);
+        T xmu = (T)0.5 * (xm + mu[pk + sy]);
+        f.xy[pk] = f.xy[pk] + dth * xmu * (c1 * (s_u[Y + 1][X] - s_u[Y][X]) + c2 * (s_u[Y + 2][X] - s_u[Y - 1][X]) +
+                                           c1 * (s_v[Y][X] - s_v[Y][X - 1]) + c2 * (s_v[Y][X + 1] - s_v[Y][X - 2]));
+        xmu = (T)0.5 * (xm + mq1);
+        f.xz[pk] = f.xz[pk] + dth * xmu * (c1 * (uq2 - uq1) + c2 * (uq3 - uq0) +
+                                           c1 * (s_w[Y][X] - s_w[Y][X - 1]) + c2 * (s_w[Y][X + 1] - s_w[Y][X - 2]));
+        xmu = (T)0.5 * (xm + mu[pk + 1 + sy + sz]);
+        f.yz[pk] = f.yz[pk] + dth * xmu * (c1 * (vq2 - vq1) + c2 * (vq3 - vq0) +
+                                           c1 * (s_w[Y + 1][X] - s_w[Y][X]) + c2 * (s_w[Y + 2][X] - s_w[Y - 1][X]));
+    }
+}
+
+inline int interior_kchunk(const Grid& g) {
+    const int nz = g.ks() - g.nabc;
+    return nz > 96 ? 64 : nz;
+}
+
+template <class T>
+void launch_vel_interior_opt(const Grid& g, const Fields<T>& f, const StepConst<T>& c, cudaStream_t st) {
+    const int nxT = g.nxt - 2 * g.nabc, nyI = g.nyt - 2 - g.nabc, nzT = g.ks() - g.nabc;
+    const int kch = interior_kchunk(g);
+    dim3 grid((nxT + TX - 1) / TX, (nyI + TY - 1) / TY, (nzT + kch - 1) / kch);
+    k_vel_interior_tiled<T><<<grid, dim3(TX, TY), 0, st>>>(g, f, c, kch);
+}
+
+template <class T>
+void launch_str_interior_opt(const Grid& g, const Fields<T>& f, const StepConst<T>& c, cudaStream_t st) {
+    const int nxT = g.nxt - 2 * g.nabc, nyI = g.nyt - 2 - g.nabc, nzT = g.ks() - g.nabc;
+    const int kch = interior_kchunk(g);
+    dim3 grid((nxT + TX - 1) / TX, (nyI + TY - 1) / TY, (nzT + kch - 1) / kch);
+    k_str_interior_tiled<T><<<grid, dim3(TX, TY), 0, st>>>(g, f, c, kch);
+}
+
+}  // namespace fd3d

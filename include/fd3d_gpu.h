@@ -1,0 +1,193 @@
+/*
+ * fd3d_gpu.h -- C ABI of the B200 (sm_100a) time-stepping path of FD3D_TSN.
+ *
+ * The reference exposes its hot path as the argument-less Fortran subroutine
+ * fd3d() (src/fd3d_theo.f90:22), which reads every input from module globals
+ * (src/fd3d_init.f90:15-121), runs the time loop (src/fd3d_theo.f90:187-602)
+ * and writes the result files under result/.  This header replaces that seam
+ * with an explicit context:
+ *
+ *     fd3d_ctx_create      <- fd3d_init() sizes + init_pml()      (fd3d_init.f90:126-208, fd3d_deriv.f90:1319-1493)
+ *     fd3d_upload_medium   <- readcrustalmodel() output lam1,mu1,d1 (fd3d_init.f90:211-279)
+ *     fd3d_upload_fault    <- forwardspecialTPV5/TPV104 or inversion_modeltofd3d output + interp_fric (fd3d_deriv.f90:3150-3190)
+ *     fd3d_run / fd3d_sync <- the time loop body                   (fd3d_theo.f90:187-602)
+ *     fd3d_fetch_history   <- the per-step WRITE(24..28) planes      (fd3d_theo.f90:546-553)
+ *     fd3d_fetch_stations  <- the per-step station lines            (fd3d_theo.f90:456-467,555-557)
+ *     fd3d_fetch_final     <- ruptime,rise,slipX/Z,sliptime after the loop (fd3d_theo.f90:604-658)
+ *     fd3d_write_results   <- the files under result/ (.res)                (fd3d_theo.f90:133-145,546-558,687-749)
+ *
+ * Conventions
+ *  - Every function returns an int status: FD3D_OK (0) or a negative FD3D_ERR_*.
+ *    No function calls exit(); the reference's `stop` on CFL (fd3d_init.f90:274-278)
+ *    becomes FD3D_ERR_CFL, its printed 'newton error?' (fd3d_deriv.f90:1157-1160)
+ *    becomes FD3D_ERR_NEWTON from fd3d_sync().
+ *  - Arrays cross the boundary in the reference's own layout: Fortran column-major,
+ *    x (i) fastest, 1-based index (i,j,k) at offset (i-1) + nxt*((j-1) + nyt*(k-1));
+ *    fault-plane arrays (i,k) at (i-1) + nxt*(k-1).  Host arrays are borrowed for
+ *    the duration of the call only.
+ *  - real_kind selects the host element type of a buffer: 4 (float) or 8 (double),
+ *    as the reference's `real` is 4 bytes by default and 8 bytes with -r8.
+ *  - One context is driven by one host thread at a time.  Device memory is owned by
+ *    the context.  Work is enqueued on the context's own CUDA stream.
+ */
+#ifndef FD3D_GPU_H
+#define FD3D_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---------------------------------------------------- */
+#define FD3D_OK              0
+#define FD3D_ERR_ARG        -1   /* bad argument or size                          */
+#define FD3D_ERR_CFL        -2   /* vp_max*dt/dh > 0.25 (fd3d_init.f90:274-278)    */
+#define FD3D_ERR_CUDA       -3   /* a CUDA runtime call failed                    */
+#define FD3D_ERR_NOMEM      -4   /* request exceeds device memory / HBM budget    */
+#define FD3D_ERR_NEWTON     -5   /* FVW Newton solve hit its iteration cap        */
+#define FD3D_ERR_NONFINITE  -6   /* NaN/Inf found on the fault plane              */
+#define FD3D_ERR_STATE      -7   /* call out of order (e.g. run before upload)    */
+#define FD3D_ERR_IO         -8   /* input or result file could not be read/written */
+#define FD3D_ERR_NODEV      -9   /* no CUDA device / library built without one    */
+#define FD3D_ERR_BUSY      -10   /* batch/serving object has no free slot         */
+
+/* ---- friction law (compile-time -DFVW switch of the reference) -------- */
+#define FD3D_LAW_SW   0   /* linear slip weakening (reference default)   */
+#define FD3D_LAW_FVW  1   /* fast-velocity-weakening rate and state      */
+
+/* ---- arithmetic of the wave field ------------------------------------ */
+#define FD3D_PREC_F32 0   /* FP32 fields and PML; FP64 slip, slip path, rupture time, psi, Newton */
+#define FD3D_PREC_F64 1   /* everything FP64: the reference built with -r8 */
+
+/* ---- history planes (unformatted stream files of the reference) ------ */
+#define FD3D_HIST_SLIPRATE_X    0   /* result/sliprateX.res    */
+#define FD3D_HIST_SLIPRATE_Z    1   /* result/sliprateZ.res    */
+#define FD3D_HIST_SHEARSTRESS_X 2   /* result/shearstressX.res */
+#define FD3D_HIST_SHEARSTRESS_Z 3   /* result/shearstressZ.res */
+#define FD3D_HIST_PSI           4   /* result/psi.res (FVW)    */
+#define FD3D_HIST_NFIELDS       5
+
+/* ---- wave-field / state selectors for fd3d_fetch_field ---------------- */
+#define FD3D_FIELD_U   0
+#define FD3D_FIELD_V   1
+#define FD3D_FIELD_W   2
+#define FD3D_FIELD_XX  3
+#define FD3D_FIELD_YY  4
+#define FD3D_FIELD_ZZ  5
+#define FD3D_FIELD_XY  6
+#define FD3D_FIELD_YZ  7
+#define FD3D_FIELD_XZ  8
+
+/* fault-plane (nxt,nzt) arrays for fd3d_fetch_plane */
+#define FD3D_PLANE_TX        0
+#define FD3D_PLANE_TZ        1
+#define FD3D_PLANE_SLIPX     2
+#define FD3D_PLANE_SLIPZ     3
+#define FD3D_PLANE_RUPTIME   4
+#define FD3D_PLANE_RISE      5   /* last time above threshold (before rise-=ruptime) */
+#define FD3D_PLANE_SLIPTIME  6
+#define FD3D_PLANE_DISTX     7
+#define FD3D_PLANE_DISTZ     8
+#define FD3D_PLANE_PSIX      9
+#define FD3D_PLANE_PSIZ     10
+#define FD3D_PLANE_T0X      11
+#define FD3D_PLANE_T0Z      12
+#define FD3D_PLANE_SCHANGEX 13
+#define FD3D_PLANE_SCHANGEZ 14
+#define FD3D_PLANE_NPLANES  15
+
+#define FD3D_MAX_STATIONS 10  /* units 31..40 of the reference (fd3d_theo.f90:117-128) */
+
+/*
+ * Grid and run parameters: the contents of inputfd3d.dat (fd3d_init.f90:145-173)
+ * after padding.  nxt = nxtT + 2*nabc, nyt = nytT + nabc, nzt = nztT + nabc + nfs,
+ * fault plane at j = nyt (nysc = nyt).
+ */
+typedef struct fd3d_params {
+    int    nxt, nyt, nzt;      /* padded grid                                     */
+    int    nabc;               /* PML thickness (cells)                           */
+    int    nfs;                /* rows above the free surface (2; FSPACE is not built) */
+    int    ntfd;               /* number of time steps of a full solve            */
+    double dh, dt;             /* grid step [m], time step [s]                    */
+    double damp_s;             /* damping near the fault                          */
+    double pml_vp, pml_fact;   /* omegaM_pml = pml_fact*pml_vp/(2*dh*(nabc-1))    */
+    double vp_max;             /* for the CFL check; <=0 skips it                 */
+    int    law;                /* FD3D_LAW_SW | FD3D_LAW_FVW                      */
+    int    precision;          /* FD3D_PREC_F32 | FD3D_PREC_F64                   */
+    int    nstations;          /* 0..FD3D_MAX_STATIONS                            */
+    int    staX[FD3D_MAX_STATIONS], staY[FD3D_MAX_STATIONS], staZ[FD3D_MAX_STATIONS]; /* 1-based */
+    int    history_stride;     /* keep history planes every n-th step (>=1)       */
+    int    history_capacity;   /* device ring capacity in records (0 = default)   */
+} fd3d_params;
+
+/*
+ * Fault parameters on the (nxt,nzt) plane, Fortran order, double precision.
+ * SW uses striniX/Z, peak_xz, dyn_xz, Dc, coh; interp_fric is applied inside
+ * the library (X-node values are 4-point averages, fd3d_deriv.f90:3174-3189).
+ * FVW uses striniX/Z, Dc, a, b, psi, vw (Z nodes) and aX, bX, psiX, vwX (X nodes
+ * come straight from the setup, fd3d_init.f90:471-499), plus the scalars.
+ * fwZ/fwX are optional per-node weakened friction coefficients (an extension:
+ * the reference has one scalar fw, fd3d_init.f90:61); NULL means use fw.
+ */
+typedef struct fd3d_fault {
+    const double *striniX, *striniZ, *Dc;
+    const double *peak_xz, *dyn_xz, *coh;                 /* SW  */
+    const double *a, *b, *psi, *vw;                       /* FVW, Z nodes */
+    const double *aX, *bX, *psiX, *vwX;                   /* FVW, X nodes */
+    const double *fwZ, *fwX;                              /* FVW, optional */
+    double Sn, v0, f0, fw, uini, wini;                    /* FVW scalars  */
+    int    nucleation;   /* 0 off; 1 TPV103/104 ramp T0X = strinixI + bump (fd3d_theo.f90:487-542);
+                            2 the same bump added to each node's initial T0X (an extension that
+                            equals 1 when striniX is uniform, as in the TPV104 deck) */
+    double hx0, hz0, perturb, RR2, TT2, strinixI;         /* fd3d_theo.f90:487-542  */
+} fd3d_fault;
+
+typedef struct fd3d_ctx fd3d_ctx;
+
+/* library info */
+const char* fd3d_version(void);
+const char* fd3d_status_string(int status);
+int fd3d_device_count(int* count);
+/* device used by contexts created afterwards on the calling host thread */
+int fd3d_set_device(int device);
+
+/* single model */
+int fd3d_ctx_create(const fd3d_params* p, fd3d_ctx** out);
+int fd3d_ctx_destroy(fd3d_ctx* ctx);
+int fd3d_upload_medium(fd3d_ctx* ctx, const void* lam1, const void* mu1, const void* d1, int real_kind);
+/* 1-D layered medium as built by readcrustalmodel (fd3d_init.f90:241-265): one value per k */
+int fd3d_upload_medium_layers(fd3d_ctx* ctx, const double* lam_k, const double* mu_k, const double* d_k);
+int fd3d_upload_fault(fd3d_ctx* ctx, const fd3d_fault* f);
+int fd3d_reset(fd3d_ctx* ctx);                      /* zero wave field, PML and fault state (fd3d_theo.f90:59-88) */
+int fd3d_run(fd3d_ctx* ctx, int nsteps);            /* enqueue nsteps time steps; asynchronous */
+int fd3d_sync(fd3d_ctx* ctx);                       /* wait; returns first device error        */
+int fd3d_steps_done(fd3d_ctx* ctx, int* it);
+int fd3d_fetch_history(fd3d_ctx* ctx, int field, int rec0, int nrec, void* host, int real_kind);
+int fd3d_history_records(fd3d_ctx* ctx, int* nrec);  /* records held in the device ring */
+int fd3d_fetch_stations(fd3d_ctx* ctx, int rec0, int nrec, double* host /* nrec*nst*3 */);
+int fd3d_fetch_field(fd3d_ctx* ctx, int field, void* host, int real_kind);     /* (nxt,nyt,nzt) */
+int fd3d_fetch_plane(fd3d_ctx* ctx, int plane, double* host);                  /* (nxt,nzt)     */
+int fd3d_fetch_final(fd3d_ctx* ctx, double* slipX, double* slipZ, double* ruptime,
+                     double* rise, double* sliptime);
+int fd3d_write_results(fd3d_ctx* ctx, const char* dir, int real_kind);
+/* host-visible timing of the last fd3d_run span, CUDA events on the ctx stream */
+int fd3d_last_run_ms(fd3d_ctx* ctx, float* ms);
+/* per-kernel timing over the last run when profiling is switched on */
+int fd3d_set_profiling(fd3d_ctx* ctx, int on);
+int fd3d_kernel_times(fd3d_ctx* ctx, float* ms /* FD3D_NKERNELS */, int* launches);
+#define FD3D_NKERNELS 8
+/* kernel ids in fd3d_kernel_times: 0 vel_interior, 1 vel_fault, 2 vel_pml, 3 vel_fs,
+   4 str_interior, 5 str_fault, 6 str_pml, 7 fault_bc (traction+friction+output) */
+
+/* ---- input decks (the reference's own files) --------------------------- */
+/* Reads inputfd3d.dat and crustal.dat from dir (fd3d_init.f90:145-173, 211-279),
+ * fills p and returns lam1/mu1/d1 (caller frees with fd3d_free). */
+int fd3d_read_deck(const char* dir, fd3d_params* p, double** lam1, double** mu1, double** d1);
+void fd3d_free(void* p);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FD3D_GPU_H */

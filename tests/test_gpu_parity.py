@@ -1,0 +1,195 @@
+"""GPU parity: the CUDA path (through the C ABI) against the CPU oracle.
+
+* FP32 build vs the oracle's FP32-field/FP64-accumulator variant and FP64 build vs
+  the oracle's FP64 variant: same operations in the same order, so slip-weakening
+  runs agree to the last bit; FVW runs (CUDA vs libm transcendentals) agree within
+  1e-5 (FP32) / 1e-9 (FP64) relative L2.
+* FP32 build vs the FP64 oracle at the stated accuracy: relative L2 <= 1e-3 on the
+  slip-rate and traction histories, final slip <= 1e-4 (relative L2), rupture time
+  within 2*dt.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from fd3d_tsn_b200 import configs
+from fd3d_tsn_b200.abi import Fd3dError
+from fd3d_tsn_b200.solver import Solver
+from oracle.oracle import F64, MIXED, Oracle
+
+pytestmark = pytest.mark.gpu
+
+
+def rel_l2(a, b):
+    a = np.asarray(a, dtype=np.float64)
+    b = np.asarray(b, dtype=np.float64)
+    nb = np.linalg.norm(b)
+    return np.linalg.norm(a - b) / (nb if nb > 0 else 1.0)
+
+
+def run_both(model, nsteps, variant):
+    o = Oracle(model, variant)
+    oh, os_ = o.step(nsteps)
+    s = Solver(model)
+    s.run(nsteps)
+    s.sync()
+    gh = np.stack([s.history(f) for f in range(s.nf)], axis=1)
+    gs = s.stations()
+    return o, oh, os_, s, gh, gs
+
+
+@pytest.fixture(scope="module")
+def sw32():
+    m = configs.tiny_sw(nsteps=90)
+    return (m,) + run_both(m, 90, MIXED)
+
+
+def test_sw_f32_history_bitwise(sw32):
+    m, o, oh, os_, s, gh, gs = sw32
+    assert gh.shape == (90, 4, s.nzT, s.nxT)
+    assert np.abs(oh[:, 0]).max() > 0.1, "the tiny model must rupture"
+    for f in range(4):
+        np.testing.assert_array_equal(gh[:, f], oh[:, f], err_msg=f"history field {f}")
+    np.testing.assert_array_equal(gs, os_)
+
+
+def test_sw_f32_state_bitwise(sw32):
+    m, o, oh, os_, s, gh, gs = sw32
+    for name in ("u", "v", "w", "xx", "yy", "zz", "xy", "yz", "xz"):
+        np.testing.assert_array_equal(s.field(name), o.field(name), err_msg=name)
+    for name in ("tx", "tz", "slipX", "slipZ", "ruptime", "rise", "sliptime", "distX", "distZ"):
+        np.testing.assert_array_equal(s.plane(name), o.plane(name), err_msg=name)
+
+
+def test_sw_f64_bitwise():
+    m = configs.tiny_sw(nsteps=60, precision="f64")
+    o, oh, os_, s, gh, gs = run_both(m, 60, F64)
+    for f in range(4):
+        np.testing.assert_array_equal(gh[:, f], oh[:, f], err_msg=f"history field {f}")
+    for name in ("u", "w", "xx", "xz"):
+        np.testing.assert_array_equal(s.field(name), o.field(name), err_msg=name)
+
+
+@pytest.mark.parametrize("prec,variant,tol", [("f32", MIXED, 1e-5), ("f64", F64, 1e-9)])
+def test_fvw_matches_oracle(prec, variant, tol):
+    m = configs.tiny_fvw(nsteps=60, precision=prec)
+    o, oh, os_, s, gh, gs = run_both(m, 60, variant)
+    assert np.abs(oh[:, 0]).max() > 1e-3, "the nucleation must start slip"
+    for f in range(5):
+        assert rel_l2(gh[:, f], oh[:, f]) <= tol, (f, rel_l2(gh[:, f], oh[:, f]))
+    for name in ("psiX", "psiZ", "slipX", "slipZ"):
+        assert rel_l2(s.plane(name), o.plane(name)) <= tol, name
+
+
+def test_f32_vs_f64_oracle_accuracy():
+    """The production FP32 build against the FP64 oracle at the stated tolerances."""
+    m = configs.tiny_sw(nsteps=150, nxT=48, nzT=32)
+    o = Oracle(m, F64)
+    oh, _ = o.step(150)
+    s = Solver(m)
+    s.run(150)
+    s.sync()
+    for f in range(4):
+        assert rel_l2(s.history(f), oh[:, f]) <= 1e-3, f
+    fo, fg = o.final(), s.final()
+    assert rel_l2(fg["slipX"], fo["slipX"]) <= 1e-4
+    assert rel_l2(fg["slipZ"], fo["slipZ"]) <= 1e-4 or np.abs(fo["slipZ"]).max() < 1e-6
+    ruptured = fo["ruptime"] < 1e4
+    assert ruptured.sum() > 50
+    assert np.all((fg["ruptime"] < 1e4) == ruptured)
+    assert np.abs(fg["ruptime"][ruptured] - fo["ruptime"][ruptured]).max() <= 2 * m["dt"]
+
+
+def test_odd_sizes_and_partial_tiles():
+    m = configs.tiny_sw(nxT=37, nyT=11, nzT=23, nsteps=40)
+    o, oh, os_, s, gh, gs = run_both(m, 40, MIXED)
+    for f in range(4):
+        np.testing.assert_array_equal(gh[:, f], oh[:, f])
+
+
+def test_graph_chunks_equal_single_steps():
+    m = configs.tiny_sw(nsteps=40)
+    a = Solver(m)
+    a.run(40)   # two 16-step graphs + 8 eager steps
+    a.sync()
+    b = Solver(m)
+    for _ in range(40):
+        b.run(1)
+    b.sync()
+    np.testing.assert_array_equal(a.history(0), b.history(0))
+    np.testing.assert_array_equal(a.field("xz"), b.field("xz"))
+
+
+def test_reset_reproduces():
+    m = configs.tiny_fvw(nsteps=30)
+    s = Solver(m)
+    s.run(30)
+    s.sync()
+    h1 = s.history(0)
+    s.reset()
+    s.run(30)
+    s.sync()
+    np.testing.assert_array_equal(s.history(0), h1)
+
+
+def test_tiled_interior_equals_per_point_kernels():
+    m = configs.tiny_sw(nxT=70, nyT=20, nzT=36, nsteps=30)
+    a = Solver(m)
+    os.environ["FD3D_NAIVE_INTERIOR"] = "1"
+    try:
+        b = Solver(m)
+    finally:
+        del os.environ["FD3D_NAIVE_INTERIOR"]
+    for s in (a, b):
+        s.run(30)
+        s.sync()
+    for name in ("u", "v", "w", "xx", "yy", "zz", "xy", "yz", "xz"):
+        np.testing.assert_array_equal(a.field(name), b.field(name), err_msg=name)
+
+
+def test_history_stride_and_ring():
+    m = configs.tiny_sw(nsteps=40, stride=4)
+    m["history_capacity"] = 4
+    s = Solver(m)
+    s.run(40)
+    s.sync()
+    assert s.history_records() == 10
+    o = Oracle(m, MIXED)
+    oh, _ = o.step(40)
+    last = s.history(0, rec0=6, nrec=4)          # the ring keeps the last 4 records
+    np.testing.assert_array_equal(last, oh[[27, 31, 35, 39], 0])
+    with pytest.raises(Fd3dError):
+        s.history(0, rec0=0, nrec=1)             # overwritten
+
+
+def test_nonfinite_input_is_reported():
+    m = configs.tiny_sw(nsteps=10)
+    m["fault"]["striniX"] = m["fault"]["striniX"].copy()
+    m["fault"]["striniX"][25, 20] = np.nan
+    s = Solver(m)
+    s.run(10)
+    with pytest.raises(Fd3dError) as e:
+        s.sync()
+    assert "NONFINITE" in str(e.value)
+
+
+def test_write_results_files(tmp_path):
+    m = configs.tiny_sw(nsteps=20)
+    s = Solver(m)
+    s.run(12)
+    s.sync()
+    s.write_results(str(tmp_path), 4)
+    s.run(8)
+    s.sync()
+    s.write_results(str(tmp_path), 4)
+    raw = np.fromfile(tmp_path / "sliprateX.res", dtype=np.float32)
+    assert raw.size == 20 * s.nxT * s.nzT
+    np.testing.assert_array_equal(raw.reshape(20, s.nzT, s.nxT), s.history(0).astype(np.float32))
+    st = np.loadtxt(tmp_path / "stan0.txt")
+    assert st.shape == (20, 3)
+    np.testing.assert_allclose(st, s.stations()[:, 0], rtol=1e-14, atol=0)
+    rt = np.loadtxt(tmp_path / "ruptime.res")
+    assert rt.size == s.nxT * s.nzT
+    fin = s.final()["ruptime"][m["nabc"]:m["nxt"] - m["nabc"], m["nabc"]:m["nzt"] - m["nfs"]]
+    np.testing.assert_allclose(rt, fin.ravel(order="F"), rtol=1e-14)
