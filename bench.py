@@ -130,6 +130,8 @@ def workload(name):
         return configs.sw_large()
     if name == "sw_small":
         return configs.sw_small()
+    if name == "sw_mid":   # 400x200x200 cells: larger than L2, small enough for ncu captures
+        return configs.sw_model(400, 200, 200, 100.0, 1.0, 4, patch_nodes=(300, 150), ntfd=1000)
     if name == "fvw_medium":
         return configs.fvw_medium()
     raise SystemExit(f"unknown workload {name}")

@@ -151,7 +151,7 @@ struct CtxBase {
     int klaunch[FD3D_NKERNELS] = {0};
     cudaGraphExec_t gexec = nullptr;
     int gsteps = 0;
-    int opt = 1;            // use the tiled interior kernels
+    InteriorCfg icfg;       // interior sweep variant and CTA shape
     virtual ~CtxBase() {}
     virtual int alloc() = 0;
     virtual int upload_medium(const void*, const void*, const void*, int) = 0;
@@ -425,16 +425,11 @@ struct Ctx : CtxBase {
 
     int enqueue_step() override {
         const int nxT = p.nxt - 2 * p.nabc;
-        const int nyI = p.nyt - 2 - p.nabc;
         const int nzT = g.ks() - p.nabc;
         const dim3 b2(32, 8);
         // velocity half-step
         kbeg(0);
-        if (opt) launch_vel_interior_opt<T>(g, f, c, st);
-        else {
-            const int kch = 4;
-            k_vel_interior<T><<<dim3((nxT + 31) / 32, (nyI + 7) / 8, (nzT + kch - 1) / kch), b2, 0, st>>>(g, f, c, kch);
-        }
+        launch_vel_interior<T>(icfg, g, f, c, st);
         kend(0);
         kbeg(1);
         k_vel_fault<T><<<dim3((std::max(nxT, p.nxt) + 31) / 32, (nzT + 7) / 8), b2, 0, st>>>(g, f, q, c, law, fs, it_dev, status);
@@ -448,11 +443,7 @@ struct Ctx : CtxBase {
         kend(3);
         // stress half-step
         kbeg(4);
-        if (opt) launch_str_interior_opt<T>(g, f, c, st);
-        else {
-            const int kch = 4;
-            k_str_interior<T><<<dim3((nxT + 31) / 32, (nyI + 7) / 8, (nzT + kch - 1) / kch), b2, 0, st>>>(g, f, c, kch);
-        }
+        launch_str_interior<T>(icfg, g, f, c, st);
         kend(4);
         kbeg(5);
         k_str_fault<T><<<dim3((nxT + 31) / 32, (nzT + 7) / 8), b2, 0, st>>>(g, f, q, c);
@@ -583,8 +574,15 @@ int fd3d_ctx_create(const fd3d_params* p, fd3d_ctx** out) {
     if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) { cudaGetLastError(); return FD3D_ERR_NODEV; }
     CtxBase* c = (p->precision == FD3D_PREC_F64) ? (CtxBase*)new Ctx<double>() : (CtxBase*)new Ctx<float>();
     c->p = *p;
-    const char* e = std::getenv("FD3D_NAIVE_INTERIOR");
-    if (e && e[0] == '1') c->opt = 0;
+    // manual override of the interior sweep variant: FD3D_INTERIOR=point|tiled|pipe,
+    // FD3D_KCHUNK=<planes per CTA>, FD3D_BY=<CTA rows of the point kernel>
+    if (const char* e = std::getenv("FD3D_INTERIOR")) {
+        if (!std::strcmp(e, "point")) c->icfg.variant = IV_POINT;
+        else if (!std::strcmp(e, "tiled")) c->icfg.variant = IV_TILED;
+        else if (!std::strcmp(e, "pipe")) c->icfg.variant = IV_PIPE;
+    }
+    if (const char* e = std::getenv("FD3D_KCHUNK")) c->icfg.kchunk = std::max(1, std::atoi(e));
+    if (const char* e = std::getenv("FD3D_BY")) c->icfg.by = std::min(32, std::max(1, std::atoi(e)));
     rc = c->alloc();
     if (rc) {
         delete c;

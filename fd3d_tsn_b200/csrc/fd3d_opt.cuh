@@ -7,7 +7,9 @@
 // is read from HBM once per sweep.  The arithmetic and its order are those of
 // k_vel_interior / k_str_interior (uxx1/vyy1/wzz1 and dstres of fd3d_deriv.f90).
 #pragma once
+#include <algorithm>
 #include "fd3d_common.cuh"
+#include "fd3d_kernels.cuh"
 
 namespace fd3d {
 
@@ -132,25 +134,213 @@ __global__ void __launch_bounds__(NT) k_str_interior_tiled(Grid g, Fields<T> f, 
     }
 }
 
-inline int interior_kchunk(const Grid& g) {
-    const int nz = g.ks() - g.nabc;
-    return nz > 96 ? 64 : nz;
+// Per-thread share of an (H x W) staging window: elements tid, tid+NT, ...  Loads go to
+// registers first so that plane k+1 is in flight while plane k is computed.
+template <class T, int H, int W>
+struct Prefetch {
+    static constexpr int N = (H * W + NT - 1) / NT;
+    T r[N];
+    __device__ __forceinline__ void load(const T* __restrict__ a, const Grid& g, int i0, int j0, int ox, int oy,
+                                         int k, int tid) {
+        const long long base = g.at(1, 1, k);
+#pragma unroll
+        for (int n = 0; n < N; ++n) {
+            const int e = tid + n * NT;
+            T v = (T)0;
+            if (e < H * W) {
+                const int rr = e / W, cc = e - rr * W;
+                const int gi = i0 - ox + cc, gj = j0 - oy + rr;
+                if (gi <= g.nxt && gj <= g.nyt) v = a[base + (gi - 1) + (long long)g.px * (gj - 1)];
+            }
+            r[n] = v;
+        }
+    }
+    __device__ __forceinline__ void store(T* s, int tid) const {
+#pragma unroll
+        for (int n = 0; n < N; ++n) {
+            const int e = tid + n * NT;
+            if (e < H * W) s[e] = r[n];
+        }
+    }
+};
+
+// Velocity sweep, software-pipelined: the staged windows, the z-queue fronts and the
+// own-point operands of plane k+1 are loaded while plane k is computed.
+template <class T>
+__global__ void __launch_bounds__(NT) k_vel_interior_pipe(Grid g, Fields<T> f, StepConst<T> c, int kchunk) {
+    __shared__ T s_xx[TY][36];
+    __shared__ T s_xy[TY + 3][36];
+    __shared__ T s_yy[TY + 3][TX];
+    __shared__ T s_xz[TY][36];
+    __shared__ T s_yz[TY + 3][TX];
+    const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
+    const int i0 = g.nabc + 1 + blockIdx.x * TX, j0 = g.nabc + 1 + blockIdx.y * TY;
+    const int i = i0 + tx, j = j0 + ty;
+    const bool act = (i <= g.nxt - g.nabc) && (j <= g.nyt - 2);
+    const int kb = g.nabc + 1 + blockIdx.z * kchunk;
+    const int ke = min(kb + kchunk - 1, g.ks());
+    const int ic = min(i, g.nxt), jc = min(j, g.nyt);
+    const long long sz = g.plane;
+    const long long pc = g.at(ic, jc, kb);
+    const T* __restrict__ zz = f.zz; const T* __restrict__ xz = f.xz; const T* __restrict__ yz = f.yz;
+    Prefetch<T, TY, 36> pxx; Prefetch<T, TY + 3, 36> pxy; Prefetch<T, TY + 3, TX> pyy;
+    Prefetch<T, TY, 36> pxz; Prefetch<T, TY + 3, TX> pyz;
+    pxx.load(f.xx, g, i0, j0, 2, 0, kb, tid);
+    pxy.load(f.xy, g, i0, j0, 1, 2, kb, tid);
+    pyy.load(f.yy, g, i0, j0, 0, 1, kb, tid);
+    pxz.load(f.xz, g, i0, j0, 1, 0, kb, tid);
+    pyz.load(f.yz, g, i0, j0, 0, 2, kb, tid);
+    T zq0, zq1 = zz[pc - sz], zq2 = zz[pc], zq3 = zz[pc + sz], nz = zz[pc + 2 * sz];
+    T xq0, xq1 = xz[pc - 2 * sz], xq2 = xz[pc - sz], xq3 = xz[pc], nx = xz[pc + sz];
+    T yq0, yq1 = yz[pc - 2 * sz], yq2 = yz[pc - sz], yq3 = yz[pc], ny = yz[pc + sz];
+    T pd = f.d[pc], pu = f.u[pc], pv = f.v[pc], pw = f.w[pc];
+    const T c1 = c.c1, c2 = c.c2, dth = c.dth;
+    for (int k = kb; k <= ke; ++k) {
+        const long long pk = pc + (long long)(k - kb) * sz;
+        __syncthreads();
+        pxx.store(&s_xx[0][0], tid); pxy.store(&s_xy[0][0], tid); pyy.store(&s_yy[0][0], tid);
+        pxz.store(&s_xz[0][0], tid); pyz.store(&s_yz[0][0], tid);
+        zq0 = zq1; zq1 = zq2; zq2 = zq3; zq3 = nz;
+        xq0 = xq1; xq1 = xq2; xq2 = xq3; xq3 = nx;
+        yq0 = yq1; yq1 = yq2; yq2 = yq3; yq3 = ny;
+        const T cd = pd, cu = pu, cv = pv, cw = pw;
+        if (k < ke) {
+            pxx.load(f.xx, g, i0, j0, 2, 0, k + 1, tid);
+            pxy.load(f.xy, g, i0, j0, 1, 2, k + 1, tid);
+            pyy.load(f.yy, g, i0, j0, 0, 1, k + 1, tid);
+            pxz.load(f.xz, g, i0, j0, 1, 0, k + 1, tid);
+            pyz.load(f.yz, g, i0, j0, 0, 2, k + 1, tid);
+            nz = zz[pk + 3 * sz]; nx = xz[pk + 2 * sz]; ny = yz[pk + 2 * sz];
+            pd = f.d[pk + sz]; pu = f.u[pk + sz]; pv = f.v[pk + sz]; pw = f.w[pk + sz];
+        }
+        __syncthreads();
+        if (!act) continue;
+        const T r = dth / cd;
+        f.u[pk] = cu + r * (c1 * (s_xx[ty][tx + 2] - s_xx[ty][tx + 1]) + c2 * (s_xx[ty][tx + 3] - s_xx[ty][tx]) +
+                            c1 * (s_xy[ty + 2][tx + 1] - s_xy[ty + 1][tx + 1]) + c2 * (s_xy[ty + 3][tx + 1] - s_xy[ty][tx + 1]) +
+                            c1 * (xq2 - xq1) + c2 * (xq3 - xq0));
+        f.v[pk] = cv + r * (c1 * (s_xy[ty + 2][tx + 2] - s_xy[ty + 2][tx + 1]) + c2 * (s_xy[ty + 2][tx + 3] - s_xy[ty + 2][tx]) +
+                            c1 * (s_yy[ty + 2][tx] - s_yy[ty + 1][tx]) + c2 * (s_yy[ty + 3][tx] - s_yy[ty][tx]) +
+                            c1 * (yq2 - yq1) + c2 * (yq3 - yq0));
+        f.w[pk] = cw + r * (c1 * (s_xz[ty][tx + 2] - s_xz[ty][tx + 1]) + c2 * (s_xz[ty][tx + 3] - s_xz[ty][tx]) +
+                            c1 * (s_yz[ty + 2][tx] - s_yz[ty + 1][tx]) + c2 * (s_yz[ty + 3][tx] - s_yz[ty][tx]) +
+                            c1 * (zq2 - zq1) + c2 * (zq3 - zq0));
+    }
+}
+
+// Stress sweep, software-pipelined like k_vel_interior_pipe.
+template <class T>
+__global__ void __launch_bounds__(NT) k_str_interior_pipe(Grid g, Fields<T> f, StepConst<T> c, int kchunk) {
+    __shared__ T s_u[TY + 4][36];
+    __shared__ T s_v[TY + 4][36];
+    __shared__ T s_w[TY + 4][36];
+    const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
+    const int i0 = g.nabc + 1 + blockIdx.x * TX, j0 = g.nabc + 1 + blockIdx.y * TY;
+    const int i = i0 + tx, j = j0 + ty;
+    const bool act = (i <= g.nxt - g.nabc) && (j <= g.nyt - 2);
+    const int kb = g.nabc + 1 + blockIdx.z * kchunk;
+    const int ke = min(kb + kchunk - 1, g.ks());
+    const int ic = min(i, g.nxt - 1), jc = min(j, g.nyt - 1);  // keeps the (i+1,j+1) taps in range
+    const long long sy = g.px, sz = g.plane;
+    const long long pc = g.at(ic, jc, kb);
+    const T* __restrict__ u = f.u; const T* __restrict__ v = f.v; const T* __restrict__ w = f.w;
+    const T* __restrict__ mu = f.mu;
+    Prefetch<T, TY + 4, 36> pu_, pv_, pw_;
+    pu_.load(u, g, i0, j0, 2, 2, kb, tid);
+    pv_.load(v, g, i0, j0, 2, 2, kb, tid);
+    pw_.load(w, g, i0, j0, 2, 2, kb, tid);
+    T uq0, uq1 = u[pc - sz], uq2 = u[pc], uq3 = u[pc + sz], nu = u[pc + 2 * sz];
+    T vq0, vq1 = v[pc - sz], vq2 = v[pc], vq3 = v[pc + sz], nv = v[pc + 2 * sz];
+    T wq0, wq1 = w[pc - 2 * sz], wq2 = w[pc - sz], wq3 = w[pc], nw = w[pc + sz];
+    T mq0, mq1 = mu[pc], nm = mu[pc + sz];
+    T pl = f.lam[pc], pmy = mu[pc + sy], pmd = mu[pc + 1 + sy + sz];
+    T pxx = f.xx[pc], pyy = f.yy[pc], pzz = f.zz[pc], pxy = f.xy[pc], pxz = f.xz[pc], pyz = f.yz[pc];
+    const T c1 = c.c1, c2 = c.c2, dth = c.dth;
+    const int X = tx + 2, Y = ty + 2;
+    for (int k = kb; k <= ke; ++k) {
+        const long long pk = pc + (long long)(k - kb) * sz;
+        __syncthreads();
+        pu_.store(&s_u[0][0], tid); pv_.store(&s_v[0][0], tid); pw_.store(&s_w[0][0], tid);
+        uq0 = uq1; uq1 = uq2; uq2 = uq3; uq3 = nu;
+        vq0 = vq1; vq1 = vq2; vq2 = vq3; vq3 = nv;
+        wq0 = wq1; wq1 = wq2; wq2 = wq3; wq3 = nw;
+        mq0 = mq1; mq1 = nm;
+        const T cl = pl, cmy = pmy, cmd = pmd;
+        const T cxx = pxx, cyy = pyy, czz = pzz, cxy = pxy, cxz = pxz, cyz = pyz;
+        if (k < ke) {
+            pu_.load(u, g, i0, j0, 2, 2, k + 1, tid);
+            pv_.load(v, g, i0, j0, 2, 2, k + 1, tid);
+            pw_.load(w, g, i0, j0, 2, 2, k + 1, tid);
+            const long long pn = pk + sz;
+            nu = u[pn + 2 * sz]; nv = v[pn + 2 * sz]; nw = w[pn + sz]; nm = mu[pn + sz];
+            pl = f.lam[pn]; pmy = mu[pn + sy]; pmd = mu[pn + 1 + sy + sz];
+            pxx = f.xx[pn]; pyy = f.yy[pn]; pzz = f.zz[pn]; pxy = f.xy[pn]; pxz = f.xz[pn]; pyz = f.yz[pn];
+        }
+        __syncthreads();
+        if (!act) continue;
+        const T xl = cl, xm = mq0;
+        const T a = xl + (T)2 * xm, b = xl;
+        const T dxu1 = c1 * (s_u[Y][X + 1] - s_u[Y][X]), dxu2 = c2 * (s_u[Y][X + 2] - s_u[Y][X - 1]);
+        const T dyv1 = c1 * (s_v[Y][X] - s_v[Y - 1][X]), dyv2 = c2 * (s_v[Y + 1][X] - s_v[Y - 2][X]);
+        const T dzw1 = c1 * (wq2 - wq1), dzw2 = c2 * (wq3 - wq0);
+        f.xx[pk] = cxx + dth * a * (dxu1 + dxu2) + dth * b * (dyv1 + dyv2 + dzw1 + dzw2);
+        f.yy[pk] = cyy + dth * a * (dyv1 + dyv2) + dth * b * (dxu1 + dxu2 + dzw1 + dzw2);
+        f.zz[pk] = czz + dth * a * (dzw1 + dzw2) + dth * b * (dxu1 + dxu2 + dyv1 + dyv2);
+        T xmu = (T)0.5 * (xm + cmy);
+        f.xy[pk] = cxy + dth * xmu * (c1 * (s_u[Y + 1][X] - s_u[Y][X]) + c2 * (s_u[Y + 2][X] - s_u[Y - 1][X]) +
+                                      c1 * (s_v[Y][X] - s_v[Y][X - 1]) + c2 * (s_v[Y][X + 1] - s_v[Y][X - 2]));
+        xmu = (T)0.5 * (xm + mq1);
+        f.xz[pk] = cxz + dth * xmu * (c1 * (uq2 - uq1) + c2 * (uq3 - uq0) +
+                                      c1 * (s_w[Y][X] - s_w[Y][X - 1]) + c2 * (s_w[Y][X + 1] - s_w[Y][X - 2]));
+        xmu = (T)0.5 * (xm + cmd);
+        f.yz[pk] = cyz + dth * xmu * (c1 * (vq2 - vq1) + c2 * (vq3 - vq0) +
+                                      c1 * (s_w[Y + 1][X] - s_w[Y][X]) + c2 * (s_w[Y + 2][X] - s_w[Y - 1][X]));
+    }
+}
+
+// Interior sweep variants (chosen per context; the default is the fastest measured on B200)
+enum InteriorVariant { IV_POINT = 0, IV_TILED = 1, IV_PIPE = 2 };
+
+struct InteriorCfg {
+    // measured on B200 at 1020x410x512: pipe/32 planes reaches 66% (velocity) and 67%
+    // (stress) of HBM peak; per-point 61%/53%; tiled without prefetch 22%/26%
+    int variant = IV_PIPE;
+    int kchunk = 32;     // z-planes per CTA
+    int by = 8;          // CTA rows (IV_POINT: block = 32 x by)
+};
+
+inline int interior_nz(const Grid& g) { return g.ks() - g.nabc; }
+
+template <class T>
+void launch_vel_interior(const InteriorCfg& cfg, const Grid& g, const Fields<T>& f, const StepConst<T>& c,
+                         cudaStream_t st) {
+    const int nxT = g.nxt - 2 * g.nabc, nyI = g.nyt - 2 - g.nabc, nzT = interior_nz(g);
+    const int kch = std::max(1, std::min(cfg.kchunk, nzT));
+    if (cfg.variant == IV_POINT) {
+        const int by = cfg.by;
+        dim3 grid((nxT + 31) / 32, (nyI + by - 1) / by, (nzT + kch - 1) / kch);
+        k_vel_interior<T><<<grid, dim3(32, by), 0, st>>>(g, f, c, kch);
+        return;
+    }
+    dim3 grid((nxT + TX - 1) / TX, (nyI + TY - 1) / TY, (nzT + kch - 1) / kch);
+    if (cfg.variant == IV_TILED) k_vel_interior_tiled<T><<<grid, dim3(TX, TY), 0, st>>>(g, f, c, kch);
+    else k_vel_interior_pipe<T><<<grid, dim3(TX, TY), 0, st>>>(g, f, c, kch);
 }
 
 template <class T>
-void launch_vel_interior_opt(const Grid& g, const Fields<T>& f, const StepConst<T>& c, cudaStream_t st) {
-    const int nxT = g.nxt - 2 * g.nabc, nyI = g.nyt - 2 - g.nabc, nzT = g.ks() - g.nabc;
-    const int kch = interior_kchunk(g);
+void launch_str_interior(const InteriorCfg& cfg, const Grid& g, const Fields<T>& f, const StepConst<T>& c,
+                         cudaStream_t st) {
+    const int nxT = g.nxt - 2 * g.nabc, nyI = g.nyt - 2 - g.nabc, nzT = interior_nz(g);
+    const int kch = std::max(1, std::min(cfg.kchunk, nzT));
+    if (cfg.variant == IV_POINT) {
+        const int by = cfg.by;
+        dim3 grid((nxT + 31) / 32, (nyI + by - 1) / by, (nzT + kch - 1) / kch);
+        k_str_interior<T><<<grid, dim3(32, by), 0, st>>>(g, f, c, kch);
+        return;
+    }
     dim3 grid((nxT + TX - 1) / TX, (nyI + TY - 1) / TY, (nzT + kch - 1) / kch);
-    k_vel_interior_tiled<T><<<grid, dim3(TX, TY), 0, st>>>(g, f, c, kch);
-}
-
-template <class T>
-void launch_str_interior_opt(const Grid& g, const Fields<T>& f, const StepConst<T>& c, cudaStream_t st) {
-    const int nxT = g.nxt - 2 * g.nabc, nyI = g.nyt - 2 - g.nabc, nzT = g.ks() - g.nabc;
-    const int kch = interior_kchunk(g);
-    dim3 grid((nxT + TX - 1) / TX, (nyI + TY - 1) / TY, (nzT + kch - 1) / kch);
-    k_str_interior_tiled<T><<<grid, dim3(TX, TY), 0, st>>>(g, f, c, kch);
+    if (cfg.variant == IV_TILED) k_str_interior_tiled<T><<<grid, dim3(TX, TY), 0, st>>>(g, f, c, kch);
+    else k_str_interior_pipe<T><<<grid, dim3(TX, TY), 0, st>>>(g, f, c, kch);
 }
 
 }  // namespace fd3d

@@ -133,14 +133,20 @@ def test_reset_reproduces():
     np.testing.assert_array_equal(s.history(0), h1)
 
 
-def test_tiled_interior_equals_per_point_kernels():
+@pytest.mark.parametrize("variant,kchunk", [("tiled", 64), ("pipe", 64), ("pipe", 5), ("point", 1), ("point", 3)])
+def test_interior_variants_identical(variant, kchunk):
+    """Every interior sweep variant computes the same bits as the per-point kernel."""
     m = configs.tiny_sw(nxT=70, nyT=20, nzT=36, nsteps=30)
-    a = Solver(m)
-    os.environ["FD3D_NAIVE_INTERIOR"] = "1"
+    os.environ["FD3D_INTERIOR"] = "point"
+    os.environ["FD3D_KCHUNK"] = "4"
     try:
+        a = Solver(m)
+        os.environ["FD3D_INTERIOR"] = variant
+        os.environ["FD3D_KCHUNK"] = str(kchunk)
         b = Solver(m)
     finally:
-        del os.environ["FD3D_NAIVE_INTERIOR"]
+        del os.environ["FD3D_INTERIOR"]
+        del os.environ["FD3D_KCHUNK"]
     for s in (a, b):
         s.run(30)
         s.sync()
