@@ -783,3 +783,90 @@ int fd3d_write_results(fd3d_ctx* ctx, const char* dir, int rk) {
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// fd3d_run_noalloc: the time step with the fault boundary condition's trial-traction
+// scratch taken from a fixed, file-scope device array instead of memory the library
+// allocates.  Meant for hosts that cannot let the library allocate device memory once
+// their run has started (their device memory is handed out by another runtime, such
+// as the OpenACC present table of a Fortran host, or was reserved up front against a
+// fixed budget).  fd3d_run may allocate on its first call (it instantiates a CUDA graph
+// of the step); this entry point launches the kernels one by one and calls no
+// cudaMalloc, cudaFree or other allocating routine.
+//
+// Limit: nxt*nzt <= FD3D_NOALLOC_MAX_PLANE fault-plane nodes (the array holds two
+// planes of doubles, 16 MiB, on every GPU that loads the library, until exit).
+// The array is shared by every call on a device and keeps the last call's contents;
+// calls whose work overlaps on a GPU (several contexts on different streams) race on it.
+// ---------------------------------------------------------------------------
+#include <mutex>
+
+#define FD3D_NOALLOC_MAX_PLANE (1 << 20)
+
+static __device__ __align__(256) unsigned char fd3d_noalloc_scratch[2ull * FD3D_NOALLOC_MAX_PLANE * sizeof(double)];
+
+namespace {
+std::mutex g_noalloc_mu;
+void* g_noalloc_addr[256] = {};  // device address of fd3d_noalloc_scratch, per device ordinal
+
+// once per device, with that device current: the host-side name of the array is not a
+// device address, so the kernels get the address returned by cudaGetSymbolAddress
+int noalloc_scratch(int dev, void** out) {
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if (dev < 0 || dev >= 256) return FD3D_ERR_ARG;
+    if (!g_noalloc_addr[dev]) {
+        int cur = -1;
+        if (cudaGetDevice(&cur) != cudaSuccess) return FD3D_ERR_CUDA;
+        if (cur != dev && cudaSetDevice(dev) != cudaSuccess) return FD3D_ERR_CUDA;
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, fd3d_noalloc_scratch);
+        if (cur != dev) cudaSetDevice(cur);
+        if (e != cudaSuccess || !p) {
+            std::fprintf(stderr, "fd3d_run_noalloc: cudaGetSymbolAddress failed: %s\n", cudaGetErrorString(e));
+            return FD3D_ERR_CUDA;
+        }
+        g_noalloc_addr[dev] = p;
+    }
+    *out = g_noalloc_addr[dev];
+    return FD3D_OK;
+}
+
+template <class T>
+int run_noalloc_t(Ctx<T>* c, int nsteps, void* scratch) {
+    const size_t n2 = (size_t)c->p.nxt * c->p.nzt;
+    // cells outside the interior plane are read as zero by the friction launch
+    CK(cudaMemsetAsync(scratch, 0, 2 * n2 * sizeof(T), c->st));
+    CK(cudaEventRecord(c->ev0, c->st));
+    T* const txt0 = c->q.txt;
+    T* const tzt0 = c->q.tzt;
+    c->q.txt = (T*)scratch;
+    c->q.tzt = (T*)scratch + n2;
+    for (int s = 0; s < nsteps; ++s) c->enqueue_step();
+    c->q.txt = txt0;
+    c->q.tzt = tzt0;
+    CK(cudaGetLastError());
+    CK(cudaEventRecord(c->ev1, c->st));
+    c->steps_done += nsteps;
+    return FD3D_OK;
+}
+}  // namespace
+
+extern "C" int fd3d_run_noalloc(fd3d_ctx* ctx, int nsteps) {
+    if (!ctx || nsteps < 0) return FD3D_ERR_ARG;
+    CtxBase* c = ctx->impl;
+    if (!c->medium_ok || !c->fault_ok) return FD3D_ERR_STATE;
+    const long long n2 = (long long)c->p.nxt * c->p.nzt;
+    if (n2 > FD3D_NOALLOC_MAX_PLANE) {
+        std::fprintf(stderr, "fd3d_run_noalloc: fault plane nxt*nzt = %lld nodes exceeds the limit of %d\n", n2,
+                     FD3D_NOALLOC_MAX_PLANE);
+        return FD3D_ERR_ARG;
+    }
+    cudaPointerAttributes attr;
+    CK(cudaPointerGetAttributes(&attr, c->it_dev));  // the device the context lives on
+    void* scratch = nullptr;
+    int rc = noalloc_scratch(attr.device, &scratch);
+    if (rc) return rc;
+    if (auto* cf = dynamic_cast<Ctx<float>*>(c)) return run_noalloc_t(cf, nsteps, scratch);
+    if (auto* cd = dynamic_cast<Ctx<double>*>(c)) return run_noalloc_t(cd, nsteps, scratch);
+    return FD3D_ERR_STATE;
+}

@@ -163,6 +163,17 @@ int fd3d_upload_fault(fd3d_ctx* ctx, const fd3d_fault* f);
 int fd3d_reset(fd3d_ctx* ctx);                      /* zero wave field, PML and fault state (fd3d_theo.f90:59-88) */
 int fd3d_run(fd3d_ctx* ctx, int nsteps);            /* enqueue nsteps time steps; asynchronous */
 int fd3d_sync(fd3d_ctx* ctx);                       /* wait; returns first device error        */
+/* No counterpart in the reference.  Same time steps as fd3d_run, for hosts that cannot
+ * let the library allocate device memory once their run has started (device memory
+ * owned by another runtime, e.g. a Fortran host's OpenACC data region, or reserved up
+ * front against a fixed budget).  It calls no cudaMalloc/cudaFree and instantiates no
+ * graph; the trial-traction scratch of the fault boundary condition lives in a fixed
+ * device array of the library (2 planes of doubles for up to 2^20 = nxt*nzt fault-plane
+ * nodes, 16 MiB held on every GPU that loads the library until exit).  Larger planes
+ * are rejected with FD3D_ERR_ARG.  The first call on a device looks up that array's
+ * device address, so make it before any stream capture.  All calls share the array:
+ * calls whose work overlaps on one GPU (contexts on different streams) race on it. */
+int fd3d_run_noalloc(fd3d_ctx* ctx, int nsteps);
 int fd3d_steps_done(fd3d_ctx* ctx, int* it);
 int fd3d_fetch_history(fd3d_ctx* ctx, int field, int rec0, int nrec, void* host, int real_kind);
 int fd3d_history_records(fd3d_ctx* ctx, int* nrec);  /* records held in the device ring */
