@@ -172,6 +172,9 @@ struct Ctx : CtxBase {
     StepConst<T> c{};
     PmlDesc D{};
     PmlAux<T> X{};
+    VelMaps vmaps{};        // TMA descriptors of the interior sweeps
+    StrMaps smaps{};
+    bool tma_ok = false;
     std::vector<void*> allocs;
     T* fieldpool = nullptr;
     std::vector<double> psiX0, psiZ0;  // initial FVW state, restored by reset
@@ -232,6 +235,8 @@ struct Ctx : CtxBase {
         if (dalloc(&dprof, prof.size())) return FD3D_ERR_NOMEM;
         CK(cudaMemcpyAsync(dprof, prof.data(), prof.size() * sizeof(T), cudaMemcpyHostToDevice, st));
         X.prof = dprof;
+        tma_ok = make_interior_maps<T>(g, f, vmaps, smaps) && prepare_tma_kernels<T>();
+        if (!tma_ok && icfg.variant == IV_TMA) icfg.variant = IV_PIPE;
         if (dalloc(&it_dev, 1)) return FD3D_ERR_NOMEM;
         if (dalloc(&status, 1)) return FD3D_ERR_NOMEM;
         const int stride = std::max(1, p.history_stride);
@@ -429,7 +434,8 @@ struct Ctx : CtxBase {
         const dim3 b2(32, 8);
         // velocity half-step
         kbeg(0);
-        launch_vel_interior<T>(icfg, g, f, c, st);
+        if (icfg.variant == IV_TMA) launch_vel_interior_tma<T>(vmaps, icfg, g, f, c, status, st);
+        else launch_vel_interior<T>(icfg, g, f, c, st);
         kend(0);
         kbeg(1);
         k_vel_fault<T><<<dim3((std::max(nxT, p.nxt) + 31) / 32, (nzT + 7) / 8), b2, 0, st>>>(g, f, q, c, law, fs, it_dev, status);
@@ -443,7 +449,8 @@ struct Ctx : CtxBase {
         kend(3);
         // stress half-step
         kbeg(4);
-        launch_str_interior<T>(icfg, g, f, c, st);
+        if (icfg.variant == IV_TMA) launch_str_interior_tma<T>(smaps, icfg, g, f, c, status, st);
+        else launch_str_interior<T>(icfg, g, f, c, st);
         kend(4);
         kbeg(5);
         k_str_fault<T><<<dim3((nxT + 31) / 32, (nzT + 7) / 8), b2, 0, st>>>(g, f, q, c);
@@ -545,6 +552,7 @@ const char* fd3d_status_string(int s) {
         case FD3D_ERR_IO: return "file I/O error";
         case FD3D_ERR_NODEV: return "no CUDA device";
         case FD3D_ERR_BUSY: return "no free slot";
+        case FD3D_ERR_TIMEOUT: return "a bounded device-side wait timed out";
         default: return "unknown status";
     }
 }
@@ -580,8 +588,10 @@ int fd3d_ctx_create(const fd3d_params* p, fd3d_ctx** out) {
         if (!std::strcmp(e, "point")) c->icfg.variant = IV_POINT;
         else if (!std::strcmp(e, "tiled")) c->icfg.variant = IV_TILED;
         else if (!std::strcmp(e, "pipe")) c->icfg.variant = IV_PIPE;
+        else if (!std::strcmp(e, "tma")) c->icfg.variant = IV_TMA;
     }
-    if (const char* e = std::getenv("FD3D_KCHUNK")) c->icfg.kchunk = std::max(1, std::atoi(e));
+    if (const char* e = std::getenv("FD3D_KCHUNK")) c->icfg.kchunk = c->icfg.kchunk_str = std::max(1, std::atoi(e));
+    if (const char* e = std::getenv("FD3D_KCHUNK_STR")) c->icfg.kchunk_str = std::max(1, std::atoi(e));
     if (const char* e = std::getenv("FD3D_BY")) c->icfg.by = std::min(32, std::max(1, std::atoi(e)));
     rc = c->alloc();
     if (rc) {
@@ -664,6 +674,7 @@ int fd3d_sync(fd3d_ctx* ctx) {
     CK(cudaEventElapsedTime(&c->last_ms, c->ev0, c->ev1));
     int st = 0;
     CK(cudaMemcpy(&st, c->status, sizeof(int), cudaMemcpyDeviceToHost));
+    if (st & ST_TIMEOUT) return FD3D_ERR_TIMEOUT;
     if (st & ST_NONFINITE) return FD3D_ERR_NONFINITE;
     if (st & ST_NEWTON) return FD3D_ERR_NEWTON;
     return FD3D_OK;

@@ -299,13 +299,15 @@ __global__ void __launch_bounds__(NT) k_str_interior_pipe(Grid g, Fields<T> f, S
 }
 
 // Interior sweep variants (chosen per context; the default is the fastest measured on B200)
-enum InteriorVariant { IV_POINT = 0, IV_TILED = 1, IV_PIPE = 2 };
+enum InteriorVariant { IV_POINT = 0, IV_TILED = 1, IV_PIPE = 2, IV_TMA = 3 };
 
 struct InteriorCfg {
-    // measured on B200 at 1020x410x512: pipe/32 planes reaches 66% (velocity) and 67%
-    // (stress) of HBM peak; per-point 61%/53%; tiled without prefetch 22%/26%
-    int variant = IV_PIPE;
-    int kchunk = 32;     // z-planes per CTA
+    // measured on B200 at 1020x410x512 (fraction of the measured HBM copy bandwidth):
+    // TMA ring 97% (velocity, 16 planes per CTA) and 92% (stress, 8 planes);
+    // register-prefetch pipe 66%/67%; per-point 61%/53%; tiled without prefetch 22%/26%
+    int variant = IV_TMA;
+    int kchunk = 16;     // z-planes per CTA of the velocity sweep
+    int kchunk_str = 8;  // z-planes per CTA of the stress sweep
     int by = 8;          // CTA rows (IV_POINT: block = 32 x by)
 };
 
@@ -331,7 +333,7 @@ template <class T>
 void launch_str_interior(const InteriorCfg& cfg, const Grid& g, const Fields<T>& f, const StepConst<T>& c,
                          cudaStream_t st) {
     const int nxT = g.nxt - 2 * g.nabc, nyI = g.nyt - 2 - g.nabc, nzT = interior_nz(g);
-    const int kch = std::max(1, std::min(cfg.kchunk, nzT));
+    const int kch = std::max(1, std::min(cfg.kchunk_str, nzT));
     if (cfg.variant == IV_POINT) {
         const int by = cfg.by;
         dim3 grid((nxT + 31) / 32, (nyI + by - 1) / by, (nzT + kch - 1) / kch);
@@ -341,6 +343,99 @@ void launch_str_interior(const InteriorCfg& cfg, const Grid& g, const Fields<T>&
     dim3 grid((nxT + TX - 1) / TX, (nyI + TY - 1) / TY, (nzT + kch - 1) / kch);
     if (cfg.variant == IV_TILED) k_str_interior_tiled<T><<<grid, dim3(TX, TY), 0, st>>>(g, f, c, kch);
     else k_str_interior_pipe<T><<<grid, dim3(TX, TY), 0, st>>>(g, f, c, kch);
+}
+
+}  // namespace fd3d
+
+#include "fd3d_tma.cuh"
+#include <cudaTypedefs.h>
+
+namespace fd3d {
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no libcuda link)
+inline PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static bool tried = false;
+    if (!tried) {
+        tried = true;
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (PFN_cuTensorMapEncodeTiled_v12000)p;
+        else
+            cudaGetLastError();
+    }
+    return fn;
+}
+
+// 3-D tiled map over one padded field array (x = row element incl. offset, y = j-1, z = k-1)
+template <class T>
+bool encode_field_map(CUtensorMap* m, const T* base, const Grid& g, int box_x, int box_y) {
+    auto enc = tensor_map_encoder();
+    if (!enc) return false;
+    cuuint64_t dims[3] = {(cuuint64_t)g.px, (cuuint64_t)g.nyt, (cuuint64_t)g.nzt};
+    cuuint64_t strides[2] = {(cuuint64_t)g.px * sizeof(T), (cuuint64_t)g.plane * sizeof(T)};
+    cuuint32_t box[3] = {(cuuint32_t)box_x, (cuuint32_t)box_y, 1};
+    cuuint32_t es[3] = {1, 1, 1};
+    CUresult r = enc(m, sizeof(T) == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3,
+                     (void*)base, dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                     CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS;
+}
+
+template <class T>
+bool make_interior_maps(const Grid& g, const Fields<T>& f, VelMaps& V, StrMaps& S) {
+    bool ok = true;
+    ok &= encode_field_map<T>(&V.xx, f.xx, g, 40, 8);
+    ok &= encode_field_map<T>(&V.xy, f.xy, g, 40, 11);
+    ok &= encode_field_map<T>(&V.yy, f.yy, g, 32, 11);
+    ok &= encode_field_map<T>(&V.xz, f.xz, g, 40, 8);
+    ok &= encode_field_map<T>(&V.yz, f.yz, g, 32, 11);
+    ok &= encode_field_map<T>(&V.d, f.d, g, 32, 8);
+    ok &= encode_field_map<T>(&V.u, f.u, g, 32, 8);
+    ok &= encode_field_map<T>(&V.v, f.v, g, 32, 8);
+    ok &= encode_field_map<T>(&V.w, f.w, g, 32, 8);
+    ok &= encode_field_map<T>(&S.u, f.u, g, 40, 12);
+    ok &= encode_field_map<T>(&S.v, f.v, g, 40, 12);
+    ok &= encode_field_map<T>(&S.w, f.w, g, 40, 12);
+    ok &= encode_field_map<T>(&S.lam, f.lam, g, 32, 8);
+    ok &= encode_field_map<T>(&S.mu, f.mu, g, 32, 9);
+    ok &= encode_field_map<T>(&S.xx, f.xx, g, 32, 8);
+    ok &= encode_field_map<T>(&S.yy, f.yy, g, 32, 8);
+    ok &= encode_field_map<T>(&S.zz, f.zz, g, 32, 8);
+    ok &= encode_field_map<T>(&S.xy, f.xy, g, 32, 8);
+    ok &= encode_field_map<T>(&S.xz, f.xz, g, 32, 8);
+    ok &= encode_field_map<T>(&S.yz, f.yz, g, 32, 8);
+    return ok;
+}
+
+template <class T>
+bool prepare_tma_kernels() {
+    const int vs = TMA_NS * VelSlot::ELEMS * (int)sizeof(T) + TMA_SMEM_PAD,
+              ss = TMA_NS * StrSlot::ELEMS * (int)sizeof(T) + TMA_SMEM_PAD;
+    bool ok = cudaFuncSetAttribute(k_vel_interior_tma<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, vs) == cudaSuccess;
+    ok &= cudaFuncSetAttribute(k_str_interior_tma<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, ss) == cudaSuccess;
+    if (!ok) cudaGetLastError();
+    return ok;
+}
+
+template <class T>
+void launch_vel_interior_tma(const VelMaps& M, const InteriorCfg& cfg, const Grid& g, const Fields<T>& f,
+                             const StepConst<T>& c, int* status, cudaStream_t st) {
+    const int nxT = g.nxt - 2 * g.nabc, nyI = g.nyt - 2 - g.nabc, nzT = interior_nz(g);
+    const int kch = std::max(1, std::min(cfg.kchunk, nzT));
+    dim3 grid((nxT + 31) / 32, (nyI + 7) / 8, (nzT + kch - 1) / kch);
+    k_vel_interior_tma<T><<<grid, dim3(32, 8), TMA_NS * VelSlot::ELEMS * sizeof(T) + TMA_SMEM_PAD, st>>>(M, g, f, c, kch, status);
+}
+
+template <class T>
+void launch_str_interior_tma(const StrMaps& M, const InteriorCfg& cfg, const Grid& g, const Fields<T>& f,
+                             const StepConst<T>& c, int* status, cudaStream_t st) {
+    const int nxT = g.nxt - 2 * g.nabc, nyI = g.nyt - 2 - g.nabc, nzT = interior_nz(g);
+    const int kch = std::max(1, std::min(cfg.kchunk_str, nzT));
+    dim3 grid((nxT + 31) / 32, (nyI + 7) / 8, (nzT + kch - 1) / kch);
+    k_str_interior_tma<T><<<grid, dim3(32, 8), TMA_NS * StrSlot::ELEMS * sizeof(T) + TMA_SMEM_PAD, st>>>(M, g, f, c, kch, status);
 }
 
 }  // namespace fd3d

@@ -52,6 +52,7 @@ extern "C" {
 #define FD3D_ERR_IO         -8   /* input or result file could not be read/written */
 #define FD3D_ERR_NODEV      -9   /* no CUDA device / library built without one    */
 #define FD3D_ERR_BUSY      -10   /* batch/serving object has no free slot         */
+#define FD3D_ERR_TIMEOUT   -11   /* a bounded device-side wait gave up            */
 
 /* ---- friction law (compile-time -DFVW switch of the reference) -------- */
 #define FD3D_LAW_SW   0   /* linear slip weakening (reference default)   */

@@ -133,7 +133,8 @@ def test_reset_reproduces():
     np.testing.assert_array_equal(s.history(0), h1)
 
 
-@pytest.mark.parametrize("variant,kchunk", [("tiled", 64), ("pipe", 64), ("pipe", 5), ("point", 1), ("point", 3)])
+@pytest.mark.parametrize("variant,kchunk", [("tiled", 64), ("pipe", 64), ("pipe", 5), ("point", 1), ("point", 3),
+                                            ("tma", 32), ("tma", 5), ("tma", 2), ("tma", 1)])
 def test_interior_variants_identical(variant, kchunk):
     """Every interior sweep variant computes the same bits as the per-point kernel."""
     m = configs.tiny_sw(nxT=70, nyT=20, nzT=36, nsteps=30)
