@@ -191,29 +191,41 @@ __global__ void __launch_bounds__(256) k_vel_pml(Grid g, Fields<T> f, PmlDesc D,
     const T ox = X.prof[S.ox_off + i2], oxS = X.prof[S.oxS_off + i2];
     const T oy = X.prof[S.oy_off + j2], oz = X.prof[S.oz_off + k2];
     const long long p = g.at(i, j, k), sy = g.px, sz = g.plane;
+    const bool dov = (j <= S.nye);
+    // every load first: a store to one array must not hold back the loads of the next
     const T d = f.d[p], dt = c.dt, dh = c.dh;
-    T pt, a0, a1, a2;
-    a0 = X.a[AX_U0][qa]; a1 = X.a[AX_U1][qa]; a2 = X.a[AX_U2][qa];
-    pt = (a0 * ((T)1 - ox) + (dt / d) * (f.xx[p] - f.xx[p - 1]) / dh);        a0 = pt / ((T)1 + ox);
-    pt = (a1 * ((T)1 - oy) + (dt / d) * (f.xy[p] - f.xy[p - sy]) / dh);       a1 = pt / ((T)1 + oy);
-    pt = (a2 * ((T)1 - oz) + (dt / d) * (f.xz[p] - f.xz[p - sz]) / dh);       a2 = pt / ((T)1 + oz);
-    X.a[AX_U0][qa] = a0; X.a[AX_U1][qa] = a1; X.a[AX_U2][qa] = a2;
-    f.u[p] = a0 + a1 + a2;
-    if (j <= S.nye) {
-        if (j == g.nyt - 1) f.v[p + sy] = f.v[p];  // bnd2d mirror of the value before this update
-        a0 = X.a[AX_V0][qa]; a1 = X.a[AX_V1][qa]; a2 = X.a[AX_V2][qa];
-        pt = a0 * ((T)1 - oxS) + (dt / d) * (f.xy[p + 1] - f.xy[p]) / dh;     a0 = pt / ((T)1 + oxS);
-        pt = a1 * ((T)1 - oy) + (dt / d) * (f.yy[p + sy] - f.yy[p]) / dh;     a1 = pt / ((T)1 + oy);
-        pt = a2 * ((T)1 - oz) + (dt / d) * (f.yz[p] - f.yz[p - sz]) / dh;     a2 = pt / ((T)1 + oz);
-        X.a[AX_V0][qa] = a0; X.a[AX_V1][qa] = a1; X.a[AX_V2][qa] = a2;
-        f.v[p] = a0 + a1 + a2;
+    const T xx0 = f.xx[p], xx1 = f.xx[p - 1], xy0 = f.xy[p], xy1 = f.xy[p - sy], xz0 = f.xz[p], xz1 = f.xz[p - sz];
+    const T xz2 = f.xz[p + 1], yz0 = f.yz[p], yz1 = f.yz[p - sy], zz0 = f.zz[p], zz1 = f.zz[p + sz];
+    T u0 = X.a[AX_U0][qa], u1 = X.a[AX_U1][qa], u2 = X.a[AX_U2][qa];
+    T w0 = X.a[AX_W0][qa], w1 = X.a[AX_W1][qa], w2 = X.a[AX_W2][qa];
+    T v0 = 0, v1 = 0, v2 = 0, xy2 = 0, yy0 = 0, yy1 = 0, yz2 = 0, vold = 0;
+    if (dov) {
+        v0 = X.a[AX_V0][qa]; v1 = X.a[AX_V1][qa]; v2 = X.a[AX_V2][qa];
+        xy2 = f.xy[p + 1]; yy0 = f.yy[p + sy]; yy1 = f.yy[p]; yz2 = f.yz[p - sz];
+        if (j == g.nyt - 1) vold = f.v[p];
     }
-    a0 = X.a[AX_W0][qa]; a1 = X.a[AX_W1][qa]; a2 = X.a[AX_W2][qa];
-    pt = a0 * ((T)1 - oxS) + (dt / d) * (f.xz[p + 1] - f.xz[p]) / dh;         a0 = pt / ((T)1 + oxS);
-    pt = a1 * ((T)1 - oy) + (dt / d) * (f.yz[p] - f.yz[p - sy]) / dh;         a1 = pt / ((T)1 + oy);
-    pt = a2 * ((T)1 - oz) + (dt / d) * (f.zz[p + sz] - f.zz[p]) / dh;         a2 = pt / ((T)1 + oz);
-    X.a[AX_W0][qa] = a0; X.a[AX_W1][qa] = a1; X.a[AX_W2][qa] = a2;
-    f.w[p] = a0 + a1 + a2;
+    const T r = dt / d;
+    T pt;
+    pt = (u0 * ((T)1 - ox) + r * (xx0 - xx1) / dh);   u0 = pt / ((T)1 + ox);
+    pt = (u1 * ((T)1 - oy) + r * (xy0 - xy1) / dh);   u1 = pt / ((T)1 + oy);
+    pt = (u2 * ((T)1 - oz) + r * (xz0 - xz1) / dh);   u2 = pt / ((T)1 + oz);
+    pt = w0 * ((T)1 - oxS) + r * (xz2 - xz0) / dh;    w0 = pt / ((T)1 + oxS);
+    pt = w1 * ((T)1 - oy) + r * (yz0 - yz1) / dh;     w1 = pt / ((T)1 + oy);
+    pt = w2 * ((T)1 - oz) + r * (zz1 - zz0) / dh;     w2 = pt / ((T)1 + oz);
+    if (dov) {
+        pt = v0 * ((T)1 - oxS) + r * (xy2 - xy0) / dh; v0 = pt / ((T)1 + oxS);
+        pt = v1 * ((T)1 - oy) + r * (yy0 - yy1) / dh;  v1 = pt / ((T)1 + oy);
+        pt = v2 * ((T)1 - oz) + r * (yz0 - yz2) / dh;  v2 = pt / ((T)1 + oz);
+    }
+    X.a[AX_U0][qa] = u0; X.a[AX_U1][qa] = u1; X.a[AX_U2][qa] = u2;
+    X.a[AX_W0][qa] = w0; X.a[AX_W1][qa] = w1; X.a[AX_W2][qa] = w2;
+    f.u[p] = u0 + u1 + u2;
+    f.w[p] = w0 + w1 + w2;
+    if (dov) {
+        if (j == g.nyt - 1) f.v[p + sy] = vold;  // bnd2d mirror of the value before this update
+        X.a[AX_V0][qa] = v0; X.a[AX_V1][qa] = v1; X.a[AX_V2][qa] = v2;
+        f.v[p] = v0 + v1 + v2;
+    }
 }
 
 // fuvw at the ghost row k=ks+1 (fd3d_deriv.f90:1018-1062).  w needs u and v of the
@@ -355,55 +367,65 @@ __global__ void __launch_bounds__(256) k_str_pml(Grid g, Fields<T> f, PmlDesc D,
     const T ozxz = (s == 3) ? ozS : oz;  // xz, yz: omegazS in strip 4
     const bool top = (s <= 2) && (k == S.nze);  // xz/yz aux zeroed at the top row, strips 1-3
     const long long p = g.at(i, j, k), sy = g.px, sz = g.plane;
+    const bool dxy = (j <= S.nye);
     const T dt = c.dt, dh = c.dh;
-    const T xl = f.lam[p], xm = f.mu[p];
-    const T a = xl + (T)2 * xm, b = xl;
-    const T diff1 = f.u[p + 1] - f.u[p];
-    const T diff2 = f.v[p] - f.v[p - sy];
-    const T diff3 = f.w[p] - f.w[p - sz];
-    T pt, a0, a1, a2;
-    a0 = X.a[AX_XX0][qa]; a1 = X.a[AX_XX1][qa]; a2 = X.a[AX_XX2][qa];
-    pt = a0 * ((T)1 - oxS) + dt * a * diff1 / dh; a0 = pt / ((T)1 + oxS);
-    pt = a1 * ((T)1 - oy) + dt * b * diff2 / dh;  a1 = pt / ((T)1 + oy);
-    pt = a2 * ((T)1 - oz) + dt * b * diff3 / dh;  a2 = pt / ((T)1 + oz);
-    X.a[AX_XX0][qa] = a0; X.a[AX_XX1][qa] = a1; X.a[AX_XX2][qa] = a2;
-    f.xx[p] = a0 + a1 + a2;
-    a0 = X.a[AX_YY0][qa]; a1 = X.a[AX_YY1][qa]; a2 = X.a[AX_YY2][qa];
-    pt = a0 * ((T)1 - oxS) + dt * b * diff1 / dh; a0 = pt / ((T)1 + oxS);
-    pt = a1 * ((T)1 - oy) + dt * a * diff2 / dh;  a1 = pt / ((T)1 + oy);
-    pt = a2 * ((T)1 - oz) + dt * b * diff3 / dh;  a2 = pt / ((T)1 + oz);
-    X.a[AX_YY0][qa] = a0; X.a[AX_YY1][qa] = a1; X.a[AX_YY2][qa] = a2;
-    f.yy[p] = a0 + a1 + a2;
-    a0 = X.a[AX_ZZ0][qa]; a1 = X.a[AX_ZZ1][qa]; a2 = X.a[AX_ZZ2][qa];
-    pt = a0 * ((T)1 - oxS) + dt * b * diff1 / dh; a0 = pt / ((T)1 + oxS);
-    pt = a1 * ((T)1 - oy) + dt * b * diff2 / dh;  a1 = pt / ((T)1 + oy);
-    pt = a2 * ((T)1 - oz) + dt * a * diff3 / dh;  a2 = pt / ((T)1 + oz);
-    X.a[AX_ZZ0][qa] = a0; X.a[AX_ZZ1][qa] = a1; X.a[AX_ZZ2][qa] = a2;
-    f.zz[p] = a0 + a1 + a2;
-    {   // xz (j up to jend_uw)
-        const T xmu = (xm + f.mu[p + sz]) / (T)2;
-        a0 = X.a[AX_XZ0][qa]; a1 = X.a[AX_XZ1][qa];
-        pt = a0 * ((T)1 - ozxz) + dt * xmu * (f.u[p + sz] - f.u[p]) / dh; a0 = pt / ((T)1 + ozxz);
-        pt = a1 * ((T)1 - ox) + dt * xmu * (f.w[p] - f.w[p - 1]) / dh;    a1 = pt / ((T)1 + ox);
-        f.xz[p] = a0 + a1;
-        if (top) { a0 = (T)0; a1 = (T)0; }
-        X.a[AX_XZ0][qa] = a0; X.a[AX_XZ1][qa] = a1;
+    // every load first: a store to one array must not hold back the loads of the next
+    const T xl = f.lam[p], xm = f.mu[p], mz = f.mu[p + sz];
+    const T up = f.u[p], ux = f.u[p + 1], uz = f.u[p + sz];
+    const T vp = f.v[p], vy = f.v[p - sy];
+    const T wp = f.w[p], wz = f.w[p - sz], wx = f.w[p - 1];
+    T x0 = X.a[AX_XX0][qa], x1 = X.a[AX_XX1][qa], x2 = X.a[AX_XX2][qa];
+    T y0 = X.a[AX_YY0][qa], y1 = X.a[AX_YY1][qa], y2 = X.a[AX_YY2][qa];
+    T z0 = X.a[AX_ZZ0][qa], z1 = X.a[AX_ZZ1][qa], z2 = X.a[AX_ZZ2][qa];
+    T q0 = X.a[AX_XZ0][qa], q1 = X.a[AX_XZ1][qa];
+    T e0 = 0, e1 = 0, h0 = 0, h1 = 0, my = 0, md = 0, uy = 0, vx = 0, vz = 0, wy = 0, xyo = 0, yzo = 0;
+    if (dxy) {
+        e0 = X.a[AX_XY0][qa]; e1 = X.a[AX_XY1][qa]; h0 = X.a[AX_YZ0][qa]; h1 = X.a[AX_YZ1][qa];
+        my = f.mu[p + sy]; md = f.mu[p + 1 + sy + sz];
+        uy = f.u[p + sy]; vx = f.v[p - 1]; vz = f.v[p + sz]; wy = f.w[p + sy];
+        if (j == g.nyt - 1) { xyo = f.xy[p]; yzo = f.yz[p]; }
     }
-    if (j <= S.nye) {
-        if (j == g.nyt - 1) { f.xy[p + sy] = f.xy[p]; f.yz[p + sy] = f.yz[p]; }  // strbnd mirror
-        T xmu = (xm + f.mu[p + sy]) / (T)2;
-        a0 = X.a[AX_XY0][qa]; a1 = X.a[AX_XY1][qa];
-        pt = a0 * ((T)1 - oyxy) + dt * xmu * (f.u[p + sy] - f.u[p]) / dh; a0 = pt / ((T)1 + oyxy);
-        pt = a1 * ((T)1 - ox) + dt * xmu * (f.v[p] - f.v[p - 1]) / dh;    a1 = pt / ((T)1 + ox);
-        X.a[AX_XY0][qa] = a0; X.a[AX_XY1][qa] = a1;
-        f.xy[p] = a0 + a1;
-        xmu = (xm + f.mu[p + 1 + sy + sz]) / (T)2;
-        a0 = X.a[AX_YZ0][qa]; a1 = X.a[AX_YZ1][qa];
-        pt = a0 * ((T)1 - ozxz) + dt * xmu * (f.v[p + sz] - f.v[p]) / dh; a0 = pt / ((T)1 + ozxz);
-        pt = a1 * ((T)1 - oyxy) + dt * xmu * (f.w[p + sy] - f.w[p]) / dh; a1 = pt / ((T)1 + oyxy);
-        f.yz[p] = a0 + a1;
-        if (top) { a0 = (T)0; a1 = (T)0; }
-        X.a[AX_YZ0][qa] = a0; X.a[AX_YZ1][qa] = a1;
+    const T a = xl + (T)2 * xm, b = xl;
+    const T diff1 = ux - up, diff2 = vp - vy, diff3 = wp - wz;
+    T pt;
+    pt = x0 * ((T)1 - oxS) + dt * a * diff1 / dh; x0 = pt / ((T)1 + oxS);
+    pt = x1 * ((T)1 - oy) + dt * b * diff2 / dh;  x1 = pt / ((T)1 + oy);
+    pt = x2 * ((T)1 - oz) + dt * b * diff3 / dh;  x2 = pt / ((T)1 + oz);
+    pt = y0 * ((T)1 - oxS) + dt * b * diff1 / dh; y0 = pt / ((T)1 + oxS);
+    pt = y1 * ((T)1 - oy) + dt * a * diff2 / dh;  y1 = pt / ((T)1 + oy);
+    pt = y2 * ((T)1 - oz) + dt * b * diff3 / dh;  y2 = pt / ((T)1 + oz);
+    pt = z0 * ((T)1 - oxS) + dt * b * diff1 / dh; z0 = pt / ((T)1 + oxS);
+    pt = z1 * ((T)1 - oy) + dt * b * diff2 / dh;  z1 = pt / ((T)1 + oy);
+    pt = z2 * ((T)1 - oz) + dt * a * diff3 / dh;  z2 = pt / ((T)1 + oz);
+    {   // xz (j up to jend_uw)
+        const T xmu = (xm + mz) / (T)2;
+        pt = q0 * ((T)1 - ozxz) + dt * xmu * (uz - up) / dh; q0 = pt / ((T)1 + ozxz);
+        pt = q1 * ((T)1 - ox) + dt * xmu * (wp - wx) / dh;   q1 = pt / ((T)1 + ox);
+    }
+    if (dxy) {
+        T xmu = (xm + my) / (T)2;
+        pt = e0 * ((T)1 - oyxy) + dt * xmu * (uy - up) / dh; e0 = pt / ((T)1 + oyxy);
+        pt = e1 * ((T)1 - ox) + dt * xmu * (vp - vx) / dh;   e1 = pt / ((T)1 + ox);
+        xmu = (xm + md) / (T)2;
+        pt = h0 * ((T)1 - ozxz) + dt * xmu * (vz - vp) / dh; h0 = pt / ((T)1 + ozxz);
+        pt = h1 * ((T)1 - oyxy) + dt * xmu * (wy - wp) / dh; h1 = pt / ((T)1 + oyxy);
+    }
+    X.a[AX_XX0][qa] = x0; X.a[AX_XX1][qa] = x1; X.a[AX_XX2][qa] = x2;
+    X.a[AX_YY0][qa] = y0; X.a[AX_YY1][qa] = y1; X.a[AX_YY2][qa] = y2;
+    X.a[AX_ZZ0][qa] = z0; X.a[AX_ZZ1][qa] = z1; X.a[AX_ZZ2][qa] = z2;
+    f.xx[p] = x0 + x1 + x2;
+    f.yy[p] = y0 + y1 + y2;
+    f.zz[p] = z0 + z1 + z2;
+    f.xz[p] = q0 + q1;
+    X.a[AX_XZ0][qa] = top ? (T)0 : q0;  // xz/yz aux zeroed at the top row (strips 1-3)
+    X.a[AX_XZ1][qa] = top ? (T)0 : q1;
+    if (dxy) {
+        if (j == g.nyt - 1) { f.xy[p + sy] = xyo; f.yz[p + sy] = yzo; }  // strbnd mirror
+        X.a[AX_XY0][qa] = e0; X.a[AX_XY1][qa] = e1;
+        f.xy[p] = e0 + e1;
+        f.yz[p] = h0 + h1;
+        X.a[AX_YZ0][qa] = top ? (T)0 : h0;
+        X.a[AX_YZ1][qa] = top ? (T)0 : h1;
     }
 }
 
