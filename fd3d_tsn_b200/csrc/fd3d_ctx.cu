@@ -15,6 +15,7 @@
 #include "fd3d_common.cuh"
 #include "fd3d_kernels.cuh"
 #include "fd3d_opt.cuh"
+#include "fd3d_setup.h"
 #include "fd3d_host.h"
 
 using namespace fd3d;
@@ -30,104 +31,6 @@ using namespace fd3d;
     } while (0)
 
 namespace fd3d {
-
-int validate_params(const fd3d_params* p) {
-    if (!p) return FD3D_ERR_ARG;
-    if (p->nabc < 3 || p->nfs != 2) return FD3D_ERR_ARG;
-    if (p->nxt < 2 * p->nabc + 4 || p->nyt < p->nabc + 4 || p->nzt < p->nabc + p->nfs + 4) return FD3D_ERR_ARG;
-    if (!(p->dh > 0) || !(p->dt > 0)) return FD3D_ERR_ARG;
-    if (p->law != FD3D_LAW_SW && p->law != FD3D_LAW_FVW) return FD3D_ERR_ARG;
-    if (p->precision != FD3D_PREC_F32 && p->precision != FD3D_PREC_F64) return FD3D_ERR_ARG;
-    if (p->nstations < 0 || p->nstations > FD3D_MAX_STATIONS) return FD3D_ERR_ARG;
-    for (int s = 0; s < p->nstations; ++s)
-        if (p->staX[s] < 1 || p->staX[s] > p->nxt || p->staY[s] < 1 || p->staY[s] > p->nyt || p->staZ[s] < 1 ||
-            p->staZ[s] > p->nzt)
-            return FD3D_ERR_ARG;
-    if (p->history_stride < 0 || p->history_capacity < 0) return FD3D_ERR_ARG;
-    if (p->vp_max > 0 && p->vp_max * p->dt / p->dh > 0.25) return FD3D_ERR_CFL;  // fd3d_init.f90:274-278
-    return FD3D_OK;
-}
-
-Grid make_grid(const fd3d_params& p) {
-    Grid g;
-    g.nxt = p.nxt; g.nyt = p.nyt; g.nzt = p.nzt; g.nabc = p.nabc; g.nfs = p.nfs;
-    g.off = (32 - (p.nabc % 32)) % 32;
-    g.px = ((p.nxt + g.off + 31) / 32) * 32;
-    g.plane = (long long)g.px * p.nyt;
-    g.n3 = g.plane * p.nzt + 64;
-    return g;
-}
-
-// init_pml (fd3d_deriv.f90:1319-1493): strip boxes and damping profiles, in T.
-template <class T>
-void make_pml(const fd3d_params& p, PmlDesc& D, std::vector<T>& prof) {
-    const int nxt = p.nxt, nyt = p.nyt, nzt = p.nzt, nabc = p.nabc, nfs = p.nfs;
-    const int bx[4][6] = {{2, nabc, nabc + 1, nyt - 1, nabc + 1, nzt - nfs},
-                          {nxt - nabc + 1, nxt - 1, nabc + 1, nyt - 1, nabc + 1, nzt - nfs},
-                          {2, nxt - 1, 2, nabc, nabc + 1, nzt - nfs},
-                          {2, nxt - 1, 2, nyt - 1, 2, nabc}};
-    long long base = 0;
-    prof.clear();
-    D.cum[0] = 0;
-    std::vector<std::vector<T>> ox(4), oxS(4), oy(4), oyS(4), oz(4), ozS(4);
-    for (int s = 0; s < 4; ++s) {
-        Strip& S = D.s[s];
-        S.nxb = bx[s][0]; S.nxe = bx[s][1]; S.nyb = bx[s][2]; S.nye = bx[s][3]; S.nzb = bx[s][4]; S.nze = bx[s][5];
-        S.ni = S.nxe - S.nxb + 1; S.nk = S.nze - S.nzb + 1; S.nj1 = S.nye - S.nyb + 2;
-        S.jend_uw = (s == 2) ? S.nye : S.nye + 1;
-        S.ncells = (long long)S.ni * S.nj1 * S.nk;
-        S.base = base;
-        base += S.ncells;
-        D.cum[s + 1] = D.cum[s] + (long long)S.ni * (S.jend_uw - S.nyb + 1) * S.nk;
-        ox[s].assign(S.ni, (T)0); oxS[s].assign(S.ni, (T)0);
-        oy[s].assign(S.nj1, (T)0); oyS[s].assign(S.nj1, (T)0);
-        oz[s].assign(S.nk, (T)0); ozS[s].assign(S.nk, (T)0);
-    }
-    const T dt = (T)p.dt, dh = (T)p.dh;
-    const T omegaM = (T)p.pml_fact * (T)p.pml_vp / ((T)2 * dh * (T)(nabc - 1));
-    const int n = nabc - 1;
-    std::vector<T> om(n), omR(n), omM(n), omRM(n);
-    for (int i = 1; i <= n; ++i) {
-        T r = (T)i / (T)n, rM = ((T)i - (T)0.5) / (T)n;
-        om[i - 1] = (T)0.5 * dt * omegaM * ((r * r) * (r * r));
-        omR[nabc - i - 1] = om[i - 1];
-        omM[i - 1] = (T)0.5 * dt * omegaM * ((rM * rM) * (rM * rM));
-        omRM[nabc - i - 1] = omM[i - 1];
-    }
-    for (int i = 1; i <= n; ++i) {  // 1-based reference index i -> 0-based i-1
-        ox[0][i - 1] = omR[i - 1];  oxS[0][i - 1] = omRM[i - 1];
-        ox[1][i - 1] = omM[i - 1];  oxS[1][i - 1] = om[i - 1];
-        oy[2][i - 1] = omR[i - 1];  ox[2][i - 1] = omR[i - 1];  ox[2][nxt - i - 2] = omM[i - 1];
-        oyS[2][i - 1] = omRM[i - 1]; oxS[2][i - 1] = omRM[i - 1]; oxS[2][nxt - i - 2] = om[i - 1];
-        oz[3][i - 1] = omR[i - 1];  ox[3][i - 1] = omR[i - 1];  ox[3][nxt - i - 2] = omM[i - 1];
-        oy[3][i - 1] = omR[i - 1];
-        ozS[3][i - 1] = omRM[i - 1]; oxS[3][i - 1] = omRM[i - 1]; oxS[3][nxt - i - 2] = om[i - 1];
-        oyS[3][i - 1] = omRM[i - 1];
-    }
-    for (int s = 0; s < 4; ++s) {
-        Strip& S = D.s[s];
-        auto put = [&](const std::vector<T>& v) { int o = (int)prof.size(); prof.insert(prof.end(), v.begin(), v.end()); return o; };
-        S.ox_off = put(ox[s]); S.oxS_off = put(oxS[s]);
-        S.oy_off = put(oy[s]); S.oyS_off = put(oyS[s]);
-        S.oz_off = put(oz[s]); S.ozS_off = put(ozS[s]);
-    }
-}
-
-template <class T>
-StepConst<T> make_const(const fd3d_params& p) {
-    StepConst<T> c;
-    c.dt = (T)p.dt; c.dh = (T)p.dh;
-    c.dth = c.dt / c.dh;
-    c.dth2 = (T)0.5 * c.dt / c.dh;
-    c.dht = c.dh / c.dt;
-    c.damp_s = (T)p.damp_s;
-    c.c1 = (T)9 / (T)8;
-    c.c2 = (T)-1 / (T)24;
-    c.dtA = p.dt;
-    c.dhA = (double)c.dh;
-    c.dthA = c.dtA / c.dhA;
-    return c;
-}
 
 struct CtxBase {
     fd3d_params p;

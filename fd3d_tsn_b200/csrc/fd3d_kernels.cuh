@@ -71,10 +71,10 @@ __device__ __forceinline__ double fvw_newton(double vtilde, double cdelta, doubl
 
 // Band j=nyt-1 (2nd order + damping, v mirror) and split-node fault velocity at j=nyt.
 template <class T>
-__global__ void k_vel_fault(Grid g, Fields<T> f, Fault<T> q, StepConst<T> c, int law, FvwScalars s,
-                            int* it_dev, int* status) {
-    const int ii = blockIdx.x * blockDim.x + threadIdx.x;
-    const int kk = blockIdx.y * blockDim.y + threadIdx.y;
+__device__ __forceinline__ void vel_fault_body(Grid g, Fields<T> f, Fault<T> q, StepConst<T> c, int law, FvwScalars s,
+                            int* it_dev, int* status, int bx_, int by_, int bz_) {
+    const int ii = bx_ * blockDim.x + threadIdx.x;
+    const int kk = by_ * blockDim.y + threadIdx.y;
     if (ii == 0 && kk == 0) atomicAdd(it_dev, 1);  // step counter read by the fault BC launches
     const int ks = g.ks();
     const long long sy = g.px, sz = g.plane;
@@ -181,8 +181,9 @@ __device__ __forceinline__ bool pml_locate(const PmlDesc& D, long long t, int& s
 
 // pml_uvw: split-field PML velocity in the 4 strips (fd3d_deriv.f90:1927-2218)
 template <class T>
-__global__ void __launch_bounds__(256) k_vel_pml(Grid g, Fields<T> f, PmlDesc D, PmlAux<T> X, StepConst<T> c) {
-    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void vel_pml_body(Grid g, Fields<T> f, PmlDesc D, PmlAux<T> X, StepConst<T> c, int bx_, int by_, int bz_) {
+    // linear index; the CTA may be 256 x 1 (single model) or 32 x 8 (persistent batch)
+    const long long t = (long long)bx_ * (blockDim.x * blockDim.y) + threadIdx.y * blockDim.x + threadIdx.x;
     int s, i, j, k;
     long long qa;
     if (!pml_locate(D, t, s, i, j, k, qa)) return;
@@ -232,9 +233,9 @@ __global__ void __launch_bounds__(256) k_vel_pml(Grid g, Fields<T> f, PmlDesc D,
 // ghost row at (i+1,j) and (i,j-1); they are recomputed with the same formula
 // (identical operands and order), so no second launch is needed.
 template <class T>
-__global__ void k_vel_fs(Grid g, Fields<T> f) {
-    const int i = 1 + blockIdx.x * blockDim.x + threadIdx.x;
-    const int j = 1 + blockIdx.y * blockDim.y + threadIdx.y;
+__device__ __forceinline__ void vel_fs_body(Grid g, Fields<T> f, int bx_, int by_, int bz_) {
+    const int i = 1 + bx_ * blockDim.x + threadIdx.x;
+    const int j = 1 + by_ * blockDim.y + threadIdx.y;
     if (i > g.nxt || j > g.nyt) return;
     const int n = g.ks();
     const long long sy = g.px, sz = g.plane;
@@ -307,9 +308,9 @@ __global__ void __launch_bounds__(256) k_str_interior(Grid g, Fields<T> f, StepC
 
 // Band j=nyt-1 stresses (2nd order) + xy/yz mirror; sxz1 and tasii at j=nyt.
 template <class T>
-__global__ void k_str_fault(Grid g, Fields<T> f, Fault<T> q, StepConst<T> c) {
-    const int i = g.nabc + 1 + blockIdx.x * blockDim.x + threadIdx.x;
-    const int k = g.nabc + 1 + blockIdx.y * blockDim.y + threadIdx.y;
+__device__ __forceinline__ void str_fault_body(Grid g, Fields<T> f, Fault<T> q, StepConst<T> c, int bx_, int by_, int bz_) {
+    const int i = g.nabc + 1 + bx_ * blockDim.x + threadIdx.x;
+    const int k = g.nabc + 1 + by_ * blockDim.y + threadIdx.y;
     if (i > g.nxt - g.nabc || k > g.ks()) return;
     const long long sy = g.px, sz = g.plane;
     const T dth = c.dth, dth2 = c.dth2, c1 = c.c1, c2 = c.c2;
@@ -353,8 +354,9 @@ __global__ void k_str_fault(Grid g, Fields<T> f, Fault<T> q, StepConst<T> c) {
 
 // pml_xyz in the 4 strips (fd3d_deriv.f90:2304-2992)
 template <class T>
-__global__ void __launch_bounds__(256) k_str_pml(Grid g, Fields<T> f, PmlDesc D, PmlAux<T> X, StepConst<T> c) {
-    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void str_pml_body(Grid g, Fields<T> f, PmlDesc D, PmlAux<T> X, StepConst<T> c, int bx_, int by_, int bz_) {
+    // linear index; the CTA may be 256 x 1 (single model) or 32 x 8 (persistent batch)
+    const long long t = (long long)bx_ * (blockDim.x * blockDim.y) + threadIdx.y * blockDim.x + threadIdx.x;
     int s, i, j, k;
     long long qa;
     if (!pml_locate(D, t, s, i, j, k, qa)) return;
@@ -431,9 +433,9 @@ __global__ void __launch_bounds__(256) k_str_pml(Grid g, Fields<T> f, PmlDesc D,
 
 // fres (fd3d_deriv.f90:1067-1104)
 template <class T>
-__global__ void k_str_fs(Grid g, Fields<T> f) {
-    const int i = 1 + blockIdx.x * blockDim.x + threadIdx.x;
-    const int j = 1 + blockIdx.y * blockDim.y + threadIdx.y;
+__device__ __forceinline__ void str_fs_body(Grid g, Fields<T> f, int bx_, int by_, int bz_) {
+    const int i = 1 + bx_ * blockDim.x + threadIdx.x;
+    const int j = 1 + by_ * blockDim.y + threadIdx.y;
     if (i > g.nxt || j > g.nyt) return;
     const long long p = g.at(i, j, g.ks()), sz = g.plane;
     f.zz[p + sz] = -f.zz[p];
@@ -449,9 +451,9 @@ __global__ void k_str_fs(Grid g, Fields<T> f) {
 // ---------------------------------------------------------------- fault BC
 // trial traction, damping, RF (fd3d_theo.f90:233-308, non-FSPACE)
 template <class T>
-__global__ void k_traction(Grid g, Fields<T> f, Fault<T> q, StepConst<T> c) {
-    const int i = g.nabc + 1 + blockIdx.x * blockDim.x + threadIdx.x;
-    const int k = g.nabc + 1 + blockIdx.y * blockDim.y + threadIdx.y;
+__device__ __forceinline__ void traction_body(Grid g, Fields<T> f, Fault<T> q, StepConst<T> c, int bx_, int by_, int bz_) {
+    const int i = g.nabc + 1 + bx_ * blockDim.x + threadIdx.x;
+    const int k = g.nabc + 1 + by_ * blockDim.y + threadIdx.y;
     const int ks = g.ks();
     if (i > g.nxt - g.nabc || k > ks) return;
     const long long sy = g.px, sz = g.plane;
@@ -489,10 +491,10 @@ __global__ void k_traction(Grid g, Fields<T> f, Fault<T> q, StepConst<T> c) {
 
 // |T| at staggered nodes, friction law, slip, rupture time (fd3d_theo.f90:313-410)
 template <class T>
-__global__ void k_friction(Grid g, Fields<T> f, Fault<T> q, StepConst<T> c, int law, FvwScalars s,
-                           const int* it_dev) {
-    const int i = g.nabc + 1 + blockIdx.x * blockDim.x + threadIdx.x;
-    const int k = g.nabc + 1 + blockIdx.y * blockDim.y + threadIdx.y;
+__device__ __forceinline__ void friction_body(Grid g, Fields<T> f, Fault<T> q, StepConst<T> c, int law, FvwScalars s,
+                           const int* it_dev, int bx_, int by_, int bz_) {
+    const int i = g.nabc + 1 + bx_ * blockDim.x + threadIdx.x;
+    const int k = g.nabc + 1 + by_ * blockDim.y + threadIdx.y;
     if (i > g.nxt - g.nabc || k > g.ks()) return;
     const double time = (double)(*it_dev) * c.dtA;
     const double dtA = c.dtA, rup = 1.e-3;
@@ -602,9 +604,9 @@ struct HistDesc {
 
 // output planes, stations, history ring (fd3d_theo.f90:413-467); non-finite check
 template <class T>
-__global__ void k_output(Grid g, Fields<T> f, Fault<T> q, int law, const int* it_dev, HistDesc h, int* status) {
-    const int ii = blockIdx.x * blockDim.x + threadIdx.x;
-    const int kk = blockIdx.y * blockDim.y + threadIdx.y;
+__device__ __forceinline__ void output_body(Grid g, Fields<T> f, Fault<T> q, int law, const int* it_dev, HistDesc h, int* status, int bx_, int by_, int bz_) {
+    const int ii = bx_ * blockDim.x + threadIdx.x;
+    const int kk = by_ * blockDim.y + threadIdx.y;
     const int it = *it_dev;
     const bool rec = (it % h.stride) == 0;
     const long long slot = (long long)((it / h.stride - 1) % h.cap);
@@ -655,9 +657,9 @@ __global__ void k_output(Grid g, Fields<T> f, Fault<T> q, int law, const int* it
 
 // TPV103/104 smooth nucleation of T0X (fd3d_theo.f90:487-542)
 template <class T>
-__global__ void k_nucleation(Grid g, Fault<T> q, StepConst<T> c, FvwScalars s, const int* it_dev) {
-    const int i = g.nabc - 1 + blockIdx.x * blockDim.x + threadIdx.x;
-    const int k = g.nabc - 1 + blockIdx.y * blockDim.y + threadIdx.y;
+__device__ __forceinline__ void nucleation_body(Grid g, Fault<T> q, StepConst<T> c, FvwScalars s, const int* it_dev, int bx_, int by_, int bz_) {
+    const int i = g.nabc - 1 + bx_ * blockDim.x + threadIdx.x;
+    const int k = g.nabc - 1 + by_ * blockDim.y + threadIdx.y;
     if (i > g.nxt - g.nabc || k > g.ks()) return;
     const double time = (double)(*it_dev) * c.dtA;
     const double th = time - c.dtA / 2.0;
@@ -668,6 +670,59 @@ __global__ void k_nucleation(Grid g, Fault<T> q, StepConst<T> c, FvwScalars s, c
     const double FXZ = (rr < s.RR2 - c.dhA) ? exp(rr / (rr - s.RR2 - c.dhA)) : 0.0;
     const double base = s.nucleation == 2 ? (double)q.T0Xb[g.at2(i, k)] : s.strinixI;
     q.T0X[g.at2(i, k)] = (T)(base + s.perturb * FXZ * GT);
+}
+
+// ---------------------------------------------------------------- launch wrappers
+template <class T>
+__global__ void k_vel_fault(Grid g, Fields<T> f, Fault<T> q, StepConst<T> c, int law, FvwScalars s,
+                            int* it_dev, int* status) {
+    vel_fault_body<T>(g, f, q, c, law, s, it_dev, status, blockIdx.x, blockIdx.y, blockIdx.z);
+}
+
+template <class T>
+__global__ void __launch_bounds__(256) k_vel_pml(Grid g, Fields<T> f, PmlDesc D, PmlAux<T> X, StepConst<T> c) {
+    vel_pml_body<T>(g, f, D, X, c, blockIdx.x, blockIdx.y, blockIdx.z);
+}
+
+template <class T>
+__global__ void k_vel_fs(Grid g, Fields<T> f) {
+    vel_fs_body<T>(g, f, blockIdx.x, blockIdx.y, blockIdx.z);
+}
+
+template <class T>
+__global__ void k_str_fault(Grid g, Fields<T> f, Fault<T> q, StepConst<T> c) {
+    str_fault_body<T>(g, f, q, c, blockIdx.x, blockIdx.y, blockIdx.z);
+}
+
+template <class T>
+__global__ void __launch_bounds__(256) k_str_pml(Grid g, Fields<T> f, PmlDesc D, PmlAux<T> X, StepConst<T> c) {
+    str_pml_body<T>(g, f, D, X, c, blockIdx.x, blockIdx.y, blockIdx.z);
+}
+
+template <class T>
+__global__ void k_str_fs(Grid g, Fields<T> f) {
+    str_fs_body<T>(g, f, blockIdx.x, blockIdx.y, blockIdx.z);
+}
+
+template <class T>
+__global__ void k_traction(Grid g, Fields<T> f, Fault<T> q, StepConst<T> c) {
+    traction_body<T>(g, f, q, c, blockIdx.x, blockIdx.y, blockIdx.z);
+}
+
+template <class T>
+__global__ void k_friction(Grid g, Fields<T> f, Fault<T> q, StepConst<T> c, int law, FvwScalars s,
+                           const int* it_dev) {
+    friction_body<T>(g, f, q, c, law, s, it_dev, blockIdx.x, blockIdx.y, blockIdx.z);
+}
+
+template <class T>
+__global__ void k_output(Grid g, Fields<T> f, Fault<T> q, int law, const int* it_dev, HistDesc h, int* status) {
+    output_body<T>(g, f, q, law, it_dev, h, status, blockIdx.x, blockIdx.y, blockIdx.z);
+}
+
+template <class T>
+__global__ void k_nucleation(Grid g, Fault<T> q, StepConst<T> c, FvwScalars s, const int* it_dev) {
+    nucleation_body<T>(g, q, c, s, it_dev, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
 }  // namespace fd3d

@@ -167,17 +167,17 @@ struct Prefetch {
 // Velocity sweep, software-pipelined: the staged windows, the z-queue fronts and the
 // own-point operands of plane k+1 are loaded while plane k is computed.
 template <class T>
-__global__ void __launch_bounds__(NT) k_vel_interior_pipe(Grid g, Fields<T> f, StepConst<T> c, int kchunk) {
+__device__ __forceinline__ void vel_interior_pipe_body(Grid g, Fields<T> f, StepConst<T> c, int kchunk, int bx_, int by_, int bz_) {
     __shared__ T s_xx[TY][36];
     __shared__ T s_xy[TY + 3][36];
     __shared__ T s_yy[TY + 3][TX];
     __shared__ T s_xz[TY][36];
     __shared__ T s_yz[TY + 3][TX];
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
-    const int i0 = g.nabc + 1 + blockIdx.x * TX, j0 = g.nabc + 1 + blockIdx.y * TY;
+    const int i0 = g.nabc + 1 + bx_ * TX, j0 = g.nabc + 1 + by_ * TY;
     const int i = i0 + tx, j = j0 + ty;
     const bool act = (i <= g.nxt - g.nabc) && (j <= g.nyt - 2);
-    const int kb = g.nabc + 1 + blockIdx.z * kchunk;
+    const int kb = g.nabc + 1 + bz_ * kchunk;
     const int ke = min(kb + kchunk - 1, g.ks());
     const int ic = min(i, g.nxt), jc = min(j, g.nyt);
     const long long sz = g.plane;
@@ -230,15 +230,15 @@ __global__ void __launch_bounds__(NT) k_vel_interior_pipe(Grid g, Fields<T> f, S
 
 // Stress sweep, software-pipelined like k_vel_interior_pipe.
 template <class T>
-__global__ void __launch_bounds__(NT) k_str_interior_pipe(Grid g, Fields<T> f, StepConst<T> c, int kchunk) {
+__device__ __forceinline__ void str_interior_pipe_body(Grid g, Fields<T> f, StepConst<T> c, int kchunk, int bx_, int by_, int bz_) {
     __shared__ T s_u[TY + 4][36];
     __shared__ T s_v[TY + 4][36];
     __shared__ T s_w[TY + 4][36];
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
-    const int i0 = g.nabc + 1 + blockIdx.x * TX, j0 = g.nabc + 1 + blockIdx.y * TY;
+    const int i0 = g.nabc + 1 + bx_ * TX, j0 = g.nabc + 1 + by_ * TY;
     const int i = i0 + tx, j = j0 + ty;
     const bool act = (i <= g.nxt - g.nabc) && (j <= g.nyt - 2);
-    const int kb = g.nabc + 1 + blockIdx.z * kchunk;
+    const int kb = g.nabc + 1 + bz_ * kchunk;
     const int ke = min(kb + kchunk - 1, g.ks());
     const int ic = min(i, g.nxt - 1), jc = min(j, g.nyt - 1);  // keeps the (i+1,j+1) taps in range
     const long long sy = g.px, sz = g.plane;
@@ -297,6 +297,18 @@ __global__ void __launch_bounds__(NT) k_str_interior_pipe(Grid g, Fields<T> f, S
                                       c1 * (s_w[Y + 1][X] - s_w[Y][X]) + c2 * (s_w[Y + 2][X] - s_w[Y - 1][X]));
     }
 }
+
+// ---------------------------------------------------------------- launch wrappers
+template <class T>
+__global__ void __launch_bounds__(NT) k_vel_interior_pipe(Grid g, Fields<T> f, StepConst<T> c, int kchunk) {
+    vel_interior_pipe_body<T>(g, f, c, kchunk, blockIdx.x, blockIdx.y, blockIdx.z);
+}
+
+template <class T>
+__global__ void __launch_bounds__(NT) k_str_interior_pipe(Grid g, Fields<T> f, StepConst<T> c, int kchunk) {
+    str_interior_pipe_body<T>(g, f, c, kchunk, blockIdx.x, blockIdx.y, blockIdx.z);
+}
+
 
 // Interior sweep variants (chosen per context; the default is the fastest measured on B200)
 enum InteriorVariant { IV_POINT = 0, IV_TILED = 1, IV_PIPE = 2, IV_TMA = 3 };

@@ -193,6 +193,39 @@ int fd3d_kernel_times(fd3d_ctx* ctx, float* ms /* FD3D_NKERNELS */, int* launche
 /* kernel ids in fd3d_kernel_times: 0 vel_interior, 1 vel_fault, 2 vel_pml, 3 vel_fs,
    4 str_interior, 5 str_fault, 6 str_pml, 7 fault_bc (traction+friction+output) */
 
+/* ---- many models in one persistent launch ------------------------------
+ * No counterpart in the reference, which runs one model per process
+ * (src/dynamicsolver.f90:66).  Independent forward models of uneven size share one
+ * device arena of arena_bytes; fd3d_batch_run advances every live model by up to
+ * nsteps steps (each stops at its own ntfd) in one cooperative kernel.  Models use
+ * the FP32 build, a 1-D layered medium (one value per k, as readcrustalmodel builds)
+ * and keep the last history_capacity records (default 16) of their history planes.
+ * A model's results are the same bits whether it runs alone or among others. */
+typedef struct fd3d_batch fd3d_batch;
+int fd3d_batch_create(size_t arena_bytes, int max_models, fd3d_batch** out);
+int fd3d_batch_destroy(fd3d_batch* b);
+int fd3d_batch_bytes_needed(const fd3d_params* p, size_t* bytes);       /* arena bytes one model takes */
+int fd3d_batch_add(fd3d_batch* b, const fd3d_params* p, const double* lam_k, const double* mu_k,
+                   const double* d_k, const fd3d_fault* f, int* slot);   /* FD3D_ERR_NOMEM: arena full */
+int fd3d_batch_remove(fd3d_batch* b, int slot);
+int fd3d_batch_reset(fd3d_batch* b, int slot);                          /* back to step 0 */
+int fd3d_batch_run(fd3d_batch* b, int nsteps);
+int fd3d_batch_sync(fd3d_batch* b);
+int fd3d_batch_model_status(fd3d_batch* b, int slot);                   /* per-model device error */
+int fd3d_batch_last_run_ms(fd3d_batch* b, float* ms);
+int fd3d_batch_steps_done(fd3d_batch* b, int slot, int* it);
+int fd3d_batch_live(fd3d_batch* b, int* nlive, size_t* bytes_in_use);
+int fd3d_batch_fetch_plane(fd3d_batch* b, int slot, int plane, double* host);
+int fd3d_batch_fetch_final(fd3d_batch* b, int slot, double* slipX, double* slipZ, double* ruptime,
+                           double* rise, double* sliptime);
+int fd3d_batch_fetch_history(fd3d_batch* b, int slot, int field, int rec0, int nrec, double* host);
+/* tile shape of the persistent launch: z-planes per interior tile and CTAs per SM (0 = max) */
+int fd3d_batch_set_tuning(fd3d_batch* b, int kchunk, int ctas_per_sm);
+int fd3d_batch_get_tuning(fd3d_batch* b, int* kchunk, int* ctas_per_sm, int* max_ctas_per_sm);
+/* times the tile-shape candidates on the live models (all at step 0), keeps the fastest,
+ * resets the models; cache_path/key (optional) persist the choice as JSON lines */
+int fd3d_batch_autotune(fd3d_batch* b, int steps, const char* cache_path, const char* key);
+
 /* ---- input decks (the reference's own files) --------------------------- */
 /* Reads inputfd3d.dat and crustal.dat from dir (fd3d_init.f90:145-173, 211-279),
  * fills p and returns lam1/mu1/d1 (caller frees with fd3d_free). */
