@@ -177,19 +177,24 @@ def run_reference(args, world, rank, local, pg):
     m = workload(args.workload)
     from oracle import oracle as om
     o = om.Oracle(m, om.F32)
-    for _ in range(args.warmup):
-        o.step(1, history=True)
+    o.step(1, history=True)  # first touch of the state; the CPU path has nothing else to warm
+    # whole time steps of the same model, at most args.steps and about a minute of CPU work
+    n, dt = 0, 0.0
     t0 = time.perf_counter()
-    o.step(args.steps, history=True)
-    dt = time.perf_counter() - t0
+    while n < args.steps and (n < 2 or dt < args.ref_seconds):
+        o.step(1, history=True)
+        n += 1
+        dt = time.perf_counter() - t0
     cells = m["nxt"] * m["nyt"] * m["nzt"]
-    v = cells * args.steps / dt / 1e9
+    v = cells * n / dt / 1e9
     line = {"impl": "reference", "metric": "GCell-updates/s", "value": v, "unit": "GCell-updates/s",
-            "n_gpus": 0, "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3,
+            "n_gpus": 0, "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt / n * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic", "config": describe(args.workload, m),
             "cpu_baseline": {"value": v, "unit": "GCell-updates/s", "cores": om.num_threads(), "kind": "port",
-                             "sample": f"{args.steps} whole time steps with history planes, all host threads"},
+                             "sample": f"{n} whole time steps of the {m['nxt']}x{m['nyt']}x{m['nzt']} model with "
+                                       f"history planes ({dt:.1f} s) after 1 untimed step, all host threads; the "
+                                       f"CPU restatement of the reference in FP32 (no Fortran compiler here)"},
             "e2e": {"value": v, "unit": "GCell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -322,14 +327,105 @@ def end_to_end(m, steps, local):
                                         "planes + stations read back; wall clock"}
 
 
+def _same_finals(a, b):
+    return all(np.array_equal(a[k], b[k]) for k in ("slipX", "slipZ", "ruptime", "rise", "sliptime"))
+
+
+def run_batch_bench(args, world, rank, local, pg):
+    """256 slip-weakening models of uneven size (fault 8-24 x 6-14 km, h=200 m, 8 s) in
+    one persistent launch per chunk of steps, against the same models solved one at a
+    time through the single-model path."""
+    from fd3d_tsn_b200 import configs
+    from fd3d_tsn_b200.batch import Batch, bytes_needed
+    from fd3d_tsn_b200.solver import lib
+    from fd3d_tsn_b200.serve import plain
+    lib().fd3d_set_device(local)
+    models = configs.batch_set(args.models, seed=2024 + rank)
+    for q, m in enumerate(models):
+        m["request"] = q
+    cells = sum(m["nxt"] * m["nyt"] * m["nzt"] * m["ntfd"] for m in models)
+    arena = int(sum(bytes_needed(m) for m in models) * 1.05) + (64 << 20)
+    t_setup = time.perf_counter()
+    b = Batch(arena, len(models) + 8)
+    slots = [b.add(m) for m in models]
+    tune = b.autotune(steps=10, cache_path=os.path.join(tempfile.gettempdir(), "fd3d_batch_tune.jsonl"),
+                      key=f"batch{len(models)}-seed{2024 + rank}")
+    t_setup = time.perf_counter() - t_setup
+    barrier(pg, local)
+    t0 = time.perf_counter()
+    gpu = 0.0
+    nmax = max(m["ntfd"] for m in models)
+    done = 0
+    while done < nmax:
+        b.run(64)
+        b.sync()
+        gpu += b.last_run_ms() / 1e3
+        done += 64
+    finals = {q: b.final(s) for q, s in zip(range(len(models)), slots)}
+    wall = time.perf_counter() - t0
+    b.close()
+    wall_max = max_over_ranks(pg, local, wall)
+    ref, t_plain = plain(models)
+    identical = all(_same_finals(finals[q], ref[q]) for q in ref)
+    if rank == 0:
+        line = {"metric": "batched solves/s", "value": len(models) * world / wall_max, "unit": "solves/s",
+                "n_gpus": world, "higher_is_better": True, "scaling": "weak", "dtype": "f32", "data": "synthetic",
+                "config": {"workload": "batch", "models": len(models), "h_m": 200.0, "sim_s": 8.0,
+                           "cells_x_steps": cells},
+                "gcell_updates_per_s": cells / wall / 1e9, "gpu_s": gpu, "wall_s": wall, "setup_s": t_setup,
+                "tuning": tune,
+                "plain": {"solves_per_s": len(models) / t_plain, "wall_s": t_plain,
+                          "gcell_updates_per_s": cells / t_plain / 1e9},
+                "speedup_vs_plain": (len(models) / wall) / (len(models) / t_plain),
+                "results_identical_to_plain": identical}
+        print(json.dumps(line), flush=True)
+
+
+def run_serve_bench(args, world, rank, local, pg):
+    """Poisson stream of mixed-size requests (95% batch-size models, 5% large h=100 m
+    models) through the continuous-batching loop, against one-at-a-time plain solves
+    of a sample of the same requests."""
+    from fd3d_tsn_b200 import configs
+    from fd3d_tsn_b200.serve import plain, serve
+    from fd3d_tsn_b200.solver import lib
+    lib().fd3d_set_device(local)
+    stream = configs.serving_stream(args.requests, seed=4242 + rank, rate=args.rate, sim_time=args.sim_time)
+    sample = set(range(0, len(stream), max(1, len(stream) // args.plain_sample)))
+    budget = int(args.hbm_gb * (1 << 30))
+    results, stats = serve(stream, budget, chunk=32, autotune_key=f"serve-{args.sim_time}",
+                           tune_cache=os.path.join(tempfile.gettempdir(), "fd3d_batch_tune.jsonl"),
+                           keep_final=lambda r: r in sample)
+    byreq = {r.request: r for r in results}
+    ref, t_plain = plain([m for q, (_, m) in enumerate(stream) if q in sample], keep_final=lambda r: True)
+    identical = all(_same_finals(byreq[q].final, ref[q]) for q in ref)
+    plain_rate = len(ref) / t_plain
+    if rank == 0:
+        line = {"metric": "serving solves/s", "value": stats["solves_per_s"] * world, "unit": "solves/s",
+                "n_gpus": world, "higher_is_better": True, "scaling": "weak", "dtype": "f32", "data": "synthetic",
+                "config": {"workload": "serve", "requests": len(stream), "arrival_rate_per_s": args.rate,
+                           "large_fraction": 0.05, "sim_s": args.sim_time, "hbm_budget_gb": args.hbm_gb},
+                "p50_latency_s": stats["p50_latency_s"], "p99_latency_s": stats["p99_latency_s"], "stats": stats,
+                "plain": {"solves_per_s": plain_rate, "sample": len(ref), "wall_s": t_plain},
+                "speedup_vs_plain": stats["solves_per_s"] / plain_rate,
+                "results_identical_to_plain": identical}
+        print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
+    ap.add_argument("--models", type=int, default=256, help="batch workload: number of models")
+    ap.add_argument("--requests", type=int, default=2000, help="serve workload: number of requests")
+    ap.add_argument("--rate", type=float, default=60.0, help="serve workload: Poisson arrival rate (1/s)")
+    ap.add_argument("--sim-time", type=float, default=2.0, help="serve workload: simulated seconds per request")
+    ap.add_argument("--plain-sample", type=int, default=64, help="serve workload: plain solves timed")
+    ap.add_argument("--hbm-gb", type=float, default=120.0, help="serve workload: arena (HBM budget) in GB")
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default="sw_large")
     ap.add_argument("--cpu-baseline", type=float, default=15.0, help="seconds of oracle time (0 = skip)")
+    ap.add_argument("--ref-seconds", type=float, default=60.0, help="reference arm: CPU seconds to time")
     ap.add_argument("--no-e2e", dest="e2e", action="store_false")
     args = ap.parse_args()
     if args.warmup < 3:
@@ -338,6 +434,10 @@ def main():
     try:
         if args.impl == "reference":
             run_reference(args, world, rank, local, pg)
+        elif args.workload == "batch":
+            run_batch_bench(args, world, rank, local, pg)
+        elif args.workload == "serve":
+            run_serve_bench(args, world, rank, local, pg)
         else:
             run_b200(args, world, rank, local, pg)
     finally:

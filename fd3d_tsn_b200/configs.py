@@ -241,6 +241,38 @@ def batch_model(rng, seed, h=200.0, sim_time=8.0, precision="f32", ntfd=None):
                     ntfd=ntfd)
 
 
+def batch_set(n=256, seed=2024, sim_time=8.0, ntfd=None):
+    """The batched workload: n seeded models of uneven size (batch_model)."""
+    rng = np.random.default_rng(seed)
+    return [batch_model(rng, seed * 1000 + q, sim_time=sim_time, ntfd=ntfd) for q in range(n)]
+
+
+def large_serving_model(rng, seed, sim_time=8.0, ntfd=None):
+    """The large request of the serving stream: h=100 m, 40x20 km fault, padded as
+    batch_model, 5 seeded layers as sw_large."""
+    h = 100.0
+    fx, fz = 400, 200
+    lay = layered(np.random.default_rng(seed + 7), 5, (fz + 30) * h)
+    return sw_model(fx + 60, 30, fz + 30, h, sim_time, seed, layers=lay, patch_nodes=(fx, fz), nstations=2,
+                    ntfd=ntfd)
+
+
+def serving_stream(n=2000, seed=4242, rate=30.0, large_frac=0.05, sim_time=8.0):
+    """Poisson arrivals (seeded rate in requests/s): (arrival_s, model) pairs; a fraction
+    large_frac of the requests are large_serving_model, the rest batch_model."""
+    rng = np.random.default_rng(seed)
+    t = np.cumsum(rng.exponential(1.0 / rate, size=n))
+    out = []
+    for q in range(n):
+        if rng.uniform() < large_frac:
+            m = large_serving_model(rng, seed * 10000 + q, sim_time=sim_time)
+        else:
+            m = batch_model(rng, seed * 10000 + q, sim_time=sim_time)
+        m["request"] = q
+        out.append((float(t[q]), m))
+    return out
+
+
 def tiny_sw(seed=5, nxT=40, nyT=14, nzT=28, h=200.0, nsteps=60, precision="f32", nstations=3, stride=1):
     """Parity-test model: rupture starts on step 1 from an overstressed nucleation patch."""
     return sw_model(nxT, nyT, nzT, h, 1.0, seed, patch_nodes=(nxT - 8, nzT - 8), nstations=nstations,

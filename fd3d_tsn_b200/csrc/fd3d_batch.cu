@@ -118,9 +118,22 @@ __device__ bool grid_barrier(BatchSync* b, unsigned nblocks, int* status) {
     return ok != 0;
 }
 
-__global__ void __launch_bounds__(256) k_batch(const ModelDev* __restrict__ models, const Work* __restrict__ work,
-                                               const int* __restrict__ pbeg, const int* __restrict__ limit,
-                                               int nsteps, int kchunk, BatchSync* sync, int* gstatus) {
+struct ModelMaps {  // TMA descriptors of one model's interior sweeps (global memory, 64-byte aligned)
+    VelMaps v;
+    StrMaps s;
+};
+
+constexpr int BATCH_MIN_CTAS = 3;  // register cap so that 3 CTAs of 256 threads fit an SM
+
+__global__ void __launch_bounds__(256, BATCH_MIN_CTAS)
+k_batch(const ModelDev* __restrict__ models, const ModelMaps* __restrict__ maps, const Work* __restrict__ work,
+        const int* __restrict__ pbeg, const int* __restrict__ limit, int nsteps, int kchunk, BatchSync* sync,
+        int* gstatus) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    float* ring = reinterpret_cast<float*>(smem_raw + ((128u - (smem_addr(smem_raw) & 127u)) & 127u));
+    __shared__ __align__(8) uint64_t bars[TMA_NS];
+    tma_ring_init(bars);
+    unsigned pc = 0;  // planes this CTA has put through its ring
     const unsigned nb = gridDim.x;
     for (int s = 0; s < nsteps; ++s) {
         for (int ph = 0; ph < NPHASE; ++ph) {
@@ -130,14 +143,21 @@ __global__ void __launch_bounds__(256) k_batch(const ModelDev* __restrict__ mode
                 const int m = it.tm >> 8, type = it.tm & 255;
                 if (s >= limit[m]) continue;  // uniform over the CTA: the item belongs to one model
                 const ModelDev& M = models[m];
+                bool ok = true;
                 switch (type) {
-                    case W_VEL_INT: vel_interior_pipe_body<float>(M.g, M.f, M.c, kchunk, it.bx, it.by, it.bz); break;
+                    case W_VEL_INT:
+                        ok = vel_interior_tma_body<float>(maps[m].v, M.g, M.f, M.c, kchunk, it.bx, it.by, it.bz, ring,
+                                                          bars, pc, gstatus);
+                        break;
                     case W_VEL_FAULT:
                         vel_fault_body<float>(M.g, M.f, M.q, M.c, M.law, M.fs, M.it_dev, M.status, it.bx, it.by, 0);
                         break;
                     case W_VEL_PML: vel_pml_body<float>(M.g, M.f, M.D, M.X, M.c, it.bx, 0, 0); break;
                     case W_VEL_FS: vel_fs_body<float>(M.g, M.f, it.bx, it.by, 0); break;
-                    case W_STR_INT: str_interior_pipe_body<float>(M.g, M.f, M.c, kchunk, it.bx, it.by, it.bz); break;
+                    case W_STR_INT:
+                        ok = str_interior_tma_body<float>(maps[m].s, M.g, M.f, M.c, kchunk, it.bx, it.by, it.bz, ring,
+                                                          bars, pc, gstatus);
+                        break;
                     case W_STR_FAULT: str_fault_body<float>(M.g, M.f, M.q, M.c, it.bx, it.by, 0); break;
                     case W_STR_PML: str_pml_body<float>(M.g, M.f, M.D, M.X, M.c, it.bx, 0, 0); break;
                     case W_STR_FS: str_fs_body<float>(M.g, M.f, it.bx, it.by, 0); break;
@@ -147,7 +167,11 @@ __global__ void __launch_bounds__(256) k_batch(const ModelDev* __restrict__ mode
                     case W_NUC: nucleation_body<float>(M.g, M.q, M.c, M.fs, M.it_dev, it.bx, it.by, 0); break;
                     default: break;
                 }
-                __syncthreads();  // the interior bodies reuse static shared memory
+                if (!ok) {  // a ring wait timed out: make every CTA leave at its next barrier
+                    if (threadIdx.x == 0 && threadIdx.y == 0) atomicExch(&sync->abort, 1);
+                    return;
+                }
+                __syncthreads();  // the next item may reuse the ring
             }
             if (!grid_barrier(sync, nb, gstatus)) return;
         }
@@ -243,7 +267,7 @@ size_t model_bytes(const fd3d_params& p, const Grid& g, const PmlDesc& D, int pr
     add((size_t)g.n3 * 12 * 4);
     for (int k = 0; k < NF_PLANES; ++k) add(n2 * 4);
     for (int k = 0; k < ND_PLANES; ++k) add(n2 * 8);
-    add((size_t)ncell * AX_N * 4);
+    add((size_t)aux_cells32(ncell) * AX_N * 4);
     add((size_t)prof_n * 4);
     add((size_t)cap * nf * plane * 4);
     add((size_t)cap * std::max(1, p.nstations) * 3 * 4);
@@ -276,6 +300,7 @@ struct fd3d_batch {
     Arena arena;
     std::vector<Model> models;
     ModelDev* d_models = nullptr;
+    ModelMaps* d_maps = nullptr;
     int* d_limit = nullptr;
     int* d_pbeg = nullptr;
     Work* d_work = nullptr;
@@ -366,9 +391,9 @@ int launch_batch(fd3d_batch* b, int nsteps) {
     const int per_sm = b->tun.per_sm > 0 ? std::min(b->tun.per_sm, b->max_active) : b->max_active;
     const int grid = std::max(1, per_sm * b->nsm);
     BCK(cudaMemsetAsync(b->d_sync, 0, sizeof(BatchSync), b->st));
-    void* args[] = {&b->d_models, &b->d_work, &b->d_pbeg, &b->d_limit, &nsteps, &b->tun.kchunk, &b->d_sync,
+    void* args[] = {&b->d_models, &b->d_maps, &b->d_work, &b->d_pbeg, &b->d_limit, &nsteps, &b->tun.kchunk, &b->d_sync,
                     &b->d_status};
-    BCK(cudaLaunchCooperativeKernel((void*)k_batch, dim3(grid), dim3(32, 8), args, 0, b->st));
+    BCK(cudaLaunchCooperativeKernel((void*)k_batch, dim3(grid), dim3(32, 8), args, tma_ring_bytes<float>(), b->st));
     return FD3D_OK;
 }
 
@@ -421,7 +446,7 @@ int reset_model(fd3d_batch* b, Model& M) {
     for (double* a : zd) BCK(cudaMemsetAsync(a, 0, n2 * sizeof(double), b->st));
     long long ncell = 0;
     for (int s = 0; s < 4; ++s) ncell += d.D.s[s].ncells;
-    BCK(cudaMemsetAsync(d.X.a[0], 0, (size_t)ncell * AX_N * sizeof(float), b->st));
+    BCK(cudaMemsetAsync(d.X.a[0], 0, (size_t)aux_cells32(ncell) * AX_N * sizeof(float), b->st));
     k_model_reset<<<(unsigned)((n2 + 255) / 256), 256, 0, b->st>>>(d, (int)n2);
     BCK(cudaGetLastError());
     M.steps = 0;
@@ -449,6 +474,7 @@ int fd3d_batch_create(size_t arena_bytes, int max_models, fd3d_batch** out) {
     b->arena.init(arena_bytes);
     b->models.resize(max_models);
     if (cudaMalloc(&b->d_models, sizeof(ModelDev) * max_models) != cudaSuccess ||
+        cudaMalloc(&b->d_maps, sizeof(ModelMaps) * max_models) != cudaSuccess ||
         cudaMalloc(&b->d_limit, sizeof(int) * max_models) != cudaSuccess ||
         cudaMalloc(&b->d_pbeg, sizeof(int) * (NPHASE + 1)) != cudaSuccess ||
         cudaMalloc(&b->d_sync, sizeof(BatchSync)) != cudaSuccess || cudaMalloc(&b->d_status, sizeof(int)) != cudaSuccess) {
@@ -458,7 +484,9 @@ int fd3d_batch_create(size_t arena_bytes, int max_models, fd3d_batch** out) {
     cudaMemset(b->d_status, 0, sizeof(int));
     cudaEventCreate(&b->ev0);
     cudaEventCreate(&b->ev1);
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b->max_active, k_batch, 256, 0) != cudaSuccess || b->max_active < 1) {
+    if (cudaFuncSetAttribute(k_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, tma_ring_bytes<float>()) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b->max_active, k_batch, 256, tma_ring_bytes<float>()) != cudaSuccess ||
+        b->max_active < 1 || !tensor_map_encoder()) {
         cudaGetLastError();
         return fail(FD3D_ERR_CUDA);
     }
@@ -473,6 +501,7 @@ int fd3d_batch_destroy(fd3d_batch* b) {
     if (b->st) cudaStreamSynchronize(b->st);
     cudaFree(b->arena_base);
     cudaFree(b->d_models);
+    cudaFree(b->d_maps);
     cudaFree(b->d_limit);
     cudaFree(b->d_pbeg);
     cudaFree(b->d_sync);
@@ -548,8 +577,8 @@ int fd3d_batch_add(fd3d_batch* b, const fd3d_params* pin, const double* lam_k, c
     for (double** a : dq) *a = bp.take<double>(n2);
     long long ncell = 0;
     for (int s = 0; s < 4; ++s) ncell += d.D.s[s].ncells;
-    float* aux = bp.take<float>((size_t)ncell * AX_N);
-    for (int a = 0; a < AX_N; ++a) d.X.a[a] = aux + (size_t)a * ncell;
+    float* aux = bp.take<float>((size_t)aux_cells32(ncell) * AX_N);
+    pml_aux_bind(d.X, aux, ncell);
     float* dprof = bp.take<float>(prof.size());
     d.X.prof = dprof;
     const size_t plane = (size_t)(p.nxt - 2 * p.nabc) * (p.nzt - p.nfs - p.nabc);
@@ -587,6 +616,9 @@ int fd3d_batch_add(fd3d_batch* b, const fd3d_params* pin, const double* lam_k, c
     M.live = true;
     rc = reset_model(b, M);
     if (rc) { b->arena.release(M.off, M.bytes); return rc; }
+    ModelMaps mm;
+    if (!make_interior_maps<float>(d.g, d.f, mm.v, mm.s)) { b->arena.release(M.off, M.bytes); return FD3D_ERR_CUDA; }
+    BCK(cudaMemcpyAsync(b->d_maps + m, &mm, sizeof(ModelMaps), cudaMemcpyHostToDevice, b->st));
     BCK(cudaMemcpyAsync(b->d_models + m, &M.dev, sizeof(ModelDev), cudaMemcpyHostToDevice, b->st));
     BCK(cudaStreamSynchronize(b->st));
     b->models[m] = M;

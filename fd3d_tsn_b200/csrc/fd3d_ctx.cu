@@ -132,8 +132,8 @@ struct Ctx : CtxBase {
         long long ncell = 0;
         for (int s = 0; s < 4; ++s) ncell += D.s[s].ncells;
         T* pool = nullptr;
-        if (dalloc(&pool, (size_t)ncell * AX_N)) return FD3D_ERR_NOMEM;
-        for (int a = 0; a < AX_N; ++a) X.a[a] = pool + (size_t)a * ncell;
+        if (dalloc(&pool, (size_t)aux_cells32(ncell) * AX_N)) return FD3D_ERR_NOMEM;
+        pml_aux_bind(X, pool, ncell);
         T* dprof = nullptr;
         if (dalloc(&dprof, prof.size())) return FD3D_ERR_NOMEM;
         CK(cudaMemcpyAsync(dprof, prof.data(), prof.size() * sizeof(T), cudaMemcpyHostToDevice, st));
@@ -306,7 +306,7 @@ struct Ctx : CtxBase {
         }
         long long ncell = 0;
         for (int s = 0; s < 4; ++s) ncell += D.s[s].ncells;
-        CK(cudaMemsetAsync(X.a[0], 0, (size_t)ncell * AX_N * sizeof(T), st));
+        CK(cudaMemsetAsync(X.a[0], 0, (size_t)aux_cells32(ncell) * AX_N * sizeof(T), st));
         CK(cudaMemsetAsync(it_dev, 0, sizeof(int), st));
         CK(cudaMemsetAsync(status, 0, sizeof(int), st));
         CK(cudaStreamSynchronize(st));

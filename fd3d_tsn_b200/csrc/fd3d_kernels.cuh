@@ -154,11 +154,31 @@ struct PmlDesc {
     long long cum[5];  // cumulative thread counts (u/w range) over the strips
 };
 
+// PML auxiliary components are stored in blocks of 32 cells: within a block the 32
+// values of one component are contiguous and the components of a group follow each
+// other, so the 9 velocity (or 15 stress) components a warp updates for its 32 cells
+// form one contiguous span instead of 9 (15) separate streams.  a[c] points at the
+// group base plus 32 * (index of c in its group); the cell index q of a strip cell
+// (Strip::base + local) maps to the element offset aux_blk(q, group size).
+constexpr int AUX_NV = 9, AUX_NS = 15;  // u,v,w splits / xx,yy,zz,xy,xz,yz splits
+__host__ __device__ __forceinline__ long long aux_blk(long long q, int ncomp) {
+    return (q >> 5) * (32LL * ncomp) + (q & 31);
+}
+inline long long aux_cells32(long long ncell) { return (ncell + 31) & ~31LL; }
+
 template <class T>
 struct PmlAux {
-    T* a[AX_N];         // each pool covers all 4 strips (Strip::base offsets)
+    T* a[AX_N];         // component bases (see aux_blk); both groups cover all 4 strips
     const T* prof;      // damping profiles
 };
+
+// carve the two groups out of one pool of aux_cells32(ncell) * AX_N elements
+template <class T>
+inline void pml_aux_bind(PmlAux<T>& X, T* pool, long long ncell) {
+    const long long n32 = aux_cells32(ncell);
+    for (int c = 0; c < AX_N; ++c)
+        X.a[c] = c < AUX_NV ? pool + 32LL * c : pool + n32 * AUX_NV + 32LL * (c - AUX_NV);
+}
 
 // locate strip and (i,j,k) of compact thread index t (u/w loop range of every strip)
 __device__ __forceinline__ bool pml_locate(const PmlDesc& D, long long t, int& s, int& i, int& j, int& k,
@@ -181,12 +201,13 @@ __device__ __forceinline__ bool pml_locate(const PmlDesc& D, long long t, int& s
 
 // pml_uvw: split-field PML velocity in the 4 strips (fd3d_deriv.f90:1927-2218)
 template <class T>
-__device__ __forceinline__ void vel_pml_body(Grid g, Fields<T> f, PmlDesc D, PmlAux<T> X, StepConst<T> c, int bx_, int by_, int bz_) {
+__device__ __forceinline__ void vel_pml_body(Grid g, Fields<T> f, const PmlDesc& D, const PmlAux<T>& X, StepConst<T> c, int bx_, int by_, int bz_) {
     // linear index; the CTA may be 256 x 1 (single model) or 32 x 8 (persistent batch)
     const long long t = (long long)bx_ * (blockDim.x * blockDim.y) + threadIdx.y * blockDim.x + threadIdx.x;
     int s, i, j, k;
     long long qa;
     if (!pml_locate(D, t, s, i, j, k, qa)) return;
+    const long long qv = aux_blk(qa, AUX_NV);  // velocity components of this cell
     const Strip& S = D.s[s];
     const int i2 = i - S.nxb, j2 = j - S.nyb, k2 = k - S.nzb;
     const T ox = X.prof[S.ox_off + i2], oxS = X.prof[S.oxS_off + i2];
@@ -197,11 +218,11 @@ __device__ __forceinline__ void vel_pml_body(Grid g, Fields<T> f, PmlDesc D, Pml
     const T d = f.d[p], dt = c.dt, dh = c.dh;
     const T xx0 = f.xx[p], xx1 = f.xx[p - 1], xy0 = f.xy[p], xy1 = f.xy[p - sy], xz0 = f.xz[p], xz1 = f.xz[p - sz];
     const T xz2 = f.xz[p + 1], yz0 = f.yz[p], yz1 = f.yz[p - sy], zz0 = f.zz[p], zz1 = f.zz[p + sz];
-    T u0 = X.a[AX_U0][qa], u1 = X.a[AX_U1][qa], u2 = X.a[AX_U2][qa];
-    T w0 = X.a[AX_W0][qa], w1 = X.a[AX_W1][qa], w2 = X.a[AX_W2][qa];
+    T u0 = X.a[AX_U0][qv], u1 = X.a[AX_U1][qv], u2 = X.a[AX_U2][qv];
+    T w0 = X.a[AX_W0][qv], w1 = X.a[AX_W1][qv], w2 = X.a[AX_W2][qv];
     T v0 = 0, v1 = 0, v2 = 0, xy2 = 0, yy0 = 0, yy1 = 0, yz2 = 0, vold = 0;
     if (dov) {
-        v0 = X.a[AX_V0][qa]; v1 = X.a[AX_V1][qa]; v2 = X.a[AX_V2][qa];
+        v0 = X.a[AX_V0][qv]; v1 = X.a[AX_V1][qv]; v2 = X.a[AX_V2][qv];
         xy2 = f.xy[p + 1]; yy0 = f.yy[p + sy]; yy1 = f.yy[p]; yz2 = f.yz[p - sz];
         if (j == g.nyt - 1) vold = f.v[p];
     }
@@ -218,13 +239,13 @@ __device__ __forceinline__ void vel_pml_body(Grid g, Fields<T> f, PmlDesc D, Pml
         pt = v1 * ((T)1 - oy) + r * (yy0 - yy1) / dh;  v1 = pt / ((T)1 + oy);
         pt = v2 * ((T)1 - oz) + r * (yz0 - yz2) / dh;  v2 = pt / ((T)1 + oz);
     }
-    X.a[AX_U0][qa] = u0; X.a[AX_U1][qa] = u1; X.a[AX_U2][qa] = u2;
-    X.a[AX_W0][qa] = w0; X.a[AX_W1][qa] = w1; X.a[AX_W2][qa] = w2;
+    X.a[AX_U0][qv] = u0; X.a[AX_U1][qv] = u1; X.a[AX_U2][qv] = u2;
+    X.a[AX_W0][qv] = w0; X.a[AX_W1][qv] = w1; X.a[AX_W2][qv] = w2;
     f.u[p] = u0 + u1 + u2;
     f.w[p] = w0 + w1 + w2;
     if (dov) {
         if (j == g.nyt - 1) f.v[p + sy] = vold;  // bnd2d mirror of the value before this update
-        X.a[AX_V0][qa] = v0; X.a[AX_V1][qa] = v1; X.a[AX_V2][qa] = v2;
+        X.a[AX_V0][qv] = v0; X.a[AX_V1][qv] = v1; X.a[AX_V2][qv] = v2;
         f.v[p] = v0 + v1 + v2;
     }
 }
@@ -354,12 +375,13 @@ __device__ __forceinline__ void str_fault_body(Grid g, Fields<T> f, Fault<T> q, 
 
 // pml_xyz in the 4 strips (fd3d_deriv.f90:2304-2992)
 template <class T>
-__device__ __forceinline__ void str_pml_body(Grid g, Fields<T> f, PmlDesc D, PmlAux<T> X, StepConst<T> c, int bx_, int by_, int bz_) {
+__device__ __forceinline__ void str_pml_body(Grid g, Fields<T> f, const PmlDesc& D, const PmlAux<T>& X, StepConst<T> c, int bx_, int by_, int bz_) {
     // linear index; the CTA may be 256 x 1 (single model) or 32 x 8 (persistent batch)
     const long long t = (long long)bx_ * (blockDim.x * blockDim.y) + threadIdx.y * blockDim.x + threadIdx.x;
     int s, i, j, k;
     long long qa;
     if (!pml_locate(D, t, s, i, j, k, qa)) return;
+    const long long qs = aux_blk(qa, AUX_NS);  // stress components of this cell
     const Strip& S = D.s[s];
     const int i2 = i - S.nxb, j2 = j - S.nyb, k2 = k - S.nzb;
     const T ox = X.prof[S.ox_off + i2], oxS = X.prof[S.oxS_off + i2];
@@ -376,13 +398,13 @@ __device__ __forceinline__ void str_pml_body(Grid g, Fields<T> f, PmlDesc D, Pml
     const T up = f.u[p], ux = f.u[p + 1], uz = f.u[p + sz];
     const T vp = f.v[p], vy = f.v[p - sy];
     const T wp = f.w[p], wz = f.w[p - sz], wx = f.w[p - 1];
-    T x0 = X.a[AX_XX0][qa], x1 = X.a[AX_XX1][qa], x2 = X.a[AX_XX2][qa];
-    T y0 = X.a[AX_YY0][qa], y1 = X.a[AX_YY1][qa], y2 = X.a[AX_YY2][qa];
-    T z0 = X.a[AX_ZZ0][qa], z1 = X.a[AX_ZZ1][qa], z2 = X.a[AX_ZZ2][qa];
-    T q0 = X.a[AX_XZ0][qa], q1 = X.a[AX_XZ1][qa];
+    T x0 = X.a[AX_XX0][qs], x1 = X.a[AX_XX1][qs], x2 = X.a[AX_XX2][qs];
+    T y0 = X.a[AX_YY0][qs], y1 = X.a[AX_YY1][qs], y2 = X.a[AX_YY2][qs];
+    T z0 = X.a[AX_ZZ0][qs], z1 = X.a[AX_ZZ1][qs], z2 = X.a[AX_ZZ2][qs];
+    T q0 = X.a[AX_XZ0][qs], q1 = X.a[AX_XZ1][qs];
     T e0 = 0, e1 = 0, h0 = 0, h1 = 0, my = 0, md = 0, uy = 0, vx = 0, vz = 0, wy = 0, xyo = 0, yzo = 0;
     if (dxy) {
-        e0 = X.a[AX_XY0][qa]; e1 = X.a[AX_XY1][qa]; h0 = X.a[AX_YZ0][qa]; h1 = X.a[AX_YZ1][qa];
+        e0 = X.a[AX_XY0][qs]; e1 = X.a[AX_XY1][qs]; h0 = X.a[AX_YZ0][qs]; h1 = X.a[AX_YZ1][qs];
         my = f.mu[p + sy]; md = f.mu[p + 1 + sy + sz];
         uy = f.u[p + sy]; vx = f.v[p - 1]; vz = f.v[p + sz]; wy = f.w[p + sy];
         if (j == g.nyt - 1) { xyo = f.xy[p]; yzo = f.yz[p]; }
@@ -412,22 +434,22 @@ __device__ __forceinline__ void str_pml_body(Grid g, Fields<T> f, PmlDesc D, Pml
         pt = h0 * ((T)1 - ozxz) + dt * xmu * (vz - vp) / dh; h0 = pt / ((T)1 + ozxz);
         pt = h1 * ((T)1 - oyxy) + dt * xmu * (wy - wp) / dh; h1 = pt / ((T)1 + oyxy);
     }
-    X.a[AX_XX0][qa] = x0; X.a[AX_XX1][qa] = x1; X.a[AX_XX2][qa] = x2;
-    X.a[AX_YY0][qa] = y0; X.a[AX_YY1][qa] = y1; X.a[AX_YY2][qa] = y2;
-    X.a[AX_ZZ0][qa] = z0; X.a[AX_ZZ1][qa] = z1; X.a[AX_ZZ2][qa] = z2;
+    X.a[AX_XX0][qs] = x0; X.a[AX_XX1][qs] = x1; X.a[AX_XX2][qs] = x2;
+    X.a[AX_YY0][qs] = y0; X.a[AX_YY1][qs] = y1; X.a[AX_YY2][qs] = y2;
+    X.a[AX_ZZ0][qs] = z0; X.a[AX_ZZ1][qs] = z1; X.a[AX_ZZ2][qs] = z2;
     f.xx[p] = x0 + x1 + x2;
     f.yy[p] = y0 + y1 + y2;
     f.zz[p] = z0 + z1 + z2;
     f.xz[p] = q0 + q1;
-    X.a[AX_XZ0][qa] = top ? (T)0 : q0;  // xz/yz aux zeroed at the top row (strips 1-3)
-    X.a[AX_XZ1][qa] = top ? (T)0 : q1;
+    X.a[AX_XZ0][qs] = top ? (T)0 : q0;  // xz/yz aux zeroed at the top row (strips 1-3)
+    X.a[AX_XZ1][qs] = top ? (T)0 : q1;
     if (dxy) {
         if (j == g.nyt - 1) { f.xy[p + sy] = xyo; f.yz[p + sy] = yzo; }  // strbnd mirror
-        X.a[AX_XY0][qa] = e0; X.a[AX_XY1][qa] = e1;
+        X.a[AX_XY0][qs] = e0; X.a[AX_XY1][qs] = e1;
         f.xy[p] = e0 + e1;
         f.yz[p] = h0 + h1;
-        X.a[AX_YZ0][qa] = top ? (T)0 : h0;
-        X.a[AX_YZ1][qa] = top ? (T)0 : h1;
+        X.a[AX_YZ0][qs] = top ? (T)0 : h0;
+        X.a[AX_YZ1][qs] = top ? (T)0 : h1;
     }
 }
 
@@ -604,7 +626,7 @@ struct HistDesc {
 
 // output planes, stations, history ring (fd3d_theo.f90:413-467); non-finite check
 template <class T>
-__device__ __forceinline__ void output_body(Grid g, Fields<T> f, Fault<T> q, int law, const int* it_dev, HistDesc h, int* status, int bx_, int by_, int bz_) {
+__device__ __forceinline__ void output_body(Grid g, Fields<T> f, Fault<T> q, int law, const int* it_dev, const HistDesc& h, int* status, int bx_, int by_, int bz_) {
     const int ii = bx_ * blockDim.x + threadIdx.x;
     const int kk = by_ * blockDim.y + threadIdx.y;
     const int it = *it_dev;
@@ -680,7 +702,8 @@ __global__ void k_vel_fault(Grid g, Fields<T> f, Fault<T> q, StepConst<T> c, int
 }
 
 template <class T>
-__global__ void __launch_bounds__(256) k_vel_pml(Grid g, Fields<T> f, PmlDesc D, PmlAux<T> X, StepConst<T> c) {
+__global__ void __launch_bounds__(256) k_vel_pml(Grid g, Fields<T> f, const __grid_constant__ PmlDesc D,
+                                                  const __grid_constant__ PmlAux<T> X, StepConst<T> c) {
     vel_pml_body<T>(g, f, D, X, c, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
@@ -695,7 +718,8 @@ __global__ void k_str_fault(Grid g, Fields<T> f, Fault<T> q, StepConst<T> c) {
 }
 
 template <class T>
-__global__ void __launch_bounds__(256) k_str_pml(Grid g, Fields<T> f, PmlDesc D, PmlAux<T> X, StepConst<T> c) {
+__global__ void __launch_bounds__(256) k_str_pml(Grid g, Fields<T> f, const __grid_constant__ PmlDesc D,
+                                                  const __grid_constant__ PmlAux<T> X, StepConst<T> c) {
     str_pml_body<T>(g, f, D, X, c, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
@@ -716,7 +740,8 @@ __global__ void k_friction(Grid g, Fields<T> f, Fault<T> q, StepConst<T> c, int 
 }
 
 template <class T>
-__global__ void k_output(Grid g, Fields<T> f, Fault<T> q, int law, const int* it_dev, HistDesc h, int* status) {
+__global__ void k_output(Grid g, Fields<T> f, Fault<T> q, int law, const int* it_dev, const __grid_constant__ HistDesc h,
+                         int* status) {
     output_body<T>(g, f, q, law, it_dev, h, status, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 

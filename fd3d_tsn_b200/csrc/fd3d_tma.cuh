@@ -91,58 +91,70 @@ __device__ __forceinline__ void vel_issue(const VelMaps& M, T* slot, uint32_t ba
     tma_load_3d(smem_addr(slot + VelSlot::W), &M.w, x0, y0, z, bar);
 }
 
-// wait (bounded) for every plane in [k0, ke] that was issued into the ring, then return
-__device__ __forceinline__ void tma_drain(const uint64_t* bars, int k0, int ke, int kb) {
-    for (int k = k0; k <= ke && k < k0 + TMA_NS; ++k) {
-        const int n = k - kb;
-        mbar_wait(smem_addr(&bars[n % TMA_NS]), (uint32_t)((n / TMA_NS) & 1));
-    }
-}
+// Ring bookkeeping across the tiles one CTA processes: the n-th plane a CTA ever puts
+// through its ring uses slot n % TMA_NS and mbarrier phase (n / TMA_NS) & 1.  A tile
+// consumes every plane it issued, so `pc` (planes issued so far) is all that carries over.
+__device__ __forceinline__ int ring_slot(unsigned n) { return (int)(n % TMA_NS); }
+__device__ __forceinline__ uint32_t ring_parity(unsigned n) { return (n / TMA_NS) & 1u; }
 
-template <class T>
-__global__ void __launch_bounds__(256) k_vel_interior_tma(const __grid_constant__ VelMaps M, Grid g, Fields<T> f,
-                                                           StepConst<T> c, int kchunk, int* status) {
-    extern __shared__ __align__(128) unsigned char smem_raw[];
-    // TMA destinations must start on 128 bytes: round the dynamic base up (128 spare bytes)
-    T* ring = reinterpret_cast<T*>(smem_raw + ((128u - (smem_addr(smem_raw) & 127u)) & 127u));
-    __shared__ __align__(8) uint64_t bars[TMA_NS];
-    const int tx = threadIdx.x, ty = threadIdx.y;
-    const int i0 = g.nabc + 1 + blockIdx.x * 32, j0 = g.nabc + 1 + blockIdx.y * 8;
-    const int i = i0 + tx, j = j0 + ty;
-    const bool act = (i <= g.nxt - g.nabc) && (j <= g.nyt - 2);
-    const int kb = g.nabc + 1 + blockIdx.z * kchunk;
-    const int ke = min(kb + kchunk - 1, g.ks());
-    const int x0 = g.off + i0 - 1, y0 = j0 - 1;  // tensor coordinates of the tile origin
-    const bool leader = (tx == 0 && ty == 0);
-    if (leader) {
+__device__ __forceinline__ void tma_ring_init(uint64_t* bars) {
+    if (threadIdx.x == 0 && threadIdx.y == 0) {
         for (int s = 0; s < TMA_NS; ++s) mbar_init(smem_addr(&bars[s]), 1);
         fence_mbar_init();
     }
     __syncthreads();
+}
+
+// wait (bounded) for every plane in [k0, ke] of the current tile that was issued, then return
+__device__ __forceinline__ void tma_drain_pc(const uint64_t* bars, unsigned pc, int k0, int ke, int kb) {
+    for (int k = k0; k <= ke && k < k0 + TMA_NS; ++k) {
+        const unsigned n = pc + (unsigned)(k - kb);
+        mbar_wait(smem_addr(&bars[ring_slot(n)]), ring_parity(n));
+    }
+}
+
+// One 32 x 8 x kchunk tile of the velocity sweep through the ring.  Returns false if a
+// wait timed out (ST_TIMEOUT is recorded; the caller stops).
+template <class T>
+__device__ __forceinline__ bool vel_interior_tma_body(const VelMaps& M, const Grid& g, const Fields<T>& f,
+                                                      const StepConst<T>& c, int kchunk, int bx_, int by_, int bz_,
+                                                      T* ring, uint64_t* bars, unsigned& pc, int* status) {
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    const int i0 = g.nabc + 1 + bx_ * 32, j0 = g.nabc + 1 + by_ * 8;
+    const int i = i0 + tx, j = j0 + ty;
+    const bool act = (i <= g.nxt - g.nabc) && (j <= g.nyt - 2);
+    const int kb = g.nabc + 1 + bz_ * kchunk;
+    const int ke = min(kb + kchunk - 1, g.ks());
+    const int x0 = g.off + i0 - 1, y0 = j0 - 1;  // tensor coordinates of the tile origin
+    const bool leader = (tx == 0 && ty == 0);
+    const unsigned p0 = pc;
     if (leader)
-        for (int k = kb; k <= min(ke, kb + TMA_NS - 1); ++k)
-            vel_issue<T>(M, ring + (size_t)((k - kb) % TMA_NS) * VelSlot::ELEMS, smem_addr(&bars[(k - kb) % TMA_NS]),
-                         x0, y0, k);
+        for (int k = kb; k <= min(ke, kb + TMA_NS - 1); ++k) {
+            const unsigned n = p0 + (unsigned)(k - kb);
+            vel_issue<T>(M, ring + (size_t)ring_slot(n) * VelSlot::ELEMS, smem_addr(&bars[ring_slot(n)]), x0, y0, k);
+        }
     // z queues of the own column (plain loads, one plane ahead)
     const int ic = min(i, g.nxt), jc = min(j, g.nyt);
     const long long sz = g.plane;
-    const long long pc = g.at(ic, jc, kb);
+    const long long pcol = g.at(ic, jc, kb);
     const T* __restrict__ zz = f.zz; const T* __restrict__ xz = f.xz; const T* __restrict__ yz = f.yz;
-    T zq0, zq1 = zz[pc - sz], zq2 = zz[pc], zq3 = zz[pc + sz], nz = zz[pc + 2 * sz];
-    T xq0, xq1 = xz[pc - 2 * sz], xq2 = xz[pc - sz], xq3 = xz[pc], nx = xz[pc + sz];
-    T yq0, yq1 = yz[pc - 2 * sz], yq2 = yz[pc - sz], yq3 = yz[pc], ny = yz[pc + sz];
+    T zq0, zq1 = zz[pcol - sz], zq2 = zz[pcol], zq3 = zz[pcol + sz], nz = zz[pcol + 2 * sz];
+    T xq0, xq1 = xz[pcol - 2 * sz], xq2 = xz[pcol - sz], xq3 = xz[pcol], nx = xz[pcol + sz];
+    T yq0, yq1 = yz[pcol - 2 * sz], yq2 = yz[pcol - sz], yq3 = yz[pcol], ny = yz[pcol + sz];
     const T c1 = c.c1, c2 = c.c2, dth = c.dth;
     for (int k = kb; k <= ke; ++k) {
-        const int n = k - kb, s = n % TMA_NS;
-        const long long pk = pc + (long long)n * sz;
+        const int n = k - kb;
+        const unsigned gn = p0 + (unsigned)n;
+        const int s = ring_slot(gn);
+        const long long pk = pcol + (long long)n * sz;
         zq0 = zq1; zq1 = zq2; zq2 = zq3; zq3 = nz;
         xq0 = xq1; xq1 = xq2; xq2 = xq3; xq3 = nx;
         yq0 = yq1; yq1 = yq2; yq2 = yq3; yq3 = ny;
         if (k < ke) { nz = zz[pk + 3 * sz]; nx = xz[pk + 2 * sz]; ny = yz[pk + 2 * sz]; }
-        if (!mbar_wait(smem_addr(&bars[s]), (uint32_t)((n / TMA_NS) & 1))) {
+        if (!mbar_wait(smem_addr(&bars[s]), ring_parity(gn))) {
             atomicOr(status, ST_TIMEOUT);
-            tma_drain(bars, k, ke, kb);
-            return;
+            tma_drain_pc(bars, p0, k, ke, kb);
+            return false;
         }
         const T* sl = ring + (size_t)s * VelSlot::ELEMS;
         if (act) {
@@ -169,6 +181,20 @@ __global__ void __launch_bounds__(256) k_vel_interior_tma(const __grid_constant_
             vel_issue<T>(M, ring + (size_t)s * VelSlot::ELEMS, smem_addr(&bars[s]), x0, y0, k + TMA_NS);
         }
     }
+    pc = p0 + (unsigned)(ke - kb + 1);
+    return true;
+}
+
+template <class T>
+__global__ void __launch_bounds__(256) k_vel_interior_tma(const __grid_constant__ VelMaps M, Grid g, Fields<T> f,
+                                                           StepConst<T> c, int kchunk, int* status) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    // TMA destinations must start on 128 bytes: round the dynamic base up (128 spare bytes)
+    T* ring = reinterpret_cast<T*>(smem_raw + ((128u - (smem_addr(smem_raw) & 127u)) & 127u));
+    __shared__ __align__(8) uint64_t bars[TMA_NS];
+    tma_ring_init(bars);
+    unsigned pc = 0;
+    vel_interior_tma_body<T>(M, g, f, c, kchunk, blockIdx.x, blockIdx.y, blockIdx.z, ring, bars, pc, status);
 }
 
 // Stress slot layout (elements)
@@ -200,42 +226,38 @@ __device__ __forceinline__ void str_issue(const StrMaps& M, T* slot, uint32_t ba
 }
 
 template <class T>
-__global__ void __launch_bounds__(256) k_str_interior_tma(const __grid_constant__ StrMaps M, Grid g, Fields<T> f,
-                                                           StepConst<T> c, int kchunk, int* status) {
-    extern __shared__ __align__(128) unsigned char smem_raw[];
-    // TMA destinations must start on 128 bytes: round the dynamic base up (128 spare bytes)
-    T* ring = reinterpret_cast<T*>(smem_raw + ((128u - (smem_addr(smem_raw) & 127u)) & 127u));
-    __shared__ __align__(8) uint64_t bars[TMA_NS];
+__device__ __forceinline__ bool str_interior_tma_body(const StrMaps& M, const Grid& g, const Fields<T>& f,
+                                                      const StepConst<T>& c, int kchunk, int bx_, int by_, int bz_,
+                                                      T* ring, uint64_t* bars, unsigned& pc, int* status) {
     const int tx = threadIdx.x, ty = threadIdx.y;
-    const int i0 = g.nabc + 1 + blockIdx.x * 32, j0 = g.nabc + 1 + blockIdx.y * 8;
+    const int i0 = g.nabc + 1 + bx_ * 32, j0 = g.nabc + 1 + by_ * 8;
     const int i = i0 + tx, j = j0 + ty;
     const bool act = (i <= g.nxt - g.nabc) && (j <= g.nyt - 2);
-    const int kb = g.nabc + 1 + blockIdx.z * kchunk;
+    const int kb = g.nabc + 1 + bz_ * kchunk;
     const int ke = min(kb + kchunk - 1, g.ks());
     const int x0 = g.off + i0 - 1, y0 = j0 - 1;
     const bool leader = (tx == 0 && ty == 0);
-    if (leader) {
-        for (int s = 0; s < TMA_NS; ++s) mbar_init(smem_addr(&bars[s]), 1);
-        fence_mbar_init();
-    }
-    __syncthreads();
+    const unsigned p0 = pc;
     if (leader)
-        for (int k = kb; k <= min(ke, kb + TMA_NS - 1); ++k)
-            str_issue<T>(M, ring + (size_t)((k - kb) % TMA_NS) * StrSlot::ELEMS, smem_addr(&bars[(k - kb) % TMA_NS]),
-                         x0, y0, k);
+        for (int k = kb; k <= min(ke, kb + TMA_NS - 1); ++k) {
+            const unsigned n = p0 + (unsigned)(k - kb);
+            str_issue<T>(M, ring + (size_t)ring_slot(n) * StrSlot::ELEMS, smem_addr(&bars[ring_slot(n)]), x0, y0, k);
+        }
     const int ic = min(i, g.nxt - 1), jc = min(j, g.nyt - 1);  // keeps the (i+1,j+1) tap in range
     const long long sy = g.px, sz = g.plane;
-    const long long pc = g.at(ic, jc, kb);
+    const long long pcol = g.at(ic, jc, kb);
     const T* __restrict__ u = f.u; const T* __restrict__ v = f.v; const T* __restrict__ w = f.w;
     const T* __restrict__ mu = f.mu;
-    T uq0, uq1 = u[pc - sz], uq2 = u[pc], uq3 = u[pc + sz], nu = u[pc + 2 * sz];
-    T vq0, vq1 = v[pc - sz], vq2 = v[pc], vq3 = v[pc + sz], nv = v[pc + 2 * sz];
-    T wq0, wq1 = w[pc - 2 * sz], wq2 = w[pc - sz], wq3 = w[pc], nw = w[pc + sz];
-    T mq1 = mu[pc + sz], pmd = mu[pc + 1 + sy + sz];
+    T uq0, uq1 = u[pcol - sz], uq2 = u[pcol], uq3 = u[pcol + sz], nu = u[pcol + 2 * sz];
+    T vq0, vq1 = v[pcol - sz], vq2 = v[pcol], vq3 = v[pcol + sz], nv = v[pcol + 2 * sz];
+    T wq0, wq1 = w[pcol - 2 * sz], wq2 = w[pcol - sz], wq3 = w[pcol], nw = w[pcol + sz];
+    T mq1 = mu[pcol + sz], pmd = mu[pcol + 1 + sy + sz];
     const T c1 = c.c1, c2 = c.c2, dth = c.dth;
     for (int k = kb; k <= ke; ++k) {
-        const int n = k - kb, s = n % TMA_NS;
-        const long long pk = pc + (long long)n * sz;
+        const int n = k - kb;
+        const unsigned gn = p0 + (unsigned)n;
+        const int s = ring_slot(gn);
+        const long long pk = pcol + (long long)n * sz;
         uq0 = uq1; uq1 = uq2; uq2 = uq3; uq3 = nu;
         vq0 = vq1; vq1 = vq2; vq2 = vq3; vq3 = nv;
         wq0 = wq1; wq1 = wq2; wq2 = wq3; wq3 = nw;
@@ -245,10 +267,10 @@ __global__ void __launch_bounds__(256) k_str_interior_tma(const __grid_constant_
             nu = u[pn + 2 * sz]; nv = v[pn + 2 * sz]; nw = w[pn + sz];
             mq1 = mu[pn + sz]; pmd = mu[pn + 1 + sy + sz];
         }
-        if (!mbar_wait(smem_addr(&bars[s]), (uint32_t)((n / TMA_NS) & 1))) {
+        if (!mbar_wait(smem_addr(&bars[s]), ring_parity(gn))) {
             atomicOr(status, ST_TIMEOUT);
-            tma_drain(bars, k, ke, kb);
-            return;
+            tma_drain_pc(bars, p0, k, ke, kb);
+            return false;
         }
         const T* sl = ring + (size_t)s * StrSlot::ELEMS;
         if (act) {
@@ -280,6 +302,26 @@ __global__ void __launch_bounds__(256) k_str_interior_tma(const __grid_constant_
             str_issue<T>(M, ring + (size_t)s * StrSlot::ELEMS, smem_addr(&bars[s]), x0, y0, k + TMA_NS);
         }
     }
+    pc = p0 + (unsigned)(ke - kb + 1);
+    return true;
+}
+
+template <class T>
+__global__ void __launch_bounds__(256) k_str_interior_tma(const __grid_constant__ StrMaps M, Grid g, Fields<T> f,
+                                                           StepConst<T> c, int kchunk, int* status) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    // TMA destinations must start on 128 bytes: round the dynamic base up (128 spare bytes)
+    T* ring = reinterpret_cast<T*>(smem_raw + ((128u - (smem_addr(smem_raw) & 127u)) & 127u));
+    __shared__ __align__(8) uint64_t bars[TMA_NS];
+    tma_ring_init(bars);
+    unsigned pc = 0;
+    str_interior_tma_body<T>(M, g, f, c, kchunk, blockIdx.x, blockIdx.y, blockIdx.z, ring, bars, pc, status);
+}
+
+// dynamic shared memory of a CTA that runs both sweeps through one ring
+template <class T>
+constexpr int tma_ring_bytes() {
+    return TMA_NS * (VelSlot::ELEMS > StrSlot::ELEMS ? VelSlot::ELEMS : StrSlot::ELEMS) * (int)sizeof(T) + TMA_SMEM_PAD;
 }
 
 }  // namespace fd3d
