@@ -275,12 +275,12 @@ def gpu_launches(m, steps):
     return per_step * steps
 
 
-def pinned(shape, dtype):
+def pinned(shape, dtype, order="F"):
     """Page-locked host array (cudaHostAlloc through torch)."""
     import torch
     t = torch.empty(int(np.prod(shape)), dtype=torch.float32 if dtype == np.float32 else torch.float64,
                     pin_memory=True)
-    return t.numpy().reshape(shape, order="F"), t
+    return t.numpy().reshape(shape, order=order), t
 
 
 def end_to_end(m, steps, local):
@@ -298,10 +298,12 @@ def end_to_end(m, steps, local):
     nab = m["nabc"]
     plane = (m["nxt"] - 2 * nab) * (m["nzt"] - nab - m["nfs"])
     nf = 4
-    hist, th = pinned((steps, nf, plane), np.float32)
+    hist, th = pinned((nf, steps, plane), np.float32, order="C")
     keep.append(th)
     nst = len(m.get("stations", []))
     seis = np.empty((steps, max(nst, 1), 3))
+    chunk = 16              # history records are read back every chunk of steps
+    m = dict(m, history_capacity=2 * chunk)
     s = Solver(m)           # context + fault; its medium is replaced inside the timed region
     s.run(0)
     s.sync()
@@ -309,14 +311,18 @@ def end_to_end(m, steps, local):
     t0 = time.perf_counter()
     s.upload_medium_arrays(*host, real_kind=4)
     s.upload_fault(m["fault"])
-    s.run(steps)
-    s.sync()
-    for f in range(nf):
-        rc = lib().fd3d_fetch_history(s.h, f, 0, steps, hist[:, f].ctypes.data, 4)
-        if rc:
-            raise abi.Fd3dError(rc, "fd3d_fetch_history")
-    if nst:
-        lib().fd3d_fetch_stations(s.h, 0, steps, seis.ctypes.data_as(C.POINTER(C.c_double)))
+    done = 0
+    while done < steps:
+        n = min(chunk, steps - done)
+        s.run(n)
+        s.sync()
+        for f in range(nf):
+            rc = lib().fd3d_fetch_history(s.h, f, done, n, hist[f, done:done + n].ctypes.data, 4)
+            if rc:
+                raise abi.Fd3dError(rc, "fd3d_fetch_history")
+        if nst:
+            lib().fd3d_fetch_stations(s.h, done, n, seis[done:done + n].ctypes.data_as(C.POINTER(C.c_double)))
+        done += n
     dt = time.perf_counter() - t0
     s.close()
     fault_bytes = 6 * m["nxt"] * m["nzt"] * 8
