@@ -147,6 +147,7 @@ def load_library(path: str | None = None) -> C.CDLL:
         "fd3d_kernel_times": (i, [vp, fp, C.POINTER(i)]),
         "fd3d_read_deck": (i, [C.c_char_p, C.POINTER(Params), C.POINTER(dp), C.POINTER(dp), C.POINTER(dp)]),
         "fd3d_free": (None, [vp]),
+        "fd3d_check_division": (i, [fp, i, C.POINTER(C.c_ulonglong), C.POINTER(C.c_uint)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

@@ -132,8 +132,11 @@ k_batch(const ModelDev* __restrict__ models, const ModelMaps* __restrict__ maps,
     extern __shared__ __align__(128) unsigned char smem_raw[];
     float* ring = reinterpret_cast<float*>(smem_raw + ((128u - (smem_addr(smem_raw) & 127u)) & 127u));
     __shared__ __align__(8) uint64_t bars[TMA_NS];
+    __shared__ __align__(8) uint64_t pbar;  // PML tiles staged through the ring memory
+    if (threadIdx.x == 0 && threadIdx.y == 0) mbar_init(smem_addr(&pbar), 1);
     tma_ring_init(bars);
     unsigned pc = 0;  // planes this CTA has put through its ring
+    unsigned pt = 0;  // PML tiles this CTA has staged (mbarrier phase = pt & 1)
     const unsigned nb = gridDim.x;
     for (int s = 0; s < nsteps; ++s) {
         for (int ph = 0; ph < NPHASE; ++ph) {
@@ -152,14 +155,22 @@ k_batch(const ModelDev* __restrict__ models, const ModelMaps* __restrict__ maps,
                     case W_VEL_FAULT:
                         vel_fault_body<float>(M.g, M.f, M.q, M.c, M.law, M.fs, M.it_dev, M.status, it.bx, it.by, 0);
                         break;
-                    case W_VEL_PML: vel_pml_body<float>(M.g, M.f, M.D, M.X, M.c, it.bx, 0, 0); break;
+                    case W_VEL_PML:
+                        ok = vel_pml_tile<float>(M.g, M.f, M.D, M.X, M.c, it.bx, ring, smem_addr(&pbar), pt & 1u,
+                                                 gstatus);
+                        ++pt;
+                        break;
                     case W_VEL_FS: vel_fs_body<float>(M.g, M.f, it.bx, it.by, 0); break;
                     case W_STR_INT:
                         ok = str_interior_tma_body<float>(maps[m].s, M.g, M.f, M.c, kchunk, it.bx, it.by, it.bz, ring,
                                                           bars, pc, gstatus);
                         break;
                     case W_STR_FAULT: str_fault_body<float>(M.g, M.f, M.q, M.c, it.bx, it.by, 0); break;
-                    case W_STR_PML: str_pml_body<float>(M.g, M.f, M.D, M.X, M.c, it.bx, 0, 0); break;
+                    case W_STR_PML:
+                        ok = str_pml_tile<float>(M.g, M.f, M.D, M.X, M.c, it.bx, ring, smem_addr(&pbar), pt & 1u,
+                                                 gstatus);
+                        ++pt;
+                        break;
                     case W_STR_FS: str_fs_body<float>(M.g, M.f, it.bx, it.by, 0); break;
                     case W_TRAC: traction_body<float>(M.g, M.f, M.q, M.c, it.bx, it.by, 0); break;
                     case W_FRIC: friction_body<float>(M.g, M.f, M.q, M.c, M.law, M.fs, M.it_dev, it.bx, it.by, 0); break;
@@ -173,6 +184,8 @@ k_batch(const ModelDev* __restrict__ models, const ModelMaps* __restrict__ maps,
                 }
                 __syncthreads();  // the next item may reuse the ring
             }
+            // PML write-backs of this phase complete before any CTA reads them in the next step
+            if (threadIdx.x == 0 && threadIdx.y == 0) { bulk_wait_all(); fence_proxy_async_global(); }
             if (!grid_barrier(sync, nb, gstatus)) return;
         }
     }
@@ -259,16 +272,14 @@ constexpr int NF_PLANES = 37, ND_PLANES = 11;
 
 size_t model_bytes(const fd3d_params& p, const Grid& g, const PmlDesc& D, int prof_n, int nf, int cap) {
     const size_t n2 = (size_t)p.nxt * p.nzt;
-    long long ncell = 0;
-    for (int s = 0; s < 4; ++s) ncell += D.s[s].ncells;
     const size_t plane = (size_t)(p.nxt - 2 * p.nabc) * (p.nzt - p.nfs - p.nabc);
     size_t b = 0;
     auto add = [&](size_t bytes) { b = ((b + 255) & ~(size_t)255) + bytes; };
     add((size_t)g.n3 * 12 * 4);
     for (int k = 0; k < NF_PLANES; ++k) add(n2 * 4);
     for (int k = 0; k < ND_PLANES; ++k) add(n2 * 8);
-    add((size_t)aux_cells32(ncell) * AX_N * 4);
-    add((size_t)prof_n * 4);
+    add(pml_aux_elems(D) * 4);
+    add((size_t)prof_n * sizeof(Damp<float>));
     add((size_t)cap * nf * plane * 4);
     add((size_t)cap * std::max(1, p.nstations) * 3 * 4);
     add((size_t)3 * p.nzt * 4);
@@ -444,9 +455,7 @@ int reset_model(fd3d_batch* b, Model& M) {
     for (float* a : zt) BCK(cudaMemsetAsync(a, 0, n2 * sizeof(float), b->st));
     double* zd[] = {d.q.distX, d.q.distZ, d.q.slipX, d.q.slipZ, d.q.rise};
     for (double* a : zd) BCK(cudaMemsetAsync(a, 0, n2 * sizeof(double), b->st));
-    long long ncell = 0;
-    for (int s = 0; s < 4; ++s) ncell += d.D.s[s].ncells;
-    BCK(cudaMemsetAsync(d.X.a[0], 0, (size_t)aux_cells32(ncell) * AX_N * sizeof(float), b->st));
+    BCK(cudaMemsetAsync(d.X.vel, 0, pml_aux_elems(d.D) * sizeof(float), b->st));
     k_model_reset<<<(unsigned)((n2 + 255) / 256), 256, 0, b->st>>>(d, (int)n2);
     BCK(cudaGetLastError());
     M.steps = 0;
@@ -520,7 +529,7 @@ int fd3d_batch_bytes_needed(const fd3d_params* p, size_t* bytes) {
     if (rc) return rc;
     Grid g = make_grid(*p);
     PmlDesc D;
-    std::vector<float> prof;
+    std::vector<Damp<float>> prof;
     make_pml<float>(*p, D, prof);
     const int nf = p->law == FD3D_LAW_FVW ? 5 : 4;
     const int cap = p->history_capacity > 0 ? p->history_capacity : 16;
@@ -552,7 +561,7 @@ int fd3d_batch_add(fd3d_batch* b, const fd3d_params* pin, const double* lam_k, c
     d.g = make_grid(M.p);
     d.c = make_const<float>(M.p);
     d.law = M.p.law;
-    std::vector<float> prof;
+    std::vector<Damp<float>> prof;
     make_pml<float>(M.p, d.D, prof);
     M.bytes = model_bytes(M.p, d.g, d.D, (int)prof.size(), M.nf, M.cap);
     if (!b->arena.alloc(M.bytes, &M.off)) return FD3D_ERR_NOMEM;
@@ -575,11 +584,9 @@ int fd3d_batch_add(fd3d_batch* b, const fd3d_params* pin, const double* lam_k, c
     double** dq[ND_PLANES] = {&d.q.psiX, &d.q.psiZ, &d.q.distX, &d.q.distZ, &d.q.slipX, &d.q.slipZ, &d.q.ruptime,
                               &d.q.rise, &d.q.sliptime, &d.psiX0, &d.psiZ0};
     for (double** a : dq) *a = bp.take<double>(n2);
-    long long ncell = 0;
-    for (int s = 0; s < 4; ++s) ncell += d.D.s[s].ncells;
-    float* aux = bp.take<float>((size_t)aux_cells32(ncell) * AX_N);
-    pml_aux_bind(d.X, aux, ncell);
-    float* dprof = bp.take<float>(prof.size());
+    float* aux = bp.take<float>(pml_aux_elems(d.D));
+    pml_aux_bind(d.X, aux, d.D);
+    Damp<float>* dprof = bp.take<Damp<float>>(prof.size());
     d.X.prof = dprof;
     const size_t plane = (size_t)(p.nxt - 2 * p.nabc) * (p.nzt - p.nfs - p.nabc);
     float* ring = bp.take<float>((size_t)M.cap * M.nf * plane);
@@ -612,7 +619,7 @@ int fd3d_batch_add(fd3d_batch* b, const fd3d_params* pin, const double* lam_k, c
     BCK(cudaMemcpyAsync(d.q.T0Xb, F[0].data(), n2 * sizeof(float), cudaMemcpyHostToDevice, b->st));
     BCK(cudaMemcpyAsync(d.psiZ0, pz.data(), n2 * sizeof(double), cudaMemcpyHostToDevice, b->st));
     BCK(cudaMemcpyAsync(d.psiX0, px.data(), n2 * sizeof(double), cudaMemcpyHostToDevice, b->st));
-    BCK(cudaMemcpyAsync(dprof, prof.data(), prof.size() * sizeof(float), cudaMemcpyHostToDevice, b->st));
+    BCK(cudaMemcpyAsync(dprof, prof.data(), prof.size() * sizeof(Damp<float>), cudaMemcpyHostToDevice, b->st));
     M.live = true;
     rc = reset_model(b, M);
     if (rc) { b->arena.release(M.off, M.bytes); return rc; }
@@ -814,6 +821,14 @@ int fd3d_batch_autotune(fd3d_batch* b, int steps, const char* cache_path, const 
     for (const Model& M : b->models)
         if (M.live && M.steps != 0) return FD3D_ERR_STATE;
     std::string k = key ? key : "";
+    if (!k.empty()) {  // a tuning holds for one kind of device only
+        int dev = 0;
+        cudaDeviceProp prop{};
+        BCK(cudaGetDevice(&dev));
+        BCK(cudaGetDeviceProperties(&prop, dev));
+        for (char& ch : prop.name) if (ch == '"') ch = '\'';
+        k += std::string("|") + prop.name + "|sm" + std::to_string(prop.multiProcessorCount);
+    }
     if (cache_path && !k.empty()) {
         std::ifstream in(cache_path);
         std::string line;

@@ -7,9 +7,11 @@
 //     `off` shifts the row so that i = nabc+1, the first interior column, starts on a
 //     128-byte boundary (fp32) and px (a multiple of 32) keeps every row aligned.
 //   * fault-plane arrays (i,k) at (i-1) + nxt*(k-1), the reference's own layout.
-//   * PML auxiliary arrays per strip: (ni x nj1 x nk), i fastest, as allocated by
-//     init_pml (src/fd3d_deriv.f90:1319-1410), one array per split component.
+//   * PML auxiliary (split) components of init_pml (src/fd3d_deriv.f90:1319-1410): one
+//     pool indexed by the compact cell index of the 4 strips, in 32-cell blocks per
+//     group of components (PmlAux, fd3d_kernels.cuh).
 #pragma once
+#include <cmath>
 #include <cstdint>
 #include <cuda_runtime.h>
 
@@ -37,6 +39,8 @@ struct Strip {
     long long base;                    // offset of this strip in each aux pool
     long long ncells;                  // ni*nj1*nk
     int ox_off, oxS_off, oy_off, oyS_off, oz_off, ozS_off;  // offsets into the profile table
+    float rni, rnj;                    // 1/ni, 1/(jend_uw-nyb+1) for the index split (udiv_small)
+    int fastdiv;                       // the strip's u/w range has fewer than 2^24 cells
 };
 
 // 24 split components per strip: u(3) v(3) w(3) xx(3) yy(3) zz(3) xy(2) xz(2) yz(2)
@@ -81,11 +85,69 @@ struct FvwScalars {
 template <class T>
 struct StepConst {
     T dt, dh, dth, dth2, dht, damp_s, c1, c2;
+    T rdh;                   // RN(1/dh) for div_pre (NaN: divide directly)
     double dtA, dhA, dthA;   // FP64 copies for the FP64 parts
 };
 
+// x / b rounded to nearest for a divisor b > 0 known before the launch, given
+// y = RN(1/b) formed on the host by an IEEE division.
+//
+// Method: Markstein's theorem (P. W. Markstein, "Computation of elementary functions
+// on the IBM RISC System/6000 processor", IBM J. Res. Dev. 34(1), 1990; also in
+// J.-M. Muller et al., "Handbook of Floating-Point Arithmetic", the chapter on
+// FMA-based division): if y is within half an ulp of 1/b and q within one ulp of
+// x/b, the remainder r = x - b*q is exact and RN(q + r*y) = RN(x/b).  q0 = RN(x*y)
+// can be 1.5 ulp off, so one correction step first brings it within one ulp; the
+// second step is the theorem's.  Five FP32 operations, no reciprocal
+// approximation and no branch on the common path.
+//
+// The theorem assumes that nothing under- or overflows.  For |x| outside
+// [2^-98, 2^98], NaN, infinities and a divisor outside the range checked on the host
+// (y is NaN then) the quotient is formed in FP64 and rounded to FP32: both operands
+// are exact in FP64, and rounding a quotient first to 53 bits and then to 24 (or
+// fewer, for a subnormal result) gives the directly rounded quotient because
+// 53 >= 2*24 + 2 (S. A. Figueroa, "When is double rounding innocuous?", SIGNUM
+// Newsletter 30(3), 1995).  A zero dividend returns x*y, which keeps the sign of the
+// zero as x/b does.  The result is therefore the IEEE FP32 quotient for every input;
+// an exhaustive GPU test over all 2^32 dividends (fd3d_check_division) holds it to
+// that.  (The wave field's leading edge carries long runs of tiny values, so the
+// fallback must not be the slow path of a single-precision division.)
+__device__ __forceinline__ float div_pre(float x, float b, float y) {
+    float q = __fmul_rn(x, y);
+    float r = __fmaf_rn(-q, b, x);
+    q = __fmaf_rn(r, y, q);
+    r = __fmaf_rn(-q, b, x);
+    float q2 = __fmaf_rn(r, y, q);
+    const float a = fabsf(x);
+    if (!(a >= 0x1p-98f && a <= 0x1p98f && q2 == q2))
+        q2 = (a == 0.0f && y == y) ? __fmul_rn(x, y) : __double2float_rn(__ddiv_rn((double)x, (double)b));
+    return q2;
+}
+// the FP64 build divides directly (parity build, not the fast path)
+__device__ __forceinline__ double div_pre(double x, double b, double) { return x / b; }
+
+// y = RN(1/b) for div_pre, or NaN when b is outside [2^-20, 2^20] (FP64 fallback)
+template <class T>
+inline T div_pre_recip(T b) {
+    const double ab = (double)b;
+    if (!(ab >= 0x1p-20 && ab <= 0x1p20)) return (T)NAN;
+    return (T)1 / b;
+}
+
+// n / d for n < 2^24 and 1 <= d < 2^24 with rd = RN(1/d): the float product is within
+// one of the quotient, and one remainder test each way makes it exact (a few integer
+// operations instead of a 32-bit division, which the GPU runs as a long sequence).
+__host__ __device__ __forceinline__ unsigned udiv_small(unsigned n, unsigned d, float rd, unsigned& rem) {
+    unsigned q = (unsigned)((float)n * rd);
+    int r = (int)(n - q * d);
+    if (r < 0) { --q; r += (int)d; }
+    else if (r >= (int)d) { ++q; r -= (int)d; }
+    rem = (unsigned)r;
+    return q;
+}
+
 // Device-side status word bits.
-enum { ST_NEWTON = 1, ST_NONFINITE = 2 };
+enum { ST_NEWTON = 1, ST_NONFINITE = 2, ST_TIMEOUT = 4 };
 
 #ifndef FD3D_NEWTON_MAXIT
 #define FD3D_NEWTON_MAXIT 200

@@ -49,11 +49,12 @@ struct CtxBase {
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     float last_ms = 0.f;
     bool profiling = false;
+    int pml_minb_vel = 1, pml_minb_str = 4;  // register caps of the PML sweeps (CTAs per SM)
     std::vector<cudaEvent_t> kev;   // 2 per kernel id
     float ktimes[FD3D_NKERNELS] = {0};
     int klaunch[FD3D_NKERNELS] = {0};
-    cudaGraphExec_t gexec = nullptr;
-    int gsteps = 0;
+    static constexpr int NGRAPH = 6;          // graphs of 32, 16, 8, 4, 2 and 1 steps
+    cudaGraphExec_t gexec[NGRAPH] = {};
     InteriorCfg icfg;       // interior sweep variant and CTA shape
     virtual ~CtxBase() {}
     virtual int alloc() = 0;
@@ -83,18 +84,30 @@ struct Ctx : CtxBase {
     std::vector<double> psiX0, psiZ0;  // initial FVW state, restored by reset
     size_t elem() const override { return sizeof(T); }
 
+    // Device memory of the context: one allocation (zeroed once) carved into 256-byte
+    // aligned arrays; a request beyond it gets its own allocation.
+    char* block = nullptr;
+    size_t block_bytes = 0, block_used = 0;
+    static size_t carve(size_t bytes) { return (std::max<size_t>(bytes, 1) + 255) & ~(size_t)255; }
     template <class U> int dalloc(U** ptr, size_t n) {
+        const size_t bytes = carve(n * sizeof(U));
+        if (block && block_used + bytes <= block_bytes) {
+            *ptr = (U*)(block + block_used);
+            block_used += bytes;
+            return 0;
+        }
         void* v = nullptr;
-        CK(cudaMalloc(&v, std::max<size_t>(n, 1) * sizeof(U)));
-        CK(cudaMemsetAsync(v, 0, std::max<size_t>(n, 1) * sizeof(U), st));
+        CK(cudaMalloc(&v, bytes));
+        CK(cudaMemsetAsync(v, 0, bytes, st));
         allocs.push_back(v);
         *ptr = (U*)v;
         return 0;
     }
 
     ~Ctx() override {
-        if (gexec) cudaGraphExecDestroy(gexec);
+        for (cudaGraphExec_t& gx : gexec) if (gx) cudaGraphExecDestroy(gx);
         for (void* v : allocs) cudaFree(v);
+        if (block) cudaFree(block);
         for (auto e : kev) cudaEventDestroy(e);
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
@@ -111,6 +124,30 @@ struct Ctx : CtxBase {
         c = make_const<T>(p);
         law = p.law;
         nf = (law == FD3D_LAW_FVW) ? 5 : 4;
+        std::vector<Damp<T>> prof;
+        make_pml<T>(p, D, prof);
+        const int stride = std::max(1, p.history_stride);
+        p.history_stride = stride;
+        const long long plane = (long long)(p.nxt - 2 * p.nabc) * (p.nzt - p.nfs - p.nabc);
+        int cap = p.history_capacity;
+        if (cap <= 0) {
+            // default: a ring of ~256 MB, at least 8 and at most 4096 records
+            long long rec = plane * nf * (long long)sizeof(T);
+            cap = (int)std::min<long long>(4096, std::max<long long>(8, (256ll << 20) / std::max<long long>(rec, 1)));
+        }
+        hist_cap = cap;
+        {   // size of everything below, in the order it is carved
+            const size_t n2 = (size_t)p.nxt * p.nzt;
+            block_bytes = carve((size_t)g.n3 * 12 * sizeof(T)) + 37 * carve(n2 * sizeof(T)) +
+                          9 * carve(n2 * sizeof(double)) + carve(pml_aux_elems(D) * sizeof(T)) +
+                          carve(prof.size() * sizeof(Damp<T>)) + 2 * carve(sizeof(int)) +
+                          carve((size_t)cap * nf * plane * sizeof(T)) +
+                          carve((size_t)cap * std::max(1, p.nstations) * 3 * sizeof(T));
+            void* v = nullptr;
+            if (cudaMalloc(&v, block_bytes) != cudaSuccess) { cudaGetLastError(); return FD3D_ERR_NOMEM; }
+            block = (char*)v;
+            CK(cudaMemsetAsync(block, 0, block_bytes, st));
+        }
         // 12 arrays of the 3-D grid in one pool
         if (dalloc(&fieldpool, (size_t)g.n3 * 12)) return FD3D_ERR_NOMEM;
         T* b = fieldpool;
@@ -127,31 +164,17 @@ struct Ctx : CtxBase {
         for (T** a : tp) if (dalloc(a, n2)) return FD3D_ERR_NOMEM;
         double** dp[] = {&q.psiX, &q.psiZ, &q.distX, &q.distZ, &q.slipX, &q.slipZ, &q.ruptime, &q.rise, &q.sliptime};
         for (double** a : dp) if (dalloc(a, n2)) return FD3D_ERR_NOMEM;
-        std::vector<T> prof;
-        make_pml<T>(p, D, prof);
-        long long ncell = 0;
-        for (int s = 0; s < 4; ++s) ncell += D.s[s].ncells;
         T* pool = nullptr;
-        if (dalloc(&pool, (size_t)aux_cells32(ncell) * AX_N)) return FD3D_ERR_NOMEM;
-        pml_aux_bind(X, pool, ncell);
-        T* dprof = nullptr;
+        if (dalloc(&pool, pml_aux_elems(D))) return FD3D_ERR_NOMEM;
+        pml_aux_bind(X, pool, D);
+        Damp<T>* dprof = nullptr;
         if (dalloc(&dprof, prof.size())) return FD3D_ERR_NOMEM;
-        CK(cudaMemcpyAsync(dprof, prof.data(), prof.size() * sizeof(T), cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(dprof, prof.data(), prof.size() * sizeof(Damp<T>), cudaMemcpyHostToDevice, st));
         X.prof = dprof;
         tma_ok = make_interior_maps<T>(g, f, vmaps, smaps) && prepare_tma_kernels<T>();
         if (!tma_ok && icfg.variant == IV_TMA) icfg.variant = IV_PIPE;
         if (dalloc(&it_dev, 1)) return FD3D_ERR_NOMEM;
         if (dalloc(&status, 1)) return FD3D_ERR_NOMEM;
-        const int stride = std::max(1, p.history_stride);
-        p.history_stride = stride;
-        const long long plane = (long long)(p.nxt - 2 * p.nabc) * (p.nzt - p.nfs - p.nabc);
-        int cap = p.history_capacity;
-        if (cap <= 0) {
-            // default: a ring of ~256 MB, at least 8 and at most 4096 records
-            long long rec = plane * nf * (long long)sizeof(T);
-            cap = (int)std::min<long long>(4096, std::max<long long>(8, (256ll << 20) / std::max<long long>(rec, 1)));
-        }
-        hist_cap = cap;
         T* r = nullptr;
         if (dalloc(&r, (size_t)cap * nf * plane)) return FD3D_ERR_NOMEM;
         ring = r;
@@ -304,9 +327,7 @@ struct Ctx : CtxBase {
             CK(cudaMemcpyAsync(q.psiZ, psiZ0.data(), n2 * sizeof(double), cudaMemcpyHostToDevice, st));
             CK(cudaMemcpyAsync(q.psiX, psiX0.data(), n2 * sizeof(double), cudaMemcpyHostToDevice, st));
         }
-        long long ncell = 0;
-        for (int s = 0; s < 4; ++s) ncell += D.s[s].ncells;
-        CK(cudaMemsetAsync(X.a[0], 0, (size_t)aux_cells32(ncell) * AX_N * sizeof(T), st));
+        CK(cudaMemsetAsync(X.vel, 0, pml_aux_elems(D) * sizeof(T), st));
         CK(cudaMemsetAsync(it_dev, 0, sizeof(int), st));
         CK(cudaMemsetAsync(status, 0, sizeof(int), st));
         CK(cudaStreamSynchronize(st));
@@ -343,9 +364,8 @@ struct Ctx : CtxBase {
         kbeg(1);
         k_vel_fault<T><<<dim3((std::max(nxT, p.nxt) + 31) / 32, (nzT + 7) / 8), b2, 0, st>>>(g, f, q, c, law, fs, it_dev, status);
         kend(1);
-        const long long npml = D.cum[4];
         kbeg(2);
-        k_vel_pml<T><<<(unsigned)((npml + 255) / 256), 256, 0, st>>>(g, f, D, X, c);
+        launch_pml<T>(false, pml_minb_vel, st, g, f, D, X, c, status);
         kend(2);
         kbeg(3);
         k_vel_fs<T><<<dim3((p.nxt + 31) / 32, (p.nyt + 7) / 8), b2, 0, st>>>(g, f);
@@ -359,7 +379,7 @@ struct Ctx : CtxBase {
         k_str_fault<T><<<dim3((nxT + 31) / 32, (nzT + 7) / 8), b2, 0, st>>>(g, f, q, c);
         kend(5);
         kbeg(6);
-        k_str_pml<T><<<(unsigned)((npml + 255) / 256), 256, 0, st>>>(g, f, D, X, c);
+        launch_pml<T>(true, pml_minb_str, st, g, f, D, X, c, status);
         kend(6);
         // fault boundary condition
         kbeg(7);
@@ -496,6 +516,13 @@ int fd3d_ctx_create(const fd3d_params* p, fd3d_ctx** out) {
     if (const char* e = std::getenv("FD3D_KCHUNK")) c->icfg.kchunk = c->icfg.kchunk_str = std::max(1, std::atoi(e));
     if (const char* e = std::getenv("FD3D_KCHUNK_STR")) c->icfg.kchunk_str = std::max(1, std::atoi(e));
     if (const char* e = std::getenv("FD3D_BY")) c->icfg.by = std::min(32, std::max(1, std::atoi(e)));
+    // FD3D_PML_MINB=<v>[,<s>]: CTAs per SM the velocity / stress PML sweeps are compiled for
+    if (const char* e = std::getenv("FD3D_PML_MINB")) {
+        int v = 1, s = 0;
+        const int n = std::sscanf(e, "%d,%d", &v, &s);
+        c->pml_minb_vel = std::min(4, std::max(1, v));
+        c->pml_minb_str = n == 2 ? std::min(4, std::max(1, s)) : c->pml_minb_vel;
+    }
     rc = c->alloc();
     if (rc) {
         delete c;
@@ -533,16 +560,18 @@ int fd3d_reset(fd3d_ctx* ctx) {
     return ctx->impl->reset();
 }
 
-static int build_graph(CtxBase* c, int nsteps) {
-    if (c->gexec) { cudaGraphExecDestroy(c->gexec); c->gexec = nullptr; }
-    cudaGraph_t gr;
-    CK(cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal));
-    for (int s = 0; s < nsteps; ++s) c->enqueue_step();
-    CK(cudaStreamEndCapture(c->st, &gr));
-    cudaError_t e = cudaGraphInstantiate(&c->gexec, gr, 0);
-    cudaGraphDestroy(gr);
-    if (e != cudaSuccess) { c->gexec = nullptr; return FD3D_ERR_CUDA; }
-    c->gsteps = nsteps;
+// graph g of the context holds 32 >> g time steps (captured on first use)
+static int get_graph(CtxBase* c, int g, cudaGraphExec_t* out) {
+    if (!c->gexec[g]) {
+        cudaGraph_t gr;
+        CK(cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal));
+        for (int s = 0; s < (32 >> g); ++s) c->enqueue_step();
+        CK(cudaStreamEndCapture(c->st, &gr));
+        cudaError_t e = cudaGraphInstantiate(&c->gexec[g], gr, 0);
+        cudaGraphDestroy(gr);
+        if (e != cudaSuccess) { c->gexec[g] = nullptr; return FD3D_ERR_CUDA; }
+    }
+    *out = c->gexec[g];
     return FD3D_OK;
 }
 
@@ -552,15 +581,18 @@ int fd3d_run(fd3d_ctx* ctx, int nsteps) {
     if (!c->medium_ok || !c->fault_ok) return FD3D_ERR_STATE;
     CK(cudaEventRecord(c->ev0, c->st));
     int left = nsteps;
-    const int chunk = 16;
-    if (!c->profiling && left >= chunk) {
-        if (!c->gexec || c->gsteps != chunk) {
-            int rc = build_graph(c, chunk);
+    if (!c->profiling) {
+        // the whole run as graph launches: chunks of 32 steps, the rest by its binary digits
+        for (int g = 0; g < CtxBase::NGRAPH && left > 0; ++g) {
+            const int n = 32 >> g;
+            if (left < n) continue;
+            cudaGraphExec_t gx;
+            int rc = get_graph(c, g, &gx);
             if (rc) return rc;
-        }
-        while (left >= chunk) {
-            CK(cudaGraphLaunch(c->gexec, c->st));
-            left -= chunk;
+            while (left >= n) {
+                CK(cudaGraphLaunch(gx, c->st));
+                left -= n;
+            }
         }
     }
     for (int s = 0; s < left; ++s) c->enqueue_step();

@@ -20,6 +20,7 @@
 // contraction of multiply-add switched off (--fmad=false), the FP32 and FP64
 // builds reproduce the CPU restatement's arithmetic exactly for slip weakening.
 #pragma once
+#include "fd3d_async.cuh"
 #include "fd3d_common.cuh"
 
 namespace fd3d {
@@ -151,103 +152,167 @@ __device__ __forceinline__ void vel_fault_body(Grid g, Fields<T> f, Fault<T> q, 
 
 struct PmlDesc {
     Strip s[4];
-    long long cum[5];  // cumulative thread counts (u/w range) over the strips
+    long long cum[5];  // cumulative cell counts of the u/w loop ranges over the strips
 };
 
-// PML auxiliary components are stored in blocks of 32 cells: within a block the 32
-// values of one component are contiguous and the components of a group follow each
-// other, so the 9 velocity (or 15 stress) components a warp updates for its 32 cells
-// form one contiguous span instead of 9 (15) separate streams.  a[c] points at the
-// group base plus 32 * (index of c in its group); the cell index q of a strip cell
-// (Strip::base + local) maps to the element offset aux_blk(q, group size).
-constexpr int AUX_NV = 9, AUX_NS = 15;  // u,v,w splits / xx,yy,zz,xy,xz,yz splits
-__host__ __device__ __forceinline__ long long aux_blk(long long q, int ncomp) {
-    return (q >> 5) * (32LL * ncomp) + (q & 31);
-}
-inline long long aux_cells32(long long ncell) { return (ncell + 31) & ~31LL; }
+// PML auxiliary components (the 24 split fields that init_pml allocates per strip,
+// fd3d_deriv.f90:1330-1406) are indexed by the compact cell index t of the u/w loop
+// ranges of the 4 strips (strip s holds t in [cum[s], cum[s+1])) and stored in blocks
+// of 32 cells: inside a block the 32 values of one component are contiguous and the
+// components of a group follow each other.  The velocity group (u,v,w splits, 9
+// components) and the stress group (xx,yy,zz,xy,xz,yz splits, 15) are separate spans,
+// so the auxiliaries of PML_TILE consecutive cells are one contiguous range per group:
+// one bulk copy brings a tile's range into shared memory and one writes it back.
+constexpr int AUX_NV = 9, AUX_NS = 15;
+constexpr int PML_TILE = 256;
+inline long long pml_aux_cells(const PmlDesc& D) { return (D.cum[4] + PML_TILE - 1) / PML_TILE * PML_TILE; }
+inline size_t pml_aux_elems(const PmlDesc& D) { return (size_t)pml_aux_cells(D) * (AUX_NV + AUX_NS); }
+
+// One entry of a damping profile (init_pml's omega at one index): the factors
+// 1 - omega and 1 + omega of the split-field update and y = RN(1/(1 + omega)) for
+// div_pre, formed on the host with the same IEEE operations the reference performs.
+template <class T>
+struct alignas(4 * sizeof(T)) Damp {
+    T m, p, r, o;  // 1 - omega, 1 + omega, RN(1/(1 + omega)), omega
+};
 
 template <class T>
 struct PmlAux {
-    T* a[AX_N];         // component bases (see aux_blk); both groups cover all 4 strips
-    const T* prof;      // damping profiles
+    T* vel;              // velocity group, pml_aux_cells * AUX_NV elements
+    T* str;              // stress group, pml_aux_cells * AUX_NS elements
+    const Damp<T>* prof; // damping profiles
 };
 
-// carve the two groups out of one pool of aux_cells32(ncell) * AX_N elements
+// carve the two groups out of one pool of pml_aux_elems(D) elements
 template <class T>
-inline void pml_aux_bind(PmlAux<T>& X, T* pool, long long ncell) {
-    const long long n32 = aux_cells32(ncell);
-    for (int c = 0; c < AX_N; ++c)
-        X.a[c] = c < AUX_NV ? pool + 32LL * c : pool + n32 * AUX_NV + 32LL * (c - AUX_NV);
+inline void pml_aux_bind(PmlAux<T>& X, T* pool, const PmlDesc& D) {
+    X.vel = pool;
+    X.str = pool + pml_aux_cells(D) * AUX_NV;
 }
 
-// locate strip and (i,j,k) of compact thread index t (u/w loop range of every strip)
-__device__ __forceinline__ bool pml_locate(const PmlDesc& D, long long t, int& s, int& i, int& j, int& k,
-                                           long long& qa) {
+// shared-memory slot of component c of the cell that thread l of a tile owns
+__device__ __forceinline__ int aux_sm(int l, int ncomp, int c) { return (l >> 5) * 32 * ncomp + 32 * c + (l & 31); }
+
+// locate strip and (i,j,k) of compact cell index t (u/w loop range of every strip)
+__device__ __forceinline__ bool pml_locate(const PmlDesc& D, long long t, int& s, int& i, int& j, int& k) {
     if (t >= D.cum[4]) return false;
     s = (t >= D.cum[1]) + (t >= D.cum[2]) + (t >= D.cum[3]);
     const Strip& S = D.s[s];
-    // strip-local index fits 32 bits (a strip is ni*nj*nk cells); 32-bit division is
-    // several times cheaper than 64-bit on the GPU
+    // strip-local index fits 32 bits (a strip is ni*nj*nk cells)
     unsigned r = (unsigned)(t - D.cum[s]);
     const unsigned ni = (unsigned)S.ni, nj = (unsigned)(S.jend_uw - S.nyb + 1);
-    const unsigned q1 = r / ni;
-    const int i2 = (int)(r - q1 * ni);
-    const unsigned k2 = q1 / nj;
-    const int j2 = (int)(q1 - k2 * nj);
-    i = S.nxb + i2; j = S.nyb + j2; k = S.nzb + (int)k2;
-    qa = S.base + i2 + (long long)S.ni * (j2 + (long long)S.nj1 * (int)k2);
+    unsigned q1, k2, ri, rj;
+    if (S.fastdiv) {
+        q1 = udiv_small(r, ni, S.rni, ri);
+        k2 = udiv_small(q1, nj, S.rnj, rj);
+    } else {
+        q1 = r / ni; ri = r - q1 * ni;
+        k2 = q1 / nj; rj = q1 - k2 * nj;
+    }
+    i = S.nxb + (int)ri; j = S.nyb + (int)rj; k = S.nzb + (int)k2;
     return true;
 }
 
-// pml_uvw: split-field PML velocity in the 4 strips (fd3d_deriv.f90:1927-2218)
+// Start of a tile: every thread orders its earlier generic accesses of the staging
+// buffer before the async copy, then one thread issues the bulk load of the tile's
+// range of the group (ncomp components).
 template <class T>
-__device__ __forceinline__ void vel_pml_body(Grid g, Fields<T> f, const PmlDesc& D, const PmlAux<T>& X, StepConst<T> c, int bx_, int by_, int bz_) {
-    // linear index; the CTA may be 256 x 1 (single model) or 32 x 8 (persistent batch)
-    const long long t = (long long)bx_ * (blockDim.x * blockDim.y) + threadIdx.y * blockDim.x + threadIdx.x;
-    int s, i, j, k;
-    long long qa;
-    if (!pml_locate(D, t, s, i, j, k, qa)) return;
-    const long long qv = aux_blk(qa, AUX_NV);  // velocity components of this cell
-    const Strip& S = D.s[s];
-    const int i2 = i - S.nxb, j2 = j - S.nyb, k2 = k - S.nzb;
-    const T ox = X.prof[S.ox_off + i2], oxS = X.prof[S.oxS_off + i2];
-    const T oy = X.prof[S.oy_off + j2], oz = X.prof[S.oz_off + k2];
-    const long long p = g.at(i, j, k), sy = g.px, sz = g.plane;
-    const bool dov = (j <= S.nye);
-    // every load first: a store to one array must not hold back the loads of the next
-    const T d = f.d[p], dt = c.dt, dh = c.dh;
-    const T xx0 = f.xx[p], xx1 = f.xx[p - 1], xy0 = f.xy[p], xy1 = f.xy[p - sy], xz0 = f.xz[p], xz1 = f.xz[p - sz];
-    const T xz2 = f.xz[p + 1], yz0 = f.yz[p], yz1 = f.yz[p - sy], zz0 = f.zz[p], zz1 = f.zz[p + sz];
-    T u0 = X.a[AX_U0][qv], u1 = X.a[AX_U1][qv], u2 = X.a[AX_U2][qv];
-    T w0 = X.a[AX_W0][qv], w1 = X.a[AX_W1][qv], w2 = X.a[AX_W2][qv];
-    T v0 = 0, v1 = 0, v2 = 0, xy2 = 0, yy0 = 0, yy1 = 0, yz2 = 0, vold = 0;
-    if (dov) {
-        v0 = X.a[AX_V0][qv]; v1 = X.a[AX_V1][qv]; v2 = X.a[AX_V2][qv];
-        xy2 = f.xy[p + 1]; yy0 = f.yy[p + sy]; yy1 = f.yy[p]; yz2 = f.yz[p - sz];
-        if (j == g.nyt - 1) vold = f.v[p];
+__device__ __forceinline__ void pml_tile_begin(T* sm, const T* src, int ncomp, uint32_t bar) {
+    fence_proxy_async_smem();
+    __syncthreads();
+    if (threadIdx.x == 0 && threadIdx.y == 0) {
+        fence_proxy_async_global();
+        const uint32_t bytes = PML_TILE * ncomp * (uint32_t)sizeof(T);
+        mbar_expect_tx(bar, bytes);
+        bulk_load(smem_addr(sm), src, bytes, bar);
     }
-    const T r = dt / d;
-    T pt;
-    pt = (u0 * ((T)1 - ox) + r * (xx0 - xx1) / dh);   u0 = pt / ((T)1 + ox);
-    pt = (u1 * ((T)1 - oy) + r * (xy0 - xy1) / dh);   u1 = pt / ((T)1 + oy);
-    pt = (u2 * ((T)1 - oz) + r * (xz0 - xz1) / dh);   u2 = pt / ((T)1 + oz);
-    pt = w0 * ((T)1 - oxS) + r * (xz2 - xz0) / dh;    w0 = pt / ((T)1 + oxS);
-    pt = w1 * ((T)1 - oy) + r * (yz0 - yz1) / dh;     w1 = pt / ((T)1 + oy);
-    pt = w2 * ((T)1 - oz) + r * (zz1 - zz0) / dh;     w2 = pt / ((T)1 + oz);
-    if (dov) {
-        pt = v0 * ((T)1 - oxS) + r * (xy2 - xy0) / dh; v0 = pt / ((T)1 + oxS);
-        pt = v1 * ((T)1 - oy) + r * (yy0 - yy1) / dh;  v1 = pt / ((T)1 + oy);
-        pt = v2 * ((T)1 - oz) + r * (yz0 - yz2) / dh;  v2 = pt / ((T)1 + oz);
+}
+// Wait (bounded) for the tile's load; false on every thread if any thread gave up
+// (ST_TIMEOUT recorded after one more bounded wait for the copy in flight).
+__device__ __forceinline__ bool pml_tile_wait(uint32_t bar, uint32_t parity, int* status) {
+    const bool ok = mbar_wait(bar, parity);
+    if (__syncthreads_or(!ok)) {
+        if (threadIdx.x == 0 && threadIdx.y == 0) atomicOr(status, ST_TIMEOUT);
+        mbar_wait(bar, parity);
+        return false;
     }
-    X.a[AX_U0][qv] = u0; X.a[AX_U1][qv] = u1; X.a[AX_U2][qv] = u2;
-    X.a[AX_W0][qv] = w0; X.a[AX_W1][qv] = w1; X.a[AX_W2][qv] = w2;
-    f.u[p] = u0 + u1 + u2;
-    f.w[p] = w0 + w1 + w2;
-    if (dov) {
-        if (j == g.nyt - 1) f.v[p + sy] = vold;  // bnd2d mirror of the value before this update
-        X.a[AX_V0][qv] = v0; X.a[AX_V1][qv] = v1; X.a[AX_V2][qv] = v2;
-        f.v[p] = v0 + v1 + v2;
+    return true;
+}
+// End of a tile: the updated components go back with one bulk store; the issuing
+// thread waits until the buffer has been read, so the CTA may reuse or leave it.
+template <class T>
+__device__ __forceinline__ void pml_tile_end(T* sm, T* dst, int ncomp) {
+    fence_proxy_async_smem();
+    __syncthreads();
+    if (threadIdx.x == 0 && threadIdx.y == 0) {
+        bulk_store(dst, smem_addr(sm), PML_TILE * ncomp * (uint32_t)sizeof(T));
+        bulk_commit();
+        bulk_wait_read();
     }
+}
+
+// pml_uvw: split-field PML velocity in the 4 strips (fd3d_deriv.f90:1927-2218), one
+// tile of PML_TILE consecutive cells per CTA of PML_TILE threads.  Returns false if the
+// staging copy timed out.
+template <class T>
+__device__ __forceinline__ bool vel_pml_tile(const Grid& g, const Fields<T>& f, const PmlDesc& D, const PmlAux<T>& X,
+                                             const StepConst<T>& c, int tile, T* sm, uint32_t bar, uint32_t parity,
+                                             int* status) {
+    const int l = threadIdx.y * blockDim.x + threadIdx.x;
+    const long long t0 = (long long)tile * PML_TILE;
+    T* gaux = X.vel + t0 * AUX_NV;
+    pml_tile_begin(sm, gaux, AUX_NV, bar);
+    int s = 0, i = 0, j = 0, k = 0;
+    const bool act = pml_locate(D, t0 + l, s, i, j, k);
+    T d = 1, xx0 = 0, xx1 = 0, xy0 = 0, xy1 = 0, xz0 = 0, xz1 = 0, xz2 = 0, yz0 = 0, yz1 = 0, zz0 = 0, zz1 = 0;
+    T xy2 = 0, yy0 = 0, yy1 = 0, yz2 = 0, vold = 0;
+    Damp<T> ox{}, oxS{}, oy{}, oz{};
+    long long p = 0;
+    bool dov = false;
+    const long long sy = g.px, sz = g.plane;
+    if (act) {  // field loads overlap the staging copy
+        const Strip& S = D.s[s];
+        const int i2 = i - S.nxb, j2 = j - S.nyb, k2 = k - S.nzb;
+        ox = X.prof[S.ox_off + i2]; oxS = X.prof[S.oxS_off + i2];
+        oy = X.prof[S.oy_off + j2]; oz = X.prof[S.oz_off + k2];
+        p = g.at(i, j, k);
+        dov = (j <= S.nye);
+        d = f.d[p];
+        xx0 = f.xx[p]; xx1 = f.xx[p - 1]; xy0 = f.xy[p]; xy1 = f.xy[p - sy]; xz0 = f.xz[p]; xz1 = f.xz[p - sz];
+        xz2 = f.xz[p + 1]; yz0 = f.yz[p]; yz1 = f.yz[p - sy]; zz0 = f.zz[p]; zz1 = f.zz[p + sz];
+        if (dov) {
+            xy2 = f.xy[p + 1]; yy0 = f.yy[p + sy]; yy1 = f.yy[p]; yz2 = f.yz[p - sz];
+            if (j == g.nyt - 1) vold = f.v[p];
+        }
+    }
+    if (!pml_tile_wait(bar, parity, status)) return false;
+    if (act) {
+        const T dt = c.dt, dh = c.dh, rdh = c.rdh;
+        const T r = dt / d;
+        // p = (p*(1 - omega) + (dt/d)*diff/dh) / (1 + omega), every division rounded as IEEE
+        auto upd = [&](int comp, const Damp<T>& o, T diff) {
+            T& a = sm[aux_sm(l, AUX_NV, comp)];
+            a = div_pre(a * o.m + div_pre(r * diff, dh, rdh), o.p, o.r);
+            return a;
+        };
+        const T u0 = upd(AX_U0, ox, xx0 - xx1);
+        const T u1 = upd(AX_U1, oy, xy0 - xy1);
+        const T u2 = upd(AX_U2, oz, xz0 - xz1);
+        const T w0 = upd(AX_W0, oxS, xz2 - xz0);
+        const T w1 = upd(AX_W1, oy, yz0 - yz1);
+        const T w2 = upd(AX_W2, oz, zz1 - zz0);
+        f.u[p] = u0 + u1 + u2;
+        f.w[p] = w0 + w1 + w2;
+        if (dov) {
+            const T v0 = upd(AX_V0, oxS, xy2 - xy0);
+            const T v1 = upd(AX_V1, oy, yy0 - yy1);
+            const T v2 = upd(AX_V2, oz, yz0 - yz2);
+            if (j == g.nyt - 1) f.v[p + sy] = vold;  // bnd2d mirror of the value before this update
+            f.v[p] = v0 + v1 + v2;
+        }
+    }
+    pml_tile_end(sm, gaux, AUX_NV);
+    return true;
 }
 
 // fuvw at the ghost row k=ks+1 (fd3d_deriv.f90:1018-1062).  w needs u and v of the
@@ -373,84 +438,89 @@ __device__ __forceinline__ void str_fault_body(Grid g, Fields<T> f, Fault<T> q, 
     }
 }
 
-// pml_xyz in the 4 strips (fd3d_deriv.f90:2304-2992)
+// pml_xyz in the 4 strips (fd3d_deriv.f90:2304-2992), one tile per CTA as vel_pml_tile
 template <class T>
-__device__ __forceinline__ void str_pml_body(Grid g, Fields<T> f, const PmlDesc& D, const PmlAux<T>& X, StepConst<T> c, int bx_, int by_, int bz_) {
-    // linear index; the CTA may be 256 x 1 (single model) or 32 x 8 (persistent batch)
-    const long long t = (long long)bx_ * (blockDim.x * blockDim.y) + threadIdx.y * blockDim.x + threadIdx.x;
-    int s, i, j, k;
-    long long qa;
-    if (!pml_locate(D, t, s, i, j, k, qa)) return;
-    const long long qs = aux_blk(qa, AUX_NS);  // stress components of this cell
-    const Strip& S = D.s[s];
-    const int i2 = i - S.nxb, j2 = j - S.nyb, k2 = k - S.nzb;
-    const T ox = X.prof[S.ox_off + i2], oxS = X.prof[S.oxS_off + i2];
-    const T oy = X.prof[S.oy_off + j2], oyS = X.prof[S.oyS_off + j2];
-    const T oz = X.prof[S.oz_off + k2], ozS = X.prof[S.ozS_off + k2];
-    const T oyxy = (s >= 2) ? oyS : oy;  // xy, yz: omegayS in strips 3,4
-    const T ozxz = (s == 3) ? ozS : oz;  // xz, yz: omegazS in strip 4
-    const bool top = (s <= 2) && (k == S.nze);  // xz/yz aux zeroed at the top row, strips 1-3
-    const long long p = g.at(i, j, k), sy = g.px, sz = g.plane;
-    const bool dxy = (j <= S.nye);
-    const T dt = c.dt, dh = c.dh;
-    // every load first: a store to one array must not hold back the loads of the next
-    const T xl = f.lam[p], xm = f.mu[p], mz = f.mu[p + sz];
-    const T up = f.u[p], ux = f.u[p + 1], uz = f.u[p + sz];
-    const T vp = f.v[p], vy = f.v[p - sy];
-    const T wp = f.w[p], wz = f.w[p - sz], wx = f.w[p - 1];
-    T x0 = X.a[AX_XX0][qs], x1 = X.a[AX_XX1][qs], x2 = X.a[AX_XX2][qs];
-    T y0 = X.a[AX_YY0][qs], y1 = X.a[AX_YY1][qs], y2 = X.a[AX_YY2][qs];
-    T z0 = X.a[AX_ZZ0][qs], z1 = X.a[AX_ZZ1][qs], z2 = X.a[AX_ZZ2][qs];
-    T q0 = X.a[AX_XZ0][qs], q1 = X.a[AX_XZ1][qs];
-    T e0 = 0, e1 = 0, h0 = 0, h1 = 0, my = 0, md = 0, uy = 0, vx = 0, vz = 0, wy = 0, xyo = 0, yzo = 0;
-    if (dxy) {
-        e0 = X.a[AX_XY0][qs]; e1 = X.a[AX_XY1][qs]; h0 = X.a[AX_YZ0][qs]; h1 = X.a[AX_YZ1][qs];
-        my = f.mu[p + sy]; md = f.mu[p + 1 + sy + sz];
-        uy = f.u[p + sy]; vx = f.v[p - 1]; vz = f.v[p + sz]; wy = f.w[p + sy];
-        if (j == g.nyt - 1) { xyo = f.xy[p]; yzo = f.yz[p]; }
+__device__ __forceinline__ bool str_pml_tile(const Grid& g, const Fields<T>& f, const PmlDesc& D, const PmlAux<T>& X,
+                                             const StepConst<T>& c, int tile, T* sm, uint32_t bar, uint32_t parity,
+                                             int* status) {
+    const int l = threadIdx.y * blockDim.x + threadIdx.x;
+    const long long t0 = (long long)tile * PML_TILE;
+    T* gaux = X.str + t0 * AUX_NS;
+    pml_tile_begin(sm, gaux, AUX_NS, bar);
+    int s = 0, i = 0, j = 0, k = 0;
+    const bool act = pml_locate(D, t0 + l, s, i, j, k);
+    long long p = 0;
+    bool dxy = false, top = false;
+    const long long sy = g.px, sz = g.plane;
+    T xl = 0, xm = 0, mz = 0, up = 0, ux = 0, uz = 0, vp = 0, vy = 0, wp = 0, wz = 0, wx = 0;
+    T my = 0, md = 0, uy = 0, vx = 0, vz = 0, wy = 0, xyo = 0, yzo = 0;
+    if (act) {  // field loads overlap the staging copy
+        const Strip& S = D.s[s];
+        p = g.at(i, j, k);
+        dxy = (j <= S.nye);
+        top = (s <= 2) && (k == S.nze);  // xz/yz aux zeroed at the top row, strips 1-3
+        xl = f.lam[p]; xm = f.mu[p]; mz = f.mu[p + sz];
+        up = f.u[p]; ux = f.u[p + 1]; uz = f.u[p + sz];
+        vp = f.v[p]; vy = f.v[p - sy];
+        wp = f.w[p]; wz = f.w[p - sz]; wx = f.w[p - 1];
+        if (dxy) {
+            my = f.mu[p + sy]; md = f.mu[p + 1 + sy + sz];
+            uy = f.u[p + sy]; vx = f.v[p - 1]; vz = f.v[p + sz]; wy = f.w[p + sy];
+            if (j == g.nyt - 1) { xyo = f.xy[p]; yzo = f.yz[p]; }
+        }
     }
-    const T a = xl + (T)2 * xm, b = xl;
-    const T diff1 = ux - up, diff2 = vp - vy, diff3 = wp - wz;
-    T pt;
-    pt = x0 * ((T)1 - oxS) + dt * a * diff1 / dh; x0 = pt / ((T)1 + oxS);
-    pt = x1 * ((T)1 - oy) + dt * b * diff2 / dh;  x1 = pt / ((T)1 + oy);
-    pt = x2 * ((T)1 - oz) + dt * b * diff3 / dh;  x2 = pt / ((T)1 + oz);
-    pt = y0 * ((T)1 - oxS) + dt * b * diff1 / dh; y0 = pt / ((T)1 + oxS);
-    pt = y1 * ((T)1 - oy) + dt * a * diff2 / dh;  y1 = pt / ((T)1 + oy);
-    pt = y2 * ((T)1 - oz) + dt * b * diff3 / dh;  y2 = pt / ((T)1 + oz);
-    pt = z0 * ((T)1 - oxS) + dt * b * diff1 / dh; z0 = pt / ((T)1 + oxS);
-    pt = z1 * ((T)1 - oy) + dt * b * diff2 / dh;  z1 = pt / ((T)1 + oy);
-    pt = z2 * ((T)1 - oz) + dt * a * diff3 / dh;  z2 = pt / ((T)1 + oz);
-    {   // xz (j up to jend_uw)
-        const T xmu = (xm + mz) / (T)2;
-        pt = q0 * ((T)1 - ozxz) + dt * xmu * (uz - up) / dh; q0 = pt / ((T)1 + ozxz);
-        pt = q1 * ((T)1 - ox) + dt * xmu * (wp - wx) / dh;   q1 = pt / ((T)1 + ox);
+    if (!pml_tile_wait(bar, parity, status)) return false;
+    if (act) {
+        const Strip& S = D.s[s];
+        const int i2 = i - S.nxb, j2 = j - S.nyb, k2 = k - S.nzb;
+        const Damp<T> ox = X.prof[S.ox_off + i2], oxS = X.prof[S.oxS_off + i2];
+        const Damp<T> oy = X.prof[S.oy_off + j2], oz = X.prof[S.oz_off + k2];
+        // xy, yz use omegayS in strips 3,4; xz, yz use omegazS in strip 4
+        const Damp<T> oyxy = X.prof[(s >= 2 ? S.oyS_off : S.oy_off) + j2];
+        const Damp<T> ozxz = X.prof[(s == 3 ? S.ozS_off : S.oz_off) + k2];
+        const T dt = c.dt, dh = c.dh, rdh = c.rdh;
+        const T a = xl + (T)2 * xm, b = xl;
+        const T diff1 = ux - up, diff2 = vp - vy, diff3 = wp - wz;
+        // p = (p*(1 - omega) + dt*modulus*diff/dh) / (1 + omega), every division rounded as IEEE
+        auto upd = [&](int comp, const Damp<T>& o, T mod, T diff) {
+            T& pa = sm[aux_sm(l, AUX_NS, comp - AUX_NV)];
+            pa = div_pre(pa * o.m + div_pre(dt * mod * diff, dh, rdh), o.p, o.r);
+            return pa;
+        };
+        const T x0 = upd(AX_XX0, oxS, a, diff1);
+        const T x1 = upd(AX_XX1, oy, b, diff2);
+        const T x2 = upd(AX_XX2, oz, b, diff3);
+        f.xx[p] = x0 + x1 + x2;
+        const T y0 = upd(AX_YY0, oxS, b, diff1);
+        const T y1 = upd(AX_YY1, oy, a, diff2);
+        const T y2 = upd(AX_YY2, oz, b, diff3);
+        f.yy[p] = y0 + y1 + y2;
+        const T z0 = upd(AX_ZZ0, oxS, b, diff1);
+        const T z1 = upd(AX_ZZ1, oy, b, diff2);
+        const T z2 = upd(AX_ZZ2, oz, a, diff3);
+        f.zz[p] = z0 + z1 + z2;
+        {   // xz (j up to jend_uw)
+            const T xmu = (xm + mz) / (T)2;
+            const T q0 = upd(AX_XZ0, ozxz, xmu, uz - up);
+            const T q1 = upd(AX_XZ1, ox, xmu, wp - wx);
+            f.xz[p] = q0 + q1;
+            if (top) { sm[aux_sm(l, AUX_NS, AX_XZ0 - AUX_NV)] = (T)0; sm[aux_sm(l, AUX_NS, AX_XZ1 - AUX_NV)] = (T)0; }
+        }
+        if (dxy) {
+            T xmu = (xm + my) / (T)2;
+            const T e0 = upd(AX_XY0, oyxy, xmu, uy - up);
+            const T e1 = upd(AX_XY1, ox, xmu, vp - vx);
+            xmu = (xm + md) / (T)2;
+            const T h0 = upd(AX_YZ0, ozxz, xmu, vz - vp);
+            const T h1 = upd(AX_YZ1, oyxy, xmu, wy - wp);
+            if (j == g.nyt - 1) { f.xy[p + sy] = xyo; f.yz[p + sy] = yzo; }  // strbnd mirror
+            f.xy[p] = e0 + e1;
+            f.yz[p] = h0 + h1;
+            if (top) { sm[aux_sm(l, AUX_NS, AX_YZ0 - AUX_NV)] = (T)0; sm[aux_sm(l, AUX_NS, AX_YZ1 - AUX_NV)] = (T)0; }
+        }
     }
-    if (dxy) {
-        T xmu = (xm + my) / (T)2;
-        pt = e0 * ((T)1 - oyxy) + dt * xmu * (uy - up) / dh; e0 = pt / ((T)1 + oyxy);
-        pt = e1 * ((T)1 - ox) + dt * xmu * (vp - vx) / dh;   e1 = pt / ((T)1 + ox);
-        xmu = (xm + md) / (T)2;
-        pt = h0 * ((T)1 - ozxz) + dt * xmu * (vz - vp) / dh; h0 = pt / ((T)1 + ozxz);
-        pt = h1 * ((T)1 - oyxy) + dt * xmu * (wy - wp) / dh; h1 = pt / ((T)1 + oyxy);
-    }
-    X.a[AX_XX0][qs] = x0; X.a[AX_XX1][qs] = x1; X.a[AX_XX2][qs] = x2;
-    X.a[AX_YY0][qs] = y0; X.a[AX_YY1][qs] = y1; X.a[AX_YY2][qs] = y2;
-    X.a[AX_ZZ0][qs] = z0; X.a[AX_ZZ1][qs] = z1; X.a[AX_ZZ2][qs] = z2;
-    f.xx[p] = x0 + x1 + x2;
-    f.yy[p] = y0 + y1 + y2;
-    f.zz[p] = z0 + z1 + z2;
-    f.xz[p] = q0 + q1;
-    X.a[AX_XZ0][qs] = top ? (T)0 : q0;  // xz/yz aux zeroed at the top row (strips 1-3)
-    X.a[AX_XZ1][qs] = top ? (T)0 : q1;
-    if (dxy) {
-        if (j == g.nyt - 1) { f.xy[p + sy] = xyo; f.yz[p + sy] = yzo; }  // strbnd mirror
-        X.a[AX_XY0][qs] = e0; X.a[AX_XY1][qs] = e1;
-        f.xy[p] = e0 + e1;
-        f.yz[p] = h0 + h1;
-        X.a[AX_YZ0][qs] = top ? (T)0 : h0;
-        X.a[AX_YZ1][qs] = top ? (T)0 : h1;
-    }
+    pml_tile_end(sm, gaux, AUX_NS);
+    return true;
 }
 
 // fres (fd3d_deriv.f90:1067-1104)
@@ -701,10 +771,16 @@ __global__ void k_vel_fault(Grid g, Fields<T> f, Fault<T> q, StepConst<T> c, int
     vel_fault_body<T>(g, f, q, c, law, s, it_dev, status, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
-template <class T>
-__global__ void __launch_bounds__(256) k_vel_pml(Grid g, Fields<T> f, const __grid_constant__ PmlDesc D,
-                                                  const __grid_constant__ PmlAux<T> X, StepConst<T> c) {
-    vel_pml_body<T>(g, f, D, X, c, blockIdx.x, blockIdx.y, blockIdx.z);
+// One PML tile per CTA of PML_TILE threads.  MINB: CTAs that must fit one SM
+// (register cap); 1 leaves it free.
+template <class T, int MINB = 1>
+__global__ void __launch_bounds__(PML_TILE, MINB) k_vel_pml(Grid g, Fields<T> f, const __grid_constant__ PmlDesc D,
+                                                             const __grid_constant__ PmlAux<T> X, StepConst<T> c,
+                                                             int* status) {
+    __shared__ __align__(128) T sm[PML_TILE * AUX_NV];
+    __shared__ __align__(8) uint64_t bar;
+    if (threadIdx.x == 0) { mbar_init(smem_addr(&bar), 1); fence_mbar_init(); }
+    vel_pml_tile<T>(g, f, D, X, c, blockIdx.x, sm, smem_addr(&bar), 0u, status);
 }
 
 template <class T>
@@ -717,10 +793,36 @@ __global__ void k_str_fault(Grid g, Fields<T> f, Fault<T> q, StepConst<T> c) {
     str_fault_body<T>(g, f, q, c, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
+template <class T, int MINB = 1>
+__global__ void __launch_bounds__(PML_TILE, MINB) k_str_pml(Grid g, Fields<T> f, const __grid_constant__ PmlDesc D,
+                                                             const __grid_constant__ PmlAux<T> X, StepConst<T> c,
+                                                             int* status) {
+    __shared__ __align__(128) T sm[PML_TILE * AUX_NS];
+    __shared__ __align__(8) uint64_t bar;
+    if (threadIdx.x == 0) { mbar_init(smem_addr(&bar), 1); fence_mbar_init(); }
+    str_pml_tile<T>(g, f, D, X, c, blockIdx.x, sm, smem_addr(&bar), 0u, status);
+}
+
+// launch of a PML sweep with a register cap picked at run time
 template <class T>
-__global__ void __launch_bounds__(256) k_str_pml(Grid g, Fields<T> f, const __grid_constant__ PmlDesc D,
-                                                  const __grid_constant__ PmlAux<T> X, StepConst<T> c) {
-    str_pml_body<T>(g, f, D, X, c, blockIdx.x, blockIdx.y, blockIdx.z);
+inline void launch_pml(bool stress, int minb, cudaStream_t st, const Grid& g, const Fields<T>& f, const PmlDesc& D,
+                       const PmlAux<T>& X, const StepConst<T>& c, int* status) {
+    const unsigned nblk = (unsigned)((D.cum[4] + PML_TILE - 1) / PML_TILE);
+    if (nblk == 0) return;
+#define FD3D_PML_CASE(MB)                                                               \
+    case MB:                                                                            \
+        if (stress) k_str_pml<T, MB><<<nblk, PML_TILE, 0, st>>>(g, f, D, X, c, status);  \
+        else k_vel_pml<T, MB><<<nblk, PML_TILE, 0, st>>>(g, f, D, X, c, status);         \
+        break;
+    switch (minb) {
+        FD3D_PML_CASE(2)
+        FD3D_PML_CASE(3)
+        FD3D_PML_CASE(4)
+        default:
+            if (stress) k_str_pml<T, 1><<<nblk, PML_TILE, 0, st>>>(g, f, D, X, c, status);
+            else k_vel_pml<T, 1><<<nblk, PML_TILE, 0, st>>>(g, f, D, X, c, status);
+    }
+#undef FD3D_PML_CASE
 }
 
 template <class T>

@@ -39,7 +39,7 @@ inline Grid make_grid(const fd3d_params& p) {
 
 // init_pml (fd3d_deriv.f90:1319-1493): strip boxes and damping profiles, in T.
 template <class T>
-void make_pml(const fd3d_params& p, PmlDesc& D, std::vector<T>& prof) {
+void make_pml(const fd3d_params& p, PmlDesc& D, std::vector<Damp<T>>& prof) {
     const int nxt = p.nxt, nyt = p.nyt, nzt = p.nzt, nabc = p.nabc, nfs = p.nfs;
     const int bx[4][6] = {{2, nabc, nabc + 1, nyt - 1, nabc + 1, nzt - nfs},
                           {nxt - nabc + 1, nxt - 1, nabc + 1, nyt - 1, nabc + 1, nzt - nfs},
@@ -58,6 +58,9 @@ void make_pml(const fd3d_params& p, PmlDesc& D, std::vector<T>& prof) {
         S.base = base;
         base += S.ncells;
         D.cum[s + 1] = D.cum[s] + (long long)S.ni * (S.jend_uw - S.nyb + 1) * S.nk;
+        S.rni = 1.0f / (float)S.ni;
+        S.rnj = 1.0f / (float)(S.jend_uw - S.nyb + 1);
+        S.fastdiv = (D.cum[s + 1] - D.cum[s]) < (1LL << 24);
         ox[s].assign(S.ni, (T)0); oxS[s].assign(S.ni, (T)0);
         oy[s].assign(S.nj1, (T)0); oyS[s].assign(S.nj1, (T)0);
         oz[s].assign(S.nk, (T)0); ozS[s].assign(S.nk, (T)0);
@@ -85,7 +88,18 @@ void make_pml(const fd3d_params& p, PmlDesc& D, std::vector<T>& prof) {
     }
     for (int s = 0; s < 4; ++s) {
         Strip& S = D.s[s];
-        auto put = [&](const std::vector<T>& v) { int o = (int)prof.size(); prof.insert(prof.end(), v.begin(), v.end()); return o; };
+        auto put = [&](const std::vector<T>& v) {
+            const int o = (int)prof.size();
+            for (T om : v) {
+                Damp<T> e;
+                e.o = om;
+                e.m = (T)1 - om;
+                e.p = (T)1 + om;
+                e.r = div_pre_recip(e.p);
+                prof.push_back(e);
+            }
+            return o;
+        };
         S.ox_off = put(ox[s]); S.oxS_off = put(oxS[s]);
         S.oy_off = put(oy[s]); S.oyS_off = put(oyS[s]);
         S.oz_off = put(oz[s]); S.ozS_off = put(ozS[s]);
@@ -102,6 +116,7 @@ StepConst<T> make_const(const fd3d_params& p) {
     c.damp_s = (T)p.damp_s;
     c.c1 = (T)9 / (T)8;
     c.c2 = (T)-1 / (T)24;
+    c.rdh = div_pre_recip(c.dh);
     c.dtA = p.dt;
     c.dhA = (double)c.dh;
     c.dthA = c.dtA / c.dhA;

@@ -16,53 +16,23 @@
 // copies still in flight and returns.
 #pragma once
 #include <cuda.h>
+#include "fd3d_async.cuh"
 #include "fd3d_common.cuh"
 
 namespace fd3d {
-
-enum { ST_TIMEOUT = 4 };
 
 struct VelMaps { CUtensorMap xx, xy, yy, xz, yz, d, u, v, w; };
 struct StrMaps { CUtensorMap u, v, w, lam, mu, xx, yy, zz, xy, xz, yz; };
 
 constexpr int TMA_NS = 3;            // ring slots: plane k computed, k+1 and k+2 in flight
-constexpr int TMA_WAIT_LIMIT = 1 << 20;
 constexpr int TMA_SMEM_PAD = 128;  // alignment slack of the dynamic ring
 
-__device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
-
-__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
-}
-__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
-}
-__device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
-    uint32_t ok;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}"
-        : "=r"(ok)
-        : "r"(bar), "r"(parity)
-        : "memory");
-    return ok != 0;
-}
-// bounded wait on an mbarrier phase; false after TMA_WAIT_LIMIT unsuccessful polls
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
-    for (int n = 0; n < TMA_WAIT_LIMIT; ++n)
-        if (mbar_try_wait(bar, parity)) return true;
-    return false;
-}
 __device__ __forceinline__ void tma_load_3d(uint32_t dst, const CUtensorMap* map, int x, int y, int z, uint32_t bar) {
     asm volatile(
         "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];" ::
             "r"(dst), "l"((uint64_t)map), "r"(x), "r"(y), "r"(z), "r"(bar)
         : "memory");
 }
-__device__ __forceinline__ void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
-__device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
-
 // Velocity slot layout (elements; every window starts on 128 bytes)
 //   xx [8][40]  x i0-4..i0+35, y j0..j0+7
 //   xy [11][40] x i0-4..,      y j0-2..j0+8

@@ -226,6 +226,15 @@ int fd3d_batch_get_tuning(fd3d_batch* b, int* kchunk, int* ctas_per_sm, int* max
  * resets the models; cache_path/key (optional) persist the choice as JSON lines */
 int fd3d_batch_autotune(fd3d_batch* b, int steps, const char* cache_path, const char* key);
 
+/* ---- self-test ----------------------------------------------------------
+ * No counterpart in the reference.  The PML kernels divide by dh and by 1 + omega
+ * (fd3d_deriv.f90:1498-1925) through a quotient formed from a reciprocal computed on
+ * the host; this runs that routine and the IEEE division on all 2^32 float bit
+ * patterns for each of the n divisors on the current device and stores the number
+ * of dividends whose quotients differ (0 expected) and the first such bit pattern
+ * (0xffffffff if none). */
+int fd3d_check_division(const float* divisors, int n, unsigned long long* mismatches, unsigned* first_bad);
+
 /* ---- input decks (the reference's own files) --------------------------- */
 /* Reads inputfd3d.dat and crustal.dat from dir (fd3d_init.f90:145-173, 211-279),
  * fills p and returns lam1/mu1/d1 (caller frees with fd3d_free). */
