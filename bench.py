@@ -93,35 +93,54 @@ class ClockSampler:
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def dist_setup(ngpus):
+def dist_setup(ngpus, backend=None):
+    """One process per GPU under torchrun: the process group carries only the barrier
+    around the timed region and the max-over-ranks reduction of the timings (replicas,
+    no data-path collective).  backend "gloo" (FD3D_BENCH_BACKEND) runs the same
+    plumbing on CPU tensors."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
+    backend = backend or os.environ.get("FD3D_BENCH_BACKEND", "nccl")
     pg = None
     if world > 1:
         import datetime
         import torch
         import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
         pg = dist
     return world, rank, local, pg
+
+
+def _on_gpu(pg):
+    return pg is not None and pg.get_backend() == "nccl"
 
 
 def barrier(pg, local):
     if pg is not None:
         import torch
-        pg.barrier(device_ids=[local])
-        torch.cuda.synchronize()
+        if _on_gpu(pg):
+            pg.barrier(device_ids=[local])
+            torch.cuda.synchronize()
+        else:
+            pg.barrier()
 
 
 def max_over_ranks(pg, local, v):
     if pg is None:
         return v
     import torch
-    t = torch.tensor([v], dtype=torch.float64, device=f"cuda:{local}")
+    t = torch.tensor([v], dtype=torch.float64, device=f"cuda:{local}" if _on_gpu(pg) else "cpu")
     pg.all_reduce(t, op=pg.ReduceOp.MAX)
     return float(t.item())
+
+
+def whole_job_rate(units_per_rank, world, seconds_max):
+    """Weak scaling over replicas: every rank processed units_per_rank; the job took the
+    slowest rank's time."""
+    return units_per_rank * world / seconds_max
 
 
 def workload(name):
@@ -220,7 +239,7 @@ def run_b200(args, world, rank, local, pg):
     ms = s.last_run_ms()          # CUDA events on the stream the steps are launched on
     ck = clocks.stop()
     ms_max = max_over_ranks(pg, local, ms)
-    value = cells * args.steps * world / (ms_max / 1e3) / 1e9
+    value = whole_job_rate(cells * args.steps, world, ms_max / 1e3) / 1e9
 
     # per-kernel times (CUDA events around each launch) over a few extra steps
     s.set_profiling(True)
@@ -254,7 +273,7 @@ def run_b200(args, world, rank, local, pg):
     if args.e2e:
         e2e = end_to_end(m, args.steps, local)
         e2e_v = max_over_ranks(pg, local, e2e.pop("_seconds"))
-        e2e["value"] = cells * args.steps * world / e2e_v / 1e9
+        e2e["value"] = whole_job_rate(cells * args.steps, world, e2e_v) / 1e9
 
     cpu = None
     if rank == 0 and world == 1 and args.cpu_baseline > 0:
@@ -297,11 +316,13 @@ def end_to_end(m, steps, local):
         keep.append(t)
     nab = m["nabc"]
     plane = (m["nxt"] - 2 * nab) * (m["nzt"] - nab - m["nfs"])
-    nf = 4
-    hist, th = pinned((nf, steps, plane), np.float32, order="C")
+    nf = 5 if m.get("law") == "fvw" else 4   # slip rates, shear tractions (+ psi for FVW)
+    stride = max(1, int(m.get("history_stride", 1)))
+    nrec = steps // stride
+    hist, th = pinned((nf, max(nrec, 1), plane), np.float32, order="C")
     keep.append(th)
     nst = len(m.get("stations", []))
-    seis = np.empty((steps, max(nst, 1), 3))
+    seis = np.empty((max(nrec, 1), max(nst, 1), 3))
     chunk = 16              # history records are read back every chunk of steps
     m = dict(m, history_capacity=2 * chunk)
     s = Solver(m)           # context + fault; its medium is replaced inside the timed region
@@ -311,26 +332,32 @@ def end_to_end(m, steps, local):
     t0 = time.perf_counter()
     s.upload_medium_arrays(*host, real_kind=4)
     s.upload_fault(m["fault"])
-    done = 0
+    done = got = 0
     while done < steps:
         n = min(chunk, steps - done)
         s.run(n)
         s.sync()
-        for f in range(nf):
-            rc = lib().fd3d_fetch_history(s.h, f, done, n, hist[f, done:done + n].ctypes.data, 4)
-            if rc:
-                raise abi.Fd3dError(rc, "fd3d_fetch_history")
-        if nst:
-            lib().fd3d_fetch_stations(s.h, done, n, seis[done:done + n].ctypes.data_as(C.POINTER(C.c_double)))
         done += n
+        have = done // stride
+        if have > got:
+            for f in range(nf):
+                rc = lib().fd3d_fetch_history(s.h, f, got, have - got, hist[f, got:have].ctypes.data, 4)
+                if rc:
+                    raise abi.Fd3dError(rc, "fd3d_fetch_history")
+            if nst:
+                rc = lib().fd3d_fetch_stations(s.h, got, have - got,
+                                               seis[got:have].ctypes.data_as(C.POINTER(C.c_double)))
+                if rc:
+                    raise abi.Fd3dError(rc, "fd3d_fetch_stations")
+            got = have
     dt = time.perf_counter() - t0
     s.close()
     fault_bytes = 6 * m["nxt"] * m["nzt"] * 8
     h2d = 3 * int(np.prod(shp)) * 4 + fault_bytes
-    d2h = nf * plane * 4 + nst * 3 * 8
-    return {"unit": "GCell-updates/s", "h2d_bytes_per_step": h2d / steps, "d2h_bytes_per_step": d2h,
-            "_seconds": dt, "includes": "medium (fp32, pinned) + fault upload, K steps, K history records of 4 "
-                                        "planes + stations read back; wall clock"}
+    d2h = (nf * plane * 4 + nst * 3 * 8) * nrec
+    return {"unit": "GCell-updates/s", "h2d_bytes_per_step": h2d / steps, "d2h_bytes_per_step": d2h / steps,
+            "_seconds": dt, "includes": f"medium (fp32, pinned) + fault upload, K steps, the {nrec} history records "
+                                        f"({nf} planes each, every {stride} steps) + stations read back; wall clock"}
 
 
 def _same_finals(a, b):
@@ -374,7 +401,7 @@ def run_batch_bench(args, world, rank, local, pg):
     ref, t_plain = plain(models)
     identical = all(_same_finals(finals[q], ref[q]) for q in ref)
     if rank == 0:
-        line = {"metric": "batched solves/s", "value": len(models) * world / wall_max, "unit": "solves/s",
+        line = {"metric": "batched solves/s", "value": whole_job_rate(len(models), world, wall_max), "unit": "solves/s",
                 "n_gpus": world, "higher_is_better": True, "scaling": "weak", "dtype": "f32", "data": "synthetic",
                 "config": {"workload": "batch", "models": len(models), "h_m": 200.0, "sim_s": 8.0,
                            "cells_x_steps": cells},
@@ -405,8 +432,10 @@ def run_serve_bench(args, world, rank, local, pg):
     ref, t_plain = plain([m for q, (_, m) in enumerate(stream) if q in sample], keep_final=lambda r: True)
     identical = all(_same_finals(byreq[q].final, ref[q]) for q in ref)
     plain_rate = len(ref) / t_plain
+    makespan_max = max_over_ranks(pg, local, stats["makespan_s"])
     if rank == 0:
-        line = {"metric": "serving solves/s", "value": stats["solves_per_s"] * world, "unit": "solves/s",
+        line = {"metric": "serving solves/s", "value": whole_job_rate(stats["requests"], world, makespan_max),
+                "unit": "solves/s",
                 "n_gpus": world, "higher_is_better": True, "scaling": "weak", "dtype": "f32", "data": "synthetic",
                 "config": {"workload": "serve", "requests": len(stream), "arrival_rate_per_s": args.rate,
                            "large_fraction": 0.05, "sim_s": args.sim_time, "hbm_budget_gb": args.hbm_gb},
