@@ -9,6 +9,7 @@ from . import abi
 from .solver import _ck, lib
 
 _SIG = False
+SCHEDULES = {"persistent": 0, "graph": 1}
 
 
 def _bind():
@@ -36,6 +37,8 @@ def _bind():
         "fd3d_batch_set_tuning": (i, [vp, i, i]),
         "fd3d_batch_get_tuning": (i, [vp, C.POINTER(i), C.POINTER(i), C.POINTER(i)]),
         "fd3d_batch_autotune": (i, [vp, i, C.c_char_p, C.c_char_p]),
+        "fd3d_batch_set_schedule": (i, [vp, i]),
+        "fd3d_batch_get_schedule": (i, [vp, C.POINTER(i)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -140,10 +143,18 @@ class Batch:
     def set_tuning(self, kchunk: int, ctas_per_sm: int = 0):
         _ck(lib().fd3d_batch_set_tuning(self.h, kchunk, ctas_per_sm), "fd3d_batch_set_tuning")
 
+    def set_schedule(self, mode: str):
+        """"persistent" (one cooperative kernel per run) or "graph" (CUDA graphs of
+        per-region kernels over all models)."""
+        _ck(lib().fd3d_batch_set_schedule(self.h, SCHEDULES[mode]), "fd3d_batch_set_schedule")
+
     def tuning(self):
         a, b, c = C.c_int(), C.c_int(), C.c_int()
         _ck(lib().fd3d_batch_get_tuning(self.h, C.byref(a), C.byref(b), C.byref(c)), "fd3d_batch_get_tuning")
-        return dict(kchunk=a.value, ctas_per_sm=b.value, max_ctas_per_sm=c.value)
+        mode = C.c_int()
+        _ck(lib().fd3d_batch_get_schedule(self.h, C.byref(mode)), "fd3d_batch_get_schedule")
+        names = {v: k for k, v in SCHEDULES.items()}
+        return dict(schedule=names[mode.value], kchunk=a.value, ctas_per_sm=b.value, max_ctas_per_sm=c.value)
 
     def autotune(self, steps: int = 10, cache_path: str | None = None, key: str | None = None):
         _ck(lib().fd3d_batch_autotune(self.h, steps, cache_path.encode() if cache_path else None,

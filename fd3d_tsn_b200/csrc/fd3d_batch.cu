@@ -1,9 +1,11 @@
-// fd3d_batch.cu -- many independent forward models in one persistent launch.
+// fd3d_batch.cu -- many independent forward models in one launch schedule.
 //
 // Models of uneven size live in one device arena (first-fit, 256-byte aligned blocks,
-// each with its own padded pitch).  A run is one cooperative kernel whose CTAs walk,
-// phase by phase, a host-built work list of (model, tile) items and meet at a bounded
-// grid-wide barrier between phases.  A time step has seven phases:
+// each with its own padded pitch).  Their work is a host-built list of (model, tile)
+// items.  Two schedules run it: the persistent one is one cooperative kernel per run
+// whose CTAs walk the items phase by phase and meet at a bounded grid-wide barrier
+// between phases; the graph one replays CUDA graphs of per-region kernels over all
+// models (see k_bint).  A time step has seven phases:
 //   0 velocity: interior tiles, fault band + fault plane, PML chunks
 //   1 free-surface velocity ghosts
 //   2 stress: interior tiles, fault band + fault plane, PML chunks
@@ -11,10 +13,9 @@
 //   4 trial traction   5 friction   6 output planes (+ nucleation ramp)
 // Every item runs the same __device__ body as the single-model launch of that region
 // (fd3d_kernels.cuh / fd3d_opt.cuh), so a model's results do not depend on which other
-// models share the launch.  The run is captured in a CUDA graph when the device
-// supports capturing cooperative launches, else launched directly.
-// The z-extent of the interior tiles and the number of CTAs per SM are picked by an
-// autotuner that times the candidates on the live batch (and resets the models after).
+// models share the launch.  The schedule, the z-extent of the interior tiles and (for
+// the persistent kernel) the number of CTAs per SM are picked by an autotuner that
+// times the candidates on the live batch (and resets the models after).
 #include <cuda_runtime.h>
 #include <algorithm>
 #include <chrono>
@@ -191,6 +192,91 @@ k_batch(const ModelDev* __restrict__ models, const ModelMaps* __restrict__ maps,
     }
 }
 
+// ---------------------------------------------------------------- graph schedule
+// The same items as k_batch, one kernel per region and step, every CTA one item.
+// A CUDA graph holds a chunk of steps: per step the interior, fault-band and PML
+// sweeps of a half-step run as three parallel branches, the plane regions follow in
+// order, and k_step_end advances the run's step counter (items of a model whose
+// step limit is reached return at once).  Each kernel gets its own register and
+// shared-memory budget, so each region runs at its own occupancy.
+constexpr int NTYPES = 12;
+
+__device__ __forceinline__ bool item_live(const Work& it, const int* limit, const int* run_step, int& m) {
+    m = it.tm >> 8;
+    return *run_step < limit[m];
+}
+
+template <bool STRESS>
+__global__ void __launch_bounds__(256) k_bint(const ModelDev* __restrict__ models, const ModelMaps* __restrict__ maps,
+                                              const Work* __restrict__ work, int b0, const int* __restrict__ limit,
+                                              const int* run_step, int kchunk, int* gstatus) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    float* ring = reinterpret_cast<float*>(smem_raw + ((128u - (smem_addr(smem_raw) & 127u)) & 127u));
+    __shared__ __align__(8) uint64_t bars[TMA_NS];
+    const Work it = work[b0 + blockIdx.x];
+    int m;
+    if (!item_live(it, limit, run_step, m)) return;
+    tma_ring_init(bars);
+    const ModelDev& M = models[m];
+    unsigned pc = 0;
+    if (STRESS)
+        str_interior_tma_body<float>(maps[m].s, M.g, M.f, M.c, kchunk, it.bx, it.by, it.bz, ring, bars, pc, gstatus);
+    else
+        vel_interior_tma_body<float>(maps[m].v, M.g, M.f, M.c, kchunk, it.bx, it.by, it.bz, ring, bars, pc, gstatus);
+}
+
+template <bool STRESS>
+__global__ void __launch_bounds__(PML_TILE, 4) k_bpml(const ModelDev* __restrict__ models,
+                                                      const Work* __restrict__ work, int b0,
+                                                      const int* __restrict__ limit, const int* run_step,
+                                                      int* gstatus) {
+    __shared__ __align__(128) float sm[PML_TILE * (STRESS ? AUX_NS : AUX_NV)];
+    __shared__ __align__(8) uint64_t bar;
+    const Work it = work[b0 + blockIdx.x];
+    int m;
+    if (!item_live(it, limit, run_step, m)) return;
+    if (threadIdx.x == 0 && threadIdx.y == 0) { mbar_init(smem_addr(&bar), 1); fence_mbar_init(); }
+    const ModelDev& M = models[m];
+    if (STRESS) str_pml_tile<float>(M.g, M.f, M.D, M.X, M.c, it.bx, sm, smem_addr(&bar), 0u, gstatus);
+    else vel_pml_tile<float>(M.g, M.f, M.D, M.X, M.c, it.bx, sm, smem_addr(&bar), 0u, gstatus);
+}
+
+__global__ void __launch_bounds__(256) k_bplane(const ModelDev* __restrict__ models, const Work* __restrict__ work,
+                                                int b0, const int* __restrict__ limit, const int* run_step) {
+    const Work it = work[b0 + blockIdx.x];
+    int m;
+    if (!item_live(it, limit, run_step, m)) return;
+    const ModelDev& M = models[m];
+    switch (it.tm & 255) {
+        case W_VEL_FAULT:
+            vel_fault_body<float>(M.g, M.f, M.q, M.c, M.law, M.fs, M.it_dev, M.status, it.bx, it.by, 0);
+            break;
+        case W_VEL_FS: vel_fs_body<float>(M.g, M.f, it.bx, it.by, 0); break;
+        case W_STR_FAULT: str_fault_body<float>(M.g, M.f, M.q, M.c, it.bx, it.by, 0); break;
+        case W_STR_FS: str_fs_body<float>(M.g, M.f, it.bx, it.by, 0); break;
+        case W_TRAC: traction_body<float>(M.g, M.f, M.q, M.c, it.bx, it.by, 0); break;
+        case W_FRIC: friction_body<float>(M.g, M.f, M.q, M.c, M.law, M.fs, M.it_dev, it.bx, it.by, 0); break;
+        case W_OUT: output_body<float>(M.g, M.f, M.q, M.law, M.it_dev, M.h, M.status, it.bx, it.by, 0); break;
+        case W_NUC: nucleation_body<float>(M.g, M.q, M.c, M.fs, M.it_dev, it.bx, it.by, 0); break;
+        default: break;
+    }
+}
+
+__global__ void k_step_end(int* run_step) { *run_step += 1; }
+
+// OR of the live models' device status words into out (one read-back per sync)
+__global__ void k_or_status(int* const* __restrict__ st, int n, int* out) {
+    int v = 0;
+    for (int q = threadIdx.x; q < n; q += blockDim.x) v |= *st[q];
+    v = __reduce_or_sync(0xffffffffu, v);
+    __shared__ int acc;
+    if (threadIdx.x == 0) acc = 0;
+    __syncthreads();
+    if ((threadIdx.x & 31) == 0) atomicOr(&acc, v);
+    __syncthreads();
+    if (threadIdx.x == 0) *out = acc;
+}
+
 // 1-D layered medium -> padded 3-D arrays of one model
 __global__ void k_fill_layers(Grid g, float* lam, float* mu, float* d, const float* lk, const float* mk,
                               const float* dk) {
@@ -297,9 +383,12 @@ struct Model {
     int cap = 0;
 };
 
+enum { MODE_PERSISTENT = FD3D_BATCH_PERSISTENT, MODE_GRAPH = FD3D_BATCH_GRAPH };
+
 struct Tuning {
     int kchunk = 16;
-    int per_sm = 0;     // CTAs per SM (0 = occupancy limit)
+    int per_sm = 0;     // CTAs per SM (0 = occupancy limit), persistent schedule
+    int mode = MODE_GRAPH;
 };
 
 }  // namespace
@@ -328,6 +417,21 @@ struct fd3d_batch {
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     float last_ms = 0.f;
     std::mutex mu;
+    // graph schedule: items sorted by type, the run's step counter, branch streams,
+    // and graphs of 32, 16, 8, 4, 2 and 1 steps captured for the current work list
+    std::vector<Work> work_t;
+    int tbeg[NTYPES + 1] = {0};
+    Work* d_work_t = nullptr;
+    size_t work_t_cap = 0;
+    int* d_run_step = nullptr;
+    cudaStream_t side[2] = {nullptr, nullptr};
+    cudaEvent_t evf[3] = {nullptr, nullptr, nullptr};
+    static constexpr int NGRAPH = 6;
+    cudaGraphExec_t gx[NGRAPH] = {};
+    int graph_kchunk = -1;
+    int** d_stptr = nullptr;     // status words of the live models (k_or_status)
+    int n_stptr = 0;
+    int* d_status_or = nullptr;
 };
 
 namespace {
@@ -383,6 +487,34 @@ int build_work(fd3d_batch* b) {
         b->pbeg[ph] = (int)b->work.size();
         b->work.insert(b->work.end(), per[ph].begin(), per[ph].end());
     }
+    {   // status words of the live models
+        std::vector<int*> sp;
+        for (const Model& M : b->models)
+            if (M.live) sp.push_back(M.dev.status);
+        b->n_stptr = (int)sp.size();
+        if (!sp.empty())
+            BCK(cudaMemcpyAsync(b->d_stptr, sp.data(), sp.size() * sizeof(int*), cudaMemcpyHostToDevice, b->st));
+    }
+    {   // the same items grouped by type for the graph schedule
+        std::vector<std::vector<Work>> byt(NTYPES);
+        for (const Work& w : b->work) byt[w.tm & 255].push_back(w);
+        b->work_t.clear();
+        for (int t = 0; t < NTYPES; ++t) {
+            b->tbeg[t] = (int)b->work_t.size();
+            b->work_t.insert(b->work_t.end(), byt[t].begin(), byt[t].end());
+        }
+        b->tbeg[NTYPES] = (int)b->work_t.size();
+        if (b->work_t.size() > b->work_t_cap) {
+            if (b->d_work_t) cudaFree(b->d_work_t);
+            b->work_t_cap = b->work_t.size() + b->work_t.size() / 2 + 64;
+            BCK(cudaMalloc(&b->d_work_t, b->work_t_cap * sizeof(Work)));
+        }
+        if (!b->work_t.empty())
+            BCK(cudaMemcpyAsync(b->d_work_t, b->work_t.data(), b->work_t.size() * sizeof(Work),
+                                cudaMemcpyHostToDevice, b->st));
+        for (cudaGraphExec_t& g : b->gx)
+            if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+    }
     b->pbeg[NPHASE] = (int)b->work.size();
     if (b->work.size() > b->work_cap) {
         if (b->d_work) cudaFree(b->d_work);
@@ -398,7 +530,97 @@ int build_work(fd3d_batch* b) {
     return FD3D_OK;
 }
 
+// one time step of the graph schedule on b->st (fork/join over the side streams)
+int enqueue_graph_step(fd3d_batch* b) {
+    const dim3 blk(32, 8);
+    const int kc = b->tun.kchunk;
+    auto n_of = [&](int t) { return b->tbeg[t + 1] - b->tbeg[t]; };
+    auto plane = [&](cudaStream_t s, int t0, int t1) {  // item types [t0, t1) in one launch
+        const int n = b->tbeg[t1] - b->tbeg[t0];
+        if (n > 0) k_bplane<<<n, blk, 0, s>>>(b->d_models, b->d_work_t, b->tbeg[t0], b->d_limit, b->d_run_step);
+    };
+    for (int half = 0; half < 2; ++half) {
+        const int ti = half ? W_STR_INT : W_VEL_INT, tf = half ? W_STR_FAULT : W_VEL_FAULT;
+        const int tp = half ? W_STR_PML : W_VEL_PML, tfs = half ? W_STR_FS : W_VEL_FS;
+        BCK(cudaEventRecord(b->evf[0], b->st));
+        BCK(cudaStreamWaitEvent(b->side[0], b->evf[0], 0));
+        BCK(cudaStreamWaitEvent(b->side[1], b->evf[0], 0));
+        if (n_of(ti) > 0) {
+            if (half)
+                k_bint<true><<<n_of(ti), blk, tma_ring_bytes<float>(), b->st>>>(
+                    b->d_models, b->d_maps, b->d_work_t, b->tbeg[ti], b->d_limit, b->d_run_step, kc, b->d_status);
+            else
+                k_bint<false><<<n_of(ti), blk, tma_ring_bytes<float>(), b->st>>>(
+                    b->d_models, b->d_maps, b->d_work_t, b->tbeg[ti], b->d_limit, b->d_run_step, kc, b->d_status);
+        }
+        plane(b->side[0], tf, tf + 1);
+        if (n_of(tp) > 0) {
+            if (half)
+                k_bpml<true><<<n_of(tp), blk, 0, b->side[1]>>>(b->d_models, b->d_work_t, b->tbeg[tp], b->d_limit,
+                                                               b->d_run_step, b->d_status);
+            else
+                k_bpml<false><<<n_of(tp), blk, 0, b->side[1]>>>(b->d_models, b->d_work_t, b->tbeg[tp], b->d_limit,
+                                                                b->d_run_step, b->d_status);
+        }
+        BCK(cudaEventRecord(b->evf[1], b->side[0]));
+        BCK(cudaEventRecord(b->evf[2], b->side[1]));
+        BCK(cudaStreamWaitEvent(b->st, b->evf[1], 0));
+        BCK(cudaStreamWaitEvent(b->st, b->evf[2], 0));
+        plane(b->st, tfs, tfs + 1);
+    }
+    plane(b->st, W_TRAC, W_TRAC + 1);
+    plane(b->st, W_FRIC, W_FRIC + 1);
+    plane(b->st, W_OUT, W_NUC + 1);  // output and nucleation ramp share a phase
+    k_step_end<<<1, 1, 0, b->st>>>(b->d_run_step);
+    BCK(cudaGetLastError());
+    return FD3D_OK;
+}
+
+// graph g holds 32 >> g steps of the graph schedule (captured on first use)
+int get_batch_graph(fd3d_batch* b, int g, cudaGraphExec_t* out) {
+    if (b->graph_kchunk != b->tun.kchunk) {
+        for (cudaGraphExec_t& x : b->gx)
+            if (x) { cudaGraphExecDestroy(x); x = nullptr; }
+        b->graph_kchunk = b->tun.kchunk;
+    }
+    if (!b->gx[g]) {
+        cudaGraph_t gr;
+        BCK(cudaStreamBeginCapture(b->st, cudaStreamCaptureModeThreadLocal));
+        int rc = FD3D_OK;
+        for (int s = 0; s < (32 >> g) && rc == FD3D_OK; ++s) rc = enqueue_graph_step(b);
+        cudaError_t e = cudaStreamEndCapture(b->st, &gr);
+        if (rc) {
+            if (e == cudaSuccess) cudaGraphDestroy(gr);
+            return rc;
+        }
+        BCK(e);
+        e = cudaGraphInstantiate(&b->gx[g], gr, 0);
+        cudaGraphDestroy(gr);
+        if (e != cudaSuccess) { b->gx[g] = nullptr; return FD3D_ERR_CUDA; }
+    }
+    *out = b->gx[g];
+    return FD3D_OK;
+}
+
+int launch_graphs(fd3d_batch* b, int nsteps) {
+    BCK(cudaMemsetAsync(b->d_run_step, 0, sizeof(int), b->st));
+    int left = nsteps;
+    for (int g = 0; g < fd3d_batch::NGRAPH && left > 0; ++g) {
+        const int n = 32 >> g;
+        if (left < n) continue;
+        cudaGraphExec_t x;
+        int rc = get_batch_graph(b, g, &x);
+        if (rc) return rc;
+        while (left >= n) {
+            BCK(cudaGraphLaunch(x, b->st));
+            left -= n;
+        }
+    }
+    return FD3D_OK;
+}
+
 int launch_batch(fd3d_batch* b, int nsteps) {
+    if (b->tun.mode == MODE_GRAPH) return launch_graphs(b, nsteps);
     const int per_sm = b->tun.per_sm > 0 ? std::min(b->tun.per_sm, b->max_active) : b->max_active;
     const int grid = std::max(1, per_sm * b->nsm);
     BCK(cudaMemsetAsync(b->d_sync, 0, sizeof(BatchSync), b->st));
@@ -486,9 +708,23 @@ int fd3d_batch_create(size_t arena_bytes, int max_models, fd3d_batch** out) {
         cudaMalloc(&b->d_maps, sizeof(ModelMaps) * max_models) != cudaSuccess ||
         cudaMalloc(&b->d_limit, sizeof(int) * max_models) != cudaSuccess ||
         cudaMalloc(&b->d_pbeg, sizeof(int) * (NPHASE + 1)) != cudaSuccess ||
-        cudaMalloc(&b->d_sync, sizeof(BatchSync)) != cudaSuccess || cudaMalloc(&b->d_status, sizeof(int)) != cudaSuccess) {
+        cudaMalloc(&b->d_sync, sizeof(BatchSync)) != cudaSuccess || cudaMalloc(&b->d_status, sizeof(int)) != cudaSuccess ||
+        cudaMalloc(&b->d_run_step, sizeof(int)) != cudaSuccess ||
+        cudaMalloc(&b->d_stptr, sizeof(int*) * max_models) != cudaSuccess ||
+        cudaMalloc(&b->d_status_or, sizeof(int)) != cudaSuccess) {
         cudaGetLastError();
         return fail(FD3D_ERR_NOMEM);
+    }
+    for (cudaStream_t& s : b->side)
+        if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) return fail(FD3D_ERR_CUDA);
+    for (cudaEvent_t& e : b->evf)
+        if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) return fail(FD3D_ERR_CUDA);
+    if (cudaFuncSetAttribute(k_bint<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, tma_ring_bytes<float>()) !=
+            cudaSuccess ||
+        cudaFuncSetAttribute(k_bint<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, tma_ring_bytes<float>()) !=
+            cudaSuccess) {
+        cudaGetLastError();
+        return fail(FD3D_ERR_CUDA);
     }
     cudaMemset(b->d_status, 0, sizeof(int));
     cudaEventCreate(&b->ev0);
@@ -501,6 +737,9 @@ int fd3d_batch_create(size_t arena_bytes, int max_models, fd3d_batch** out) {
     }
     if (const char* e = std::getenv("FD3D_BATCH_KCHUNK")) b->tun.kchunk = std::max(1, std::atoi(e));
     if (const char* e = std::getenv("FD3D_BATCH_PER_SM")) b->tun.per_sm = std::max(0, std::atoi(e));
+    // FD3D_BATCH_MODE=persistent|graph
+    if (const char* e = std::getenv("FD3D_BATCH_MODE"))
+        b->tun.mode = std::strcmp(e, "persistent") == 0 ? MODE_PERSISTENT : MODE_GRAPH;
     *out = b;
     return FD3D_OK;
 }
@@ -516,6 +755,16 @@ int fd3d_batch_destroy(fd3d_batch* b) {
     cudaFree(b->d_sync);
     cudaFree(b->d_status);
     cudaFree(b->d_work);
+    cudaFree(b->d_work_t);
+    cudaFree(b->d_run_step);
+    cudaFree(b->d_stptr);
+    cudaFree(b->d_status_or);
+    for (cudaGraphExec_t g : b->gx)
+        if (g) cudaGraphExecDestroy(g);
+    for (cudaStream_t s : b->side)
+        if (s) cudaStreamDestroy(s);
+    for (cudaEvent_t e : b->evf)
+        if (e) cudaEventDestroy(e);
     if (b->ev0) cudaEventDestroy(b->ev0);
     if (b->ev1) cudaEventDestroy(b->ev1);
     if (b->st) cudaStreamDestroy(b->st);
@@ -686,15 +935,19 @@ int fd3d_batch_sync(fd3d_batch* b) {
     if (!b) return FD3D_ERR_ARG;
     BCK(cudaStreamSynchronize(b->st));
     cudaEventElapsedTime(&b->last_ms, b->ev0, b->ev1);
-    int st = 0;
-    BCK(cudaMemcpy(&st, b->d_status, sizeof(int), cudaMemcpyDeviceToHost));
-    int any = st;
-    for (const Model& M : b->models) {
-        if (!M.live) continue;
-        int s = 0;
-        BCK(cudaMemcpy(&s, M.dev.status, sizeof(int), cudaMemcpyDeviceToHost));
-        any |= s;
+    if (b->dirty) {  // the status list follows the live models
+        int rc = build_work(b);
+        if (rc) return rc;
     }
+    int st[2] = {0, 0};
+    BCK(cudaMemcpy(&st[0], b->d_status, sizeof(int), cudaMemcpyDeviceToHost));
+    if (b->n_stptr > 0) {
+        k_or_status<<<1, 256, 0, b->st>>>(b->d_stptr, b->n_stptr, b->d_status_or);
+        BCK(cudaGetLastError());
+        BCK(cudaMemcpyAsync(&st[1], b->d_status_or, sizeof(int), cudaMemcpyDeviceToHost, b->st));
+        BCK(cudaStreamSynchronize(b->st));
+    }
+    const int any = st[0] | st[1];
     if (any & ST_TIMEOUT) return FD3D_ERR_TIMEOUT;
     if (any & ST_NONFINITE) return FD3D_ERR_NONFINITE;
     if (any & ST_NEWTON) return FD3D_ERR_NEWTON;
@@ -804,6 +1057,19 @@ int fd3d_batch_set_tuning(fd3d_batch* b, int kchunk, int ctas_per_sm) {
     return FD3D_OK;
 }
 
+int fd3d_batch_set_schedule(fd3d_batch* b, int mode) {
+    if (!b || (mode != FD3D_BATCH_PERSISTENT && mode != FD3D_BATCH_GRAPH)) return FD3D_ERR_ARG;
+    std::lock_guard<std::mutex> lk(b->mu);
+    b->tun.mode = mode;
+    return FD3D_OK;
+}
+
+int fd3d_batch_get_schedule(fd3d_batch* b, int* mode) {
+    if (!b || !mode) return FD3D_ERR_ARG;
+    *mode = b->tun.mode;
+    return FD3D_OK;
+}
+
 int fd3d_batch_get_tuning(fd3d_batch* b, int* kchunk, int* ctas_per_sm, int* max_ctas_per_sm) {
     if (!b) return FD3D_ERR_ARG;
     if (kchunk) *kchunk = b->tun.kchunk;
@@ -833,40 +1099,57 @@ int fd3d_batch_autotune(fd3d_batch* b, int steps, const char* cache_path, const 
         std::ifstream in(cache_path);
         std::string line;
         while (std::getline(in, line)) {
-            int kc = 0, ps = 0;
+            int kc = 0, ps = 0, mode = -1;
             char buf[256] = {0};
-            if (std::sscanf(line.c_str(), "{\"key\": \"%255[^\"]\", \"kchunk\": %d, \"ctas_per_sm\": %d", buf, &kc, &ps) == 3 &&
-                k == buf && kc > 0) {
+            if (std::sscanf(line.c_str(), "{\"key\": \"%255[^\"]\", \"schedule\": %d, \"kchunk\": %d, \"ctas_per_sm\": %d",
+                            buf, &mode, &kc, &ps) == 4 &&
+                k == buf && kc > 0 && (mode == MODE_GRAPH || mode == MODE_PERSISTENT)) {
+                b->tun.mode = mode;
                 b->tun.kchunk = kc;
                 b->tun.per_sm = ps;
                 return FD3D_OK;
             }
         }
     }
+    // candidates: the graph schedule per interior tile depth, the persistent kernel per
+    // tile depth and CTAs per SM
     const int kcs[] = {4, 8, 16, 32};
+    std::vector<Tuning> cand;
+    for (int kc : kcs) {
+        Tuning t;
+        t.mode = MODE_GRAPH;
+        t.kchunk = kc;
+        cand.push_back(t);
+    }
     std::vector<int> pss;
     for (int ps = 1; ps <= b->max_active; ps *= 2) pss.push_back(ps);
     if (pss.back() != b->max_active) pss.push_back(b->max_active);
-    float best = 1e30f;
-    Tuning bt = b->tun;
     for (int kc : kcs)
         for (int ps : pss) {
-            b->tun.kchunk = kc;
-            b->tun.per_sm = ps;
-            int rc = fd3d_batch_run(b, steps);
-            if (rc) return rc;
-            rc = fd3d_batch_sync(b);
-            if (rc) return rc;
-            if (b->last_ms < best) { best = b->last_ms; bt = b->tun; }
-            for (size_t m = 0; m < b->models.size(); ++m)
-                if (b->models[m].live) { rc = reset_model(b, b->models[m]); if (rc) return rc; }
-            BCK(cudaStreamSynchronize(b->st));
+            Tuning t;
+            t.mode = MODE_PERSISTENT;
+            t.kchunk = kc;
+            t.per_sm = ps;
+            cand.push_back(t);
         }
+    float best = 1e30f;
+    Tuning bt = b->tun;
+    for (const Tuning& t : cand) {
+        b->tun = t;
+        int rc = fd3d_batch_run(b, steps);
+        if (rc) return rc;
+        rc = fd3d_batch_sync(b);
+        if (rc) return rc;
+        if (b->last_ms < best) { best = b->last_ms; bt = b->tun; }
+        for (size_t m = 0; m < b->models.size(); ++m)
+            if (b->models[m].live) { rc = reset_model(b, b->models[m]); if (rc) return rc; }
+        BCK(cudaStreamSynchronize(b->st));
+    }
     b->tun = bt;
     if (cache_path && !k.empty()) {
         std::ofstream out(cache_path, std::ios::app);
-        out << "{\"key\": \"" << k << "\", \"kchunk\": " << bt.kchunk << ", \"ctas_per_sm\": " << bt.per_sm
-            << ", \"ms\": " << best << ", \"steps\": " << steps << "}\n";
+        out << "{\"key\": \"" << k << "\", \"schedule\": " << bt.mode << ", \"kchunk\": " << bt.kchunk
+            << ", \"ctas_per_sm\": " << bt.per_sm << ", \"ms\": " << best << ", \"steps\": " << steps << "}\n";
     }
     return FD3D_OK;
 }

@@ -193,14 +193,21 @@ int fd3d_kernel_times(fd3d_ctx* ctx, float* ms /* FD3D_NKERNELS */, int* launche
 /* kernel ids in fd3d_kernel_times: 0 vel_interior, 1 vel_fault, 2 vel_pml, 3 vel_fs,
    4 str_interior, 5 str_fault, 6 str_pml, 7 fault_bc (traction+friction+output) */
 
-/* ---- many models in one persistent launch ------------------------------
+/* ---- many models in one launch schedule ---------------------------------
  * No counterpart in the reference, which runs one model per process
  * (src/dynamicsolver.f90:66).  Independent forward models of uneven size share one
  * device arena of arena_bytes; fd3d_batch_run advances every live model by up to
- * nsteps steps (each stops at its own ntfd) in one cooperative kernel.  Models use
- * the FP32 build, a 1-D layered medium (one value per k, as readcrustalmodel builds)
- * and keep the last history_capacity records (default 16) of their history planes.
- * A model's results are the same bits whether it runs alone or among others. */
+ * nsteps steps (each stops at its own ntfd).  Two schedules run the same work items:
+ * FD3D_BATCH_PERSISTENT, one cooperative kernel per run whose CTAs walk the items
+ * phase by phase between grid barriers, and FD3D_BATCH_GRAPH, CUDA graphs of 32, 16,
+ * 8, 4, 2 or 1 steps with one kernel per region and step over all models (the
+ * interior, fault-band and PML sweeps of a half-step as parallel branches).
+ * fd3d_batch_autotune picks the schedule and its tile shape.  Models use the FP32
+ * build, a 1-D layered medium (one value per k, as readcrustalmodel builds) and keep
+ * the last history_capacity records (default 16) of their history planes.  A model's
+ * results are the same bits whether it runs alone or among others, in either schedule. */
+#define FD3D_BATCH_PERSISTENT 0
+#define FD3D_BATCH_GRAPH 1
 typedef struct fd3d_batch fd3d_batch;
 int fd3d_batch_create(size_t arena_bytes, int max_models, fd3d_batch** out);
 int fd3d_batch_destroy(fd3d_batch* b);
@@ -219,9 +226,12 @@ int fd3d_batch_fetch_plane(fd3d_batch* b, int slot, int plane, double* host);
 int fd3d_batch_fetch_final(fd3d_batch* b, int slot, double* slipX, double* slipZ, double* ruptime,
                            double* rise, double* sliptime);
 int fd3d_batch_fetch_history(fd3d_batch* b, int slot, int field, int rec0, int nrec, double* host);
-/* tile shape of the persistent launch: z-planes per interior tile and CTAs per SM (0 = max) */
+/* tile shape: z-planes per interior tile and, for the persistent schedule, CTAs per SM (0 = max) */
 int fd3d_batch_set_tuning(fd3d_batch* b, int kchunk, int ctas_per_sm);
 int fd3d_batch_get_tuning(fd3d_batch* b, int* kchunk, int* ctas_per_sm, int* max_ctas_per_sm);
+/* schedule: FD3D_BATCH_PERSISTENT or FD3D_BATCH_GRAPH (the default) */
+int fd3d_batch_set_schedule(fd3d_batch* b, int mode);
+int fd3d_batch_get_schedule(fd3d_batch* b, int* mode);
 /* times the tile-shape candidates on the live models (all at step 0), keeps the fastest,
  * resets the models; cache_path/key (optional) persist the choice as JSON lines */
 int fd3d_batch_autotune(fd3d_batch* b, int steps, const char* cache_path, const char* key);

@@ -1,9 +1,10 @@
-"""The batched persistent launch against the single-model path, through the C ABI.
+"""The batched schedules against the single-model path, through the C ABI.
 
 Every model in a batch must produce the same bits as the same model solved alone
 with fd3d_run (the per-item device bodies are the single-model kernels' bodies), no
-matter which other models share the launch, when it joined, or which tile shape the
-autotuner picked.
+matter which other models share the launch, when it joined, which schedule runs the
+batch (one persistent cooperative kernel, or graphs of per-region kernels) or which
+tile shape the autotuner picked.
 """
 import numpy as np
 import pytest
@@ -43,9 +44,14 @@ def same(b, slot, s, steps):
     np.testing.assert_array_equal(b.history(slot, 0, 0, steps), s.history(0, 0, steps))
 
 
-def test_batch_equals_single_model_runs():
+SCHEDULES = pytest.mark.parametrize("schedule", ["graph", "persistent"])
+
+
+@SCHEDULES
+def test_batch_equals_single_model_runs(schedule):
     models = small_models(5, steps=30)
     b = Batch(2 << 30, 16)
+    b.set_schedule(schedule)
     slots = [b.add(m) for m in models]
     b.run(30)
     b.sync()
@@ -54,11 +60,13 @@ def test_batch_equals_single_model_runs():
         same(b, slot, alone(m, 30), 30)
 
 
-def test_batch_mixed_laws_and_uneven_lengths():
+@SCHEDULES
+def test_batch_mixed_laws_and_uneven_lengths(schedule):
     sw = small_models(2, seed0=7, steps=24)
     fvw = configs.tiny_fvw(nsteps=18)
     fvw["history_capacity"] = 18
     b = Batch(2 << 30, 8)
+    b.set_schedule(schedule)
     s0, s1, s2 = b.add(sw[0]), b.add(fvw), b.add(sw[1])
     b.run(16)
     b.run(16)   # each model stops at its own ntfd
@@ -71,10 +79,12 @@ def test_batch_mixed_laws_and_uneven_lengths():
         np.testing.assert_array_equal(b.final(s1)[k], ref.final()[k])
 
 
-def test_models_joining_later_and_leaving():
+@SCHEDULES
+def test_models_joining_later_and_leaving(schedule):
     """Continuous batching: a model admitted while others run gets its own answer."""
     ms = small_models(4, seed0=40, steps=40)
     b = Batch(2 << 30, 8)
+    b.set_schedule(schedule)
     a0, a1 = b.add(ms[0]), b.add(ms[1])
     b.run(10)
     a2 = b.add(ms[2])        # joins at another model's step 10
@@ -104,7 +114,7 @@ def test_autotune_keeps_results(tmp_path):
     b = Batch(2 << 30, 8)
     slots = [b.add(m) for m in models]
     t = b.autotune(steps=5, cache_path=str(tmp_path / "tune.jsonl"), key="test3")
-    assert t["kchunk"] in (4, 8, 16, 32)
+    assert t["kchunk"] in (4, 8, 16, 32) and t["schedule"] in ("graph", "persistent")
     assert (tmp_path / "tune.jsonl").read_text().count("test3") == 1
     b.run(20)
     b.sync()
