@@ -256,10 +256,13 @@ def run_b200(args, world, rank, local, pg):
     achieved = dom_bytes / (dom_ms / 1e3) / 1e9
     step_gbs = cells * B_ALG_STEP / (ms / args.steps / 1e3) / 1e9
     traffic = None
-    tpath = os.path.join(ROOT, "profiles", "traffic.json")
+    tpath = os.path.join(ROOT, "profiles", "traffic_dram_bytes.txt")   # ncu DRAM bytes per launch
     if os.path.exists(tpath):
         with open(tpath) as f:
-            traffic = json.load(f).get(args.workload, {}).get(dom)
+            for line in f:
+                w = line.split()
+                if len(w) == 3 and not w[0].startswith("#") and w[0] == args.workload and w[1] == dom:
+                    traffic = int(w[2])
     roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "peak_source": peak_kind, "traffic": traffic,
                 "algorithmic_bytes_per_launch": dom_bytes, "avg_launch_ms": dom_ms,
