@@ -185,8 +185,6 @@ k_batch(const ModelDev* __restrict__ models, const ModelMaps* __restrict__ maps,
                 }
                 __syncthreads();  // the next item may reuse the ring
             }
-            // PML write-backs of this phase complete before any CTA reads them in the next step
-            if (threadIdx.x == 0 && threadIdx.y == 0) { bulk_wait_all(); fence_proxy_async_global(); }
             if (!grid_barrier(sync, nb, gstatus)) return;
         }
     }

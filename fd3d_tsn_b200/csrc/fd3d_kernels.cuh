@@ -238,19 +238,6 @@ __device__ __forceinline__ bool pml_tile_wait(uint32_t bar, uint32_t parity, int
     }
     return true;
 }
-// End of a tile: the updated components go back with one bulk store; the issuing
-// thread waits until the buffer has been read, so the CTA may reuse or leave it.
-template <class T>
-__device__ __forceinline__ void pml_tile_end(T* sm, T* dst, int ncomp) {
-    fence_proxy_async_smem();
-    __syncthreads();
-    if (threadIdx.x == 0 && threadIdx.y == 0) {
-        bulk_store(dst, smem_addr(sm), PML_TILE * ncomp * (uint32_t)sizeof(T));
-        bulk_commit();
-        bulk_wait_read();
-    }
-}
-
 // pml_uvw: split-field PML velocity in the 4 strips (fd3d_deriv.f90:1927-2218), one
 // tile of PML_TILE consecutive cells per CTA of PML_TILE threads.  Returns false if the
 // staging copy timed out.
@@ -290,9 +277,15 @@ __device__ __forceinline__ bool vel_pml_tile(const Grid& g, const Fields<T>& f, 
         const T dt = c.dt, dh = c.dh, rdh = c.rdh;
         const T r = dt / d;
         // p = (p*(1 - omega) + (dt/d)*diff/dh) / (1 + omega), every division rounded as IEEE
+        // Where omega is 0 (most split directions of a strip) a*(1-0) = a and x/(1+0) = x
+        // exactly, so the branch skips a multiply and a division without changing a bit.
+        // The result goes straight back to the component's global slot (one coalesced
+        // 128-byte row per warp and component), so no bulk store has to drain.
         auto upd = [&](int comp, const Damp<T>& o, T diff) {
-            T& a = sm[aux_sm(l, AUX_NV, comp)];
-            a = div_pre(a * o.m + div_pre(r * diff, dh, rdh), o.p, o.r);
+            const int q = aux_sm(l, AUX_NV, comp);
+            const T inc = div_pre(r * diff, dh, rdh);
+            const T a = (o.o == (T)0) ? sm[q] + inc : div_pre(sm[q] * o.m + inc, o.p, o.r);
+            gaux[q] = a;
             return a;
         };
         const T u0 = upd(AX_U0, ox, xx0 - xx1);
@@ -311,7 +304,6 @@ __device__ __forceinline__ bool vel_pml_tile(const Grid& g, const Fields<T>& f, 
             f.v[p] = v0 + v1 + v2;
         }
     }
-    pml_tile_end(sm, gaux, AUX_NV);
     return true;
 }
 
@@ -482,9 +474,12 @@ __device__ __forceinline__ bool str_pml_tile(const Grid& g, const Fields<T>& f, 
         const T a = xl + (T)2 * xm, b = xl;
         const T diff1 = ux - up, diff2 = vp - vy, diff3 = wp - wz;
         // p = (p*(1 - omega) + dt*modulus*diff/dh) / (1 + omega), every division rounded as IEEE
+        // omega = 0: exact shortcut as in vel_pml_tile
         auto upd = [&](int comp, const Damp<T>& o, T mod, T diff) {
-            T& pa = sm[aux_sm(l, AUX_NS, comp - AUX_NV)];
-            pa = div_pre(pa * o.m + div_pre(dt * mod * diff, dh, rdh), o.p, o.r);
+            const int q = aux_sm(l, AUX_NS, comp - AUX_NV);
+            const T inc = div_pre(dt * mod * diff, dh, rdh);
+            const T pa = (o.o == (T)0) ? sm[q] + inc : div_pre(sm[q] * o.m + inc, o.p, o.r);
+            gaux[q] = pa;
             return pa;
         };
         const T x0 = upd(AX_XX0, oxS, a, diff1);
@@ -504,7 +499,7 @@ __device__ __forceinline__ bool str_pml_tile(const Grid& g, const Fields<T>& f, 
             const T q0 = upd(AX_XZ0, ozxz, xmu, uz - up);
             const T q1 = upd(AX_XZ1, ox, xmu, wp - wx);
             f.xz[p] = q0 + q1;
-            if (top) { sm[aux_sm(l, AUX_NS, AX_XZ0 - AUX_NV)] = (T)0; sm[aux_sm(l, AUX_NS, AX_XZ1 - AUX_NV)] = (T)0; }
+            if (top) { gaux[aux_sm(l, AUX_NS, AX_XZ0 - AUX_NV)] = (T)0; gaux[aux_sm(l, AUX_NS, AX_XZ1 - AUX_NV)] = (T)0; }
         }
         if (dxy) {
             T xmu = (xm + my) / (T)2;
@@ -516,10 +511,9 @@ __device__ __forceinline__ bool str_pml_tile(const Grid& g, const Fields<T>& f, 
             if (j == g.nyt - 1) { f.xy[p + sy] = xyo; f.yz[p + sy] = yzo; }  // strbnd mirror
             f.xy[p] = e0 + e1;
             f.yz[p] = h0 + h1;
-            if (top) { sm[aux_sm(l, AUX_NS, AX_YZ0 - AUX_NV)] = (T)0; sm[aux_sm(l, AUX_NS, AX_YZ1 - AUX_NV)] = (T)0; }
+            if (top) { gaux[aux_sm(l, AUX_NS, AX_YZ0 - AUX_NV)] = (T)0; gaux[aux_sm(l, AUX_NS, AX_YZ1 - AUX_NV)] = (T)0; }
         }
     }
-    pml_tile_end(sm, gaux, AUX_NS);
     return true;
 }
 
