@@ -394,6 +394,7 @@ struct Tuning {
 struct fd3d_batch {
     int dev = 0;
     cudaStream_t st = nullptr;
+    cudaStream_t sst = nullptr;  // set-up of newly added models, concurrent with a run on st
     char* arena_base = nullptr;
     Arena arena;
     std::vector<Model> models;
@@ -666,17 +667,17 @@ void fault_planes(const fd3d_params& p, const fd3d_fault& fl, std::vector<std::v
         }
 }
 
-int reset_model(fd3d_batch* b, Model& M) {
+int reset_model(fd3d_batch* b, Model& M, cudaStream_t st) {
     const size_t n2 = (size_t)M.p.nxt * M.p.nzt;
     ModelDev& d = M.dev;
-    BCK(cudaMemsetAsync(d.f.u, 0, (size_t)d.g.n3 * 9 * sizeof(float), b->st));
+    BCK(cudaMemsetAsync(d.f.u, 0, (size_t)d.g.n3 * 9 * sizeof(float), st));
     float* zt[] = {d.q.tx, d.q.tz, d.q.txt, d.q.tzt, d.q.RFx, d.q.RFz, d.q.avdx, d.q.avdz, d.q.v1t, d.q.au1, d.q.av1,
                    d.q.aw1, d.q.uZ, d.q.wX, d.q.schangeX, d.q.schangeZ};
-    for (float* a : zt) BCK(cudaMemsetAsync(a, 0, n2 * sizeof(float), b->st));
+    for (float* a : zt) BCK(cudaMemsetAsync(a, 0, n2 * sizeof(float), st));
     double* zd[] = {d.q.distX, d.q.distZ, d.q.slipX, d.q.slipZ, d.q.rise};
-    for (double* a : zd) BCK(cudaMemsetAsync(a, 0, n2 * sizeof(double), b->st));
-    BCK(cudaMemsetAsync(d.X.vel, 0, pml_aux_elems(d.D) * sizeof(float), b->st));
-    k_model_reset<<<(unsigned)((n2 + 255) / 256), 256, 0, b->st>>>(d, (int)n2);
+    for (double* a : zd) BCK(cudaMemsetAsync(a, 0, n2 * sizeof(double), st));
+    BCK(cudaMemsetAsync(d.X.vel, 0, pml_aux_elems(d.D) * sizeof(float), st));
+    k_model_reset<<<(unsigned)((n2 + 255) / 256), 256, 0, st>>>(d, (int)n2);
     BCK(cudaGetLastError());
     M.steps = 0;
     return FD3D_OK;
@@ -698,7 +699,9 @@ int fd3d_batch_create(size_t arena_bytes, int max_models, fd3d_batch** out) {
     cudaDeviceGetAttribute(&b->nsm, cudaDevAttrMultiProcessorCount, b->dev);
     if (!coop) { delete b; return FD3D_ERR_NODEV; }
     auto fail = [&](int rc) { fd3d_batch_destroy(b); return rc; };
-    if (cudaStreamCreateWithFlags(&b->st, cudaStreamNonBlocking) != cudaSuccess) return fail(FD3D_ERR_CUDA);
+    if (cudaStreamCreateWithFlags(&b->st, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&b->sst, cudaStreamNonBlocking) != cudaSuccess)
+        return fail(FD3D_ERR_CUDA);
     if (cudaMalloc(&b->arena_base, arena_bytes) != cudaSuccess) { cudaGetLastError(); return fail(FD3D_ERR_NOMEM); }
     b->arena.init(arena_bytes);
     b->models.resize(max_models);
@@ -745,6 +748,7 @@ int fd3d_batch_create(size_t arena_bytes, int max_models, fd3d_batch** out) {
 int fd3d_batch_destroy(fd3d_batch* b) {
     if (!b) return FD3D_ERR_ARG;
     if (b->st) cudaStreamSynchronize(b->st);
+    if (b->sst) cudaStreamSynchronize(b->sst);
     cudaFree(b->arena_base);
     cudaFree(b->d_models);
     cudaFree(b->d_maps);
@@ -766,6 +770,7 @@ int fd3d_batch_destroy(fd3d_batch* b) {
     if (b->ev0) cudaEventDestroy(b->ev0);
     if (b->ev1) cudaEventDestroy(b->ev1);
     if (b->st) cudaStreamDestroy(b->st);
+    if (b->sst) cudaStreamDestroy(b->sst);
     delete b;
     return FD3D_OK;
 }
@@ -851,30 +856,30 @@ int fd3d_batch_add(fd3d_batch* b, const fd3d_params* pin, const double* lam_k, c
         d.fs.strinixI = fl->strinixI;
     }
     // whole block to zero, then medium, fault planes and profiles
-    BCK(cudaMemsetAsync(b->arena_base + M.off, 0, bp.used, b->st));
+    BCK(cudaMemsetAsync(b->arena_base + M.off, 0, bp.used, b->sst));
     std::vector<float> lay(3 * (size_t)p.nzt);
     for (int k = 0; k < p.nzt; ++k) { lay[k] = (float)lam_k[k]; lay[p.nzt + k] = (float)mu_k[k]; lay[2 * p.nzt + k] = (float)d_k[k]; }
-    BCK(cudaMemcpyAsync(layers, lay.data(), lay.size() * sizeof(float), cudaMemcpyHostToDevice, b->st));
-    k_fill_layers<<<1024, 256, 0, b->st>>>(d.g, lam, mu, dd, layers, layers + p.nzt, layers + 2 * p.nzt);
+    BCK(cudaMemcpyAsync(layers, lay.data(), lay.size() * sizeof(float), cudaMemcpyHostToDevice, b->sst));
+    k_fill_layers<<<1024, 256, 0, b->sst>>>(d.g, lam, mu, dd, layers, layers + p.nzt, layers + 2 * p.nzt);
     BCK(cudaGetLastError());
     std::vector<std::vector<float>> F;
     std::vector<double> pz, px;
     fault_planes(p, *fl, F, pz, px);
     float* dst[18] = {d.q.T0X, d.q.T0Z, d.q.Dc, d.q.peakX, d.q.dynX, d.q.DcX, d.q.peakZ, d.q.dynZ, d.q.DcZ, d.q.coh,
                       d.q.aX, d.q.bX, d.q.vwX, d.q.fwX, d.q.aZ, d.q.bZ, d.q.vwZ, d.q.fwZ};
-    for (int a = 0; a < 18; ++a) BCK(cudaMemcpyAsync(dst[a], F[a].data(), n2 * sizeof(float), cudaMemcpyHostToDevice, b->st));
-    BCK(cudaMemcpyAsync(d.q.T0Xb, F[0].data(), n2 * sizeof(float), cudaMemcpyHostToDevice, b->st));
-    BCK(cudaMemcpyAsync(d.psiZ0, pz.data(), n2 * sizeof(double), cudaMemcpyHostToDevice, b->st));
-    BCK(cudaMemcpyAsync(d.psiX0, px.data(), n2 * sizeof(double), cudaMemcpyHostToDevice, b->st));
-    BCK(cudaMemcpyAsync(dprof, prof.data(), prof.size() * sizeof(Damp<float>), cudaMemcpyHostToDevice, b->st));
+    for (int a = 0; a < 18; ++a) BCK(cudaMemcpyAsync(dst[a], F[a].data(), n2 * sizeof(float), cudaMemcpyHostToDevice, b->sst));
+    BCK(cudaMemcpyAsync(d.q.T0Xb, F[0].data(), n2 * sizeof(float), cudaMemcpyHostToDevice, b->sst));
+    BCK(cudaMemcpyAsync(d.psiZ0, pz.data(), n2 * sizeof(double), cudaMemcpyHostToDevice, b->sst));
+    BCK(cudaMemcpyAsync(d.psiX0, px.data(), n2 * sizeof(double), cudaMemcpyHostToDevice, b->sst));
+    BCK(cudaMemcpyAsync(dprof, prof.data(), prof.size() * sizeof(Damp<float>), cudaMemcpyHostToDevice, b->sst));
     M.live = true;
-    rc = reset_model(b, M);
+    rc = reset_model(b, M, b->sst);
     if (rc) { b->arena.release(M.off, M.bytes); return rc; }
     ModelMaps mm;
     if (!make_interior_maps<float>(d.g, d.f, mm.v, mm.s)) { b->arena.release(M.off, M.bytes); return FD3D_ERR_CUDA; }
-    BCK(cudaMemcpyAsync(b->d_maps + m, &mm, sizeof(ModelMaps), cudaMemcpyHostToDevice, b->st));
-    BCK(cudaMemcpyAsync(b->d_models + m, &M.dev, sizeof(ModelDev), cudaMemcpyHostToDevice, b->st));
-    BCK(cudaStreamSynchronize(b->st));
+    BCK(cudaMemcpyAsync(b->d_maps + m, &mm, sizeof(ModelMaps), cudaMemcpyHostToDevice, b->sst));
+    BCK(cudaMemcpyAsync(b->d_models + m, &M.dev, sizeof(ModelDev), cudaMemcpyHostToDevice, b->sst));
+    BCK(cudaStreamSynchronize(b->sst));
     b->models[m] = M;
     b->dirty = true;
     *slot = m;
@@ -896,7 +901,7 @@ int fd3d_batch_remove(fd3d_batch* b, int slot) {
 int fd3d_batch_reset(fd3d_batch* b, int slot) {
     if (!b || slot < 0 || slot >= (int)b->models.size() || !b->models[slot].live) return FD3D_ERR_ARG;
     std::lock_guard<std::mutex> lk(b->mu);
-    int rc = reset_model(b, b->models[slot]);
+    int rc = reset_model(b, b->models[slot], b->st);
     if (rc) return rc;
     BCK(cudaStreamSynchronize(b->st));
     return FD3D_OK;
@@ -1140,7 +1145,7 @@ int fd3d_batch_autotune(fd3d_batch* b, int steps, const char* cache_path, const 
         if (rc) return rc;
         if (b->last_ms < best) { best = b->last_ms; bt = b->tun; }
         for (size_t m = 0; m < b->models.size(); ++m)
-            if (b->models[m].live) { rc = reset_model(b, b->models[m]); if (rc) return rc; }
+            if (b->models[m].live) { rc = reset_model(b, b->models[m], b->st); if (rc) return rc; }
         BCK(cudaStreamSynchronize(b->st));
     }
     b->tun = bt;
