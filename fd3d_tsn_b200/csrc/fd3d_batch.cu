@@ -150,8 +150,8 @@ k_batch(const ModelDev* __restrict__ models, const ModelMaps* __restrict__ maps,
                 bool ok = true;
                 switch (type) {
                     case W_VEL_INT:
-                        ok = vel_interior_tma_body<float>(maps[m].v, M.g, M.f, M.c, kchunk, it.bx, it.by, it.bz, ring,
-                                                          bars, pc, gstatus);
+                        ok = vel_interior_tma_body<float, true>(maps[m].v, M.g, M.f, M.c, kchunk, it.bx, it.by, it.bz,
+                                                                ring, bars, pc, gstatus);
                         break;
                     case W_VEL_FAULT:
                         vel_fault_body<float>(M.g, M.f, M.q, M.c, M.law, M.fs, M.it_dev, M.status, it.bx, it.by, 0);
@@ -163,8 +163,8 @@ k_batch(const ModelDev* __restrict__ models, const ModelMaps* __restrict__ maps,
                         break;
                     case W_VEL_FS: vel_fs_body<float>(M.g, M.f, it.bx, it.by, 0); break;
                     case W_STR_INT:
-                        ok = str_interior_tma_body<float>(maps[m].s, M.g, M.f, M.c, kchunk, it.bx, it.by, it.bz, ring,
-                                                          bars, pc, gstatus);
+                        ok = str_interior_tma_body<float, true>(maps[m].s, M.g, M.f, M.c, kchunk, it.bx, it.by, it.bz,
+                                                                ring, bars, pc, gstatus);
                         break;
                     case W_STR_FAULT: str_fault_body<float>(M.g, M.f, M.q, M.c, it.bx, it.by, 0); break;
                     case W_STR_PML:
@@ -218,9 +218,11 @@ __global__ void __launch_bounds__(256) k_bint(const ModelDev* __restrict__ model
     const ModelDev& M = models[m];
     unsigned pc = 0;
     if (STRESS)
-        str_interior_tma_body<float>(maps[m].s, M.g, M.f, M.c, kchunk, it.bx, it.by, it.bz, ring, bars, pc, gstatus);
+        str_interior_tma_body<float, true>(maps[m].s, M.g, M.f, M.c, kchunk, it.bx, it.by, it.bz, ring, bars, pc,
+                                           gstatus);
     else
-        vel_interior_tma_body<float>(maps[m].v, M.g, M.f, M.c, kchunk, it.bx, it.by, it.bz, ring, bars, pc, gstatus);
+        vel_interior_tma_body<float, true>(maps[m].v, M.g, M.f, M.c, kchunk, it.bx, it.by, it.bz, ring, bars, pc,
+                                           gstatus);
 }
 
 template <bool STRESS>
@@ -826,7 +828,7 @@ int fd3d_batch_add(fd3d_batch* b, const fd3d_params* pin, const double* lam_k, c
     float* lam = fp + 9 * (size_t)d.g.n3;
     float* mu = fp + 10 * (size_t)d.g.n3;
     float* dd = fp + 11 * (size_t)d.g.n3;
-    d.f.lam = lam; d.f.mu = mu; d.f.d = dd;
+    d.f.lam = lam; d.f.mu = mu; d.f.d = dd;  // d.f.lay: the layer table, set below
     float** fq[NF_PLANES] = {&d.q.tx, &d.q.tz, &d.q.txt, &d.q.tzt, &d.q.RFx, &d.q.RFz, &d.q.avdx, &d.q.avdz, &d.q.v1t,
                              &d.q.au1, &d.q.av1, &d.q.aw1, &d.q.uZ, &d.q.wX, &d.q.tabsX, &d.q.tabsZ, &d.q.T0X,
                              &d.q.T0Z, &d.q.T0Xb, &d.q.Dc, &d.q.peakX, &d.q.dynX, &d.q.DcX, &d.q.peakZ, &d.q.dynZ,
@@ -844,6 +846,7 @@ int fd3d_batch_add(fd3d_batch* b, const fd3d_params* pin, const double* lam_k, c
     float* ring = bp.take<float>((size_t)M.cap * M.nf * plane);
     float* seis = bp.take<float>((size_t)M.cap * std::max(1, p.nstations) * 3);
     float* layers = bp.take<float>((size_t)3 * p.nzt);
+    d.f.lay = layers;  // batch models always carry a 1-D medium
     d.it_dev = bp.take<int>(1);
     d.status = bp.take<int>(1);
     d.h.ring = ring; d.h.cap = M.cap; d.h.stride = p.history_stride; d.h.nf = M.nf; d.h.nst = p.nstations;

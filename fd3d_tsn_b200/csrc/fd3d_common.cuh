@@ -54,6 +54,11 @@ template <class T>
 struct Fields {
     T *u, *v, *w, *xx, *yy, *zz, *xy, *yz, *xz;
     const T *lam, *mu, *d;
+    // The same medium as a 1-D profile when it varies with k only (the layered medium
+    // of readcrustalmodel): lam at lay[k-1], mu at lay[nzt+k-1], d at lay[2*nzt+k-1];
+    // null otherwise.  The interior sweeps then read three values per plane instead of
+    // three arrays per cell.
+    const T* lay;
 };
 
 // Fault-plane state.  F = field type, double = accumulators (slip, slip path,

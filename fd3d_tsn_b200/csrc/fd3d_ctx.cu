@@ -32,6 +32,28 @@ using namespace fd3d;
 
 namespace fd3d {
 
+// Whether the uploaded medium varies with k only: every (i,j) of a plane k equals
+// (1,1,k) in all three arrays (sets *nonuniform otherwise); the profile of column (1,1)
+// goes to tab (lam, mu, d, nzt values each).
+template <class T>
+__global__ void k_layer_check(Grid g, const T* lam, const T* mu, const T* d, T* tab, int* nonuniform) {
+    const long long n = (long long)g.nxt * g.nyt * g.nzt;
+    int bad = 0;
+    for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
+        const int i = 1 + (int)(q % g.nxt);
+        const long long r = q / g.nxt;
+        const int j = 1 + (int)(r % g.nyt), k = 1 + (int)(r / g.nyt);
+        const long long p = g.at(i, j, k), p0 = g.at(1, 1, k);
+        bad |= (lam[p] != lam[p0]) | (mu[p] != mu[p0]) | (d[p] != d[p0]);
+        if (i == 1 && j == 1) {
+            tab[k - 1] = lam[p0];
+            tab[g.nzt + k - 1] = mu[p0];
+            tab[2 * g.nzt + k - 1] = d[p0];
+        }
+    }
+    if (__syncthreads_or(bad) && threadIdx.x == 0) atomicOr(nonuniform, 1);
+}
+
 struct CtxBase {
     fd3d_params p;
     Grid g;
@@ -88,6 +110,8 @@ struct Ctx : CtxBase {
     // aligned arrays; a request beyond it gets its own allocation.
     char* block = nullptr;
     size_t block_bytes = 0, block_used = 0;
+    T* dlay = nullptr;      // 1-D medium profile (Fields::lay) when the medium is layered
+    int* lflag = nullptr;   // result word of the layered-medium check
     static size_t carve(size_t bytes) { return (std::max<size_t>(bytes, 1) + 255) & ~(size_t)255; }
     template <class U> int dalloc(U** ptr, size_t n) {
         const size_t bytes = carve(n * sizeof(U));
@@ -142,7 +166,8 @@ struct Ctx : CtxBase {
                           9 * carve(n2 * sizeof(double)) + carve(pml_aux_elems(D) * sizeof(T)) +
                           carve(prof.size() * sizeof(Damp<T>)) + 2 * carve(sizeof(int)) +
                           carve((size_t)cap * nf * plane * sizeof(T)) +
-                          carve((size_t)cap * std::max(1, p.nstations) * 3 * sizeof(T));
+                          carve((size_t)cap * std::max(1, p.nstations) * 3 * sizeof(T)) +
+                          carve((size_t)3 * p.nzt * sizeof(T)) + carve(sizeof(int));
             void* v = nullptr;
             if (cudaMalloc(&v, block_bytes) != cudaSuccess) { cudaGetLastError(); return FD3D_ERR_NOMEM; }
             block = (char*)v;
@@ -181,7 +206,25 @@ struct Ctx : CtxBase {
         T* sg = nullptr;
         if (dalloc(&sg, (size_t)cap * std::max(1, p.nstations) * 3)) return FD3D_ERR_NOMEM;
         seis = sg;
+        if (dalloc(&dlay, (size_t)3 * p.nzt)) return FD3D_ERR_NOMEM;
+        if (dalloc(&lflag, 1)) return FD3D_ERR_NOMEM;
         CK(cudaStreamSynchronize(st));
+        return FD3D_OK;
+    }
+
+    // After a medium upload: the kernels read the 1-D profile when the medium is layered
+    // (checked on the device), and graphs captured with the old medium are dropped.
+    int medium_uploaded() {
+        int nonuni = 0;
+        CK(cudaMemsetAsync(lflag, 0, sizeof(int), st));
+        k_layer_check<T><<<1024, 256, 0, st>>>(g, f.lam, f.mu, f.d, dlay, lflag);
+        CK(cudaGetLastError());
+        CK(cudaMemcpyAsync(&nonuni, lflag, sizeof(int), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        f.lay = nonuni ? nullptr : dlay;
+        for (cudaGraphExec_t& gx : gexec)
+            if (gx) { cudaGraphExecDestroy(gx); gx = nullptr; }
+        medium_ok = true;
         return FD3D_OK;
     }
 
@@ -198,8 +241,7 @@ struct Ctx : CtxBase {
                                      (size_t)p.nxt * sizeof(T), (size_t)p.nyt * p.nzt, cudaMemcpyHostToDevice, st));
             }
             CK(cudaStreamSynchronize(st));
-            medium_ok = true;
-            return FD3D_OK;
+            return medium_uploaded();
         }
         std::vector<T> row((size_t)g.px * p.nyt * 16);
         for (int a = 0; a < 3; ++a) {
@@ -222,8 +264,7 @@ struct Ctx : CtxBase {
             }
         }
         (void)n;
-        medium_ok = true;
-        return FD3D_OK;
+        return medium_uploaded();
     }
 
     int upload_medium_layers(const double* l, const double* m, const double* d) override {
@@ -241,8 +282,7 @@ struct Ctx : CtxBase {
                                    cudaMemcpyHostToDevice, st));
                 CK(cudaStreamSynchronize(st));
             }
-        medium_ok = true;
-        return FD3D_OK;
+        return medium_uploaded();
     }
 
     int up2(T* dst, const std::vector<T>& v) {

@@ -426,8 +426,10 @@ template <class T>
 bool prepare_tma_kernels() {
     const int vs = TMA_NS * VelSlot::ELEMS * (int)sizeof(T) + TMA_SMEM_PAD,
               ss = TMA_NS * StrSlot::ELEMS * (int)sizeof(T) + TMA_SMEM_PAD;
-    bool ok = cudaFuncSetAttribute(k_vel_interior_tma<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, vs) == cudaSuccess;
-    ok &= cudaFuncSetAttribute(k_str_interior_tma<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, ss) == cudaSuccess;
+    bool ok = cudaFuncSetAttribute(k_vel_interior_tma<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, vs) == cudaSuccess;
+    ok &= cudaFuncSetAttribute(k_str_interior_tma<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, ss) == cudaSuccess;
+    ok &= cudaFuncSetAttribute(k_vel_interior_tma<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, vs) == cudaSuccess;
+    ok &= cudaFuncSetAttribute(k_str_interior_tma<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, ss) == cudaSuccess;
     if (!ok) cudaGetLastError();
     return ok;
 }
@@ -438,7 +440,9 @@ void launch_vel_interior_tma(const VelMaps& M, const InteriorCfg& cfg, const Gri
     const int nxT = g.nxt - 2 * g.nabc, nyI = g.nyt - 2 - g.nabc, nzT = interior_nz(g);
     const int kch = std::max(1, std::min(cfg.kchunk, nzT));
     dim3 grid((nxT + 31) / 32, (nyI + 7) / 8, (nzT + kch - 1) / kch);
-    k_vel_interior_tma<T><<<grid, dim3(32, 8), TMA_NS * VelSlot::ELEMS * sizeof(T) + TMA_SMEM_PAD, st>>>(M, g, f, c, kch, status);
+    const size_t sm = TMA_NS * VelSlot::ELEMS * sizeof(T) + TMA_SMEM_PAD;
+    if (f.lay) k_vel_interior_tma<T, true><<<grid, dim3(32, 8), sm, st>>>(M, g, f, c, kch, status);
+    else k_vel_interior_tma<T, false><<<grid, dim3(32, 8), sm, st>>>(M, g, f, c, kch, status);
 }
 
 template <class T>
@@ -447,7 +451,9 @@ void launch_str_interior_tma(const StrMaps& M, const InteriorCfg& cfg, const Gri
     const int nxT = g.nxt - 2 * g.nabc, nyI = g.nyt - 2 - g.nabc, nzT = interior_nz(g);
     const int kch = std::max(1, std::min(cfg.kchunk_str, nzT));
     dim3 grid((nxT + 31) / 32, (nyI + 7) / 8, (nzT + kch - 1) / kch);
-    k_str_interior_tma<T><<<grid, dim3(32, 8), TMA_NS * StrSlot::ELEMS * sizeof(T) + TMA_SMEM_PAD, st>>>(M, g, f, c, kch, status);
+    const size_t sm = TMA_NS * StrSlot::ELEMS * sizeof(T) + TMA_SMEM_PAD;
+    if (f.lay) k_str_interior_tma<T, true><<<grid, dim3(32, 8), sm, st>>>(M, g, f, c, kch, status);
+    else k_str_interior_tma<T, false><<<grid, dim3(32, 8), sm, st>>>(M, g, f, c, kch, status);
 }
 
 }  // namespace fd3d

@@ -46,16 +46,16 @@ struct VelSlot {
     static constexpr int LOADED = 320 + 440 + 352 + 320 + 352 + 4 * 256;  // elements the 9 tiles bring
 };
 
-template <class T>
+template <class T, bool LAYERED>
 __device__ __forceinline__ void vel_issue(const VelMaps& M, T* slot, uint32_t bar, int x0, int y0, int k) {
-    mbar_expect_tx(bar, VelSlot::LOADED * sizeof(T));
+    mbar_expect_tx(bar, (VelSlot::LOADED - (LAYERED ? 256 : 0)) * sizeof(T));
     const int z = k - 1;
     tma_load_3d(smem_addr(slot + VelSlot::XX), &M.xx, x0 - 4, y0, z, bar);
     tma_load_3d(smem_addr(slot + VelSlot::XY), &M.xy, x0 - 4, y0 - 2, z, bar);
     tma_load_3d(smem_addr(slot + VelSlot::YY), &M.yy, x0, y0 - 1, z, bar);
     tma_load_3d(smem_addr(slot + VelSlot::XZ), &M.xz, x0 - 4, y0, z, bar);
     tma_load_3d(smem_addr(slot + VelSlot::YZ), &M.yz, x0, y0 - 2, z, bar);
-    tma_load_3d(smem_addr(slot + VelSlot::D), &M.d, x0, y0, z, bar);
+    if (!LAYERED) tma_load_3d(smem_addr(slot + VelSlot::D), &M.d, x0, y0, z, bar);
     tma_load_3d(smem_addr(slot + VelSlot::U), &M.u, x0, y0, z, bar);
     tma_load_3d(smem_addr(slot + VelSlot::V), &M.v, x0, y0, z, bar);
     tma_load_3d(smem_addr(slot + VelSlot::W), &M.w, x0, y0, z, bar);
@@ -85,7 +85,7 @@ __device__ __forceinline__ void tma_drain_pc(const uint64_t* bars, unsigned pc, 
 
 // One 32 x 8 x kchunk tile of the velocity sweep through the ring.  Returns false if a
 // wait timed out (ST_TIMEOUT is recorded; the caller stops).
-template <class T>
+template <class T, bool LAYERED = false>
 __device__ __forceinline__ bool vel_interior_tma_body(const VelMaps& M, const Grid& g, const Fields<T>& f,
                                                       const StepConst<T>& c, int kchunk, int bx_, int by_, int bz_,
                                                       T* ring, uint64_t* bars, unsigned& pc, int* status) {
@@ -101,7 +101,7 @@ __device__ __forceinline__ bool vel_interior_tma_body(const VelMaps& M, const Gr
     if (leader)
         for (int k = kb; k <= min(ke, kb + TMA_NS - 1); ++k) {
             const unsigned n = p0 + (unsigned)(k - kb);
-            vel_issue<T>(M, ring + (size_t)ring_slot(n) * VelSlot::ELEMS, smem_addr(&bars[ring_slot(n)]), x0, y0, k);
+            vel_issue<T, LAYERED>(M, ring + (size_t)ring_slot(n) * VelSlot::ELEMS, smem_addr(&bars[ring_slot(n)]), x0, y0, k);
         }
     // z queues of the own column (plain loads, one plane ahead)
     const int ic = min(i, g.nxt), jc = min(j, g.nyt);
@@ -121,6 +121,7 @@ __device__ __forceinline__ bool vel_interior_tma_body(const VelMaps& M, const Gr
         xq0 = xq1; xq1 = xq2; xq2 = xq3; xq3 = nx;
         yq0 = yq1; yq1 = yq2; yq2 = yq3; yq3 = ny;
         if (k < ke) { nz = zz[pk + 3 * sz]; nx = xz[pk + 2 * sz]; ny = yz[pk + 2 * sz]; }
+        const T dk = LAYERED ? f.lay[2 * g.nzt + k - 1] : (T)0;  // density of plane k (1-D medium)
         if (!mbar_wait(smem_addr(&bars[s]), ring_parity(gn))) {
             atomicOr(status, ST_TIMEOUT);
             tma_drain_pc(bars, p0, k, ke, kb);
@@ -134,7 +135,7 @@ __device__ __forceinline__ bool vel_interior_tma_body(const VelMaps& M, const Gr
             const T* sxz = sl + VelSlot::XZ + ty * 40 + tx;
             const T* syz = sl + VelSlot::YZ + (ty + 2) * 32 + tx;
             const int o = ty * 32 + tx;
-            const T r = dth / sl[VelSlot::D + o];
+            const T r = dth / (LAYERED ? dk : sl[VelSlot::D + o]);
             f.u[pk] = sl[VelSlot::U + o] +
                       r * (c1 * (sxx[4] - sxx[3]) + c2 * (sxx[5] - sxx[2]) + c1 * (sxy[4] - sxy[-40 + 4]) +
                            c2 * (sxy[40 + 4] - sxy[-80 + 4]) + c1 * (xq2 - xq1) + c2 * (xq3 - xq0));
@@ -148,14 +149,14 @@ __device__ __forceinline__ bool vel_interior_tma_body(const VelMaps& M, const Gr
         __syncthreads();  // every thread is done with slot s
         if (leader && k + TMA_NS <= ke) {
             fence_proxy_async_smem();
-            vel_issue<T>(M, ring + (size_t)s * VelSlot::ELEMS, smem_addr(&bars[s]), x0, y0, k + TMA_NS);
+            vel_issue<T, LAYERED>(M, ring + (size_t)s * VelSlot::ELEMS, smem_addr(&bars[s]), x0, y0, k + TMA_NS);
         }
     }
     pc = p0 + (unsigned)(ke - kb + 1);
     return true;
 }
 
-template <class T>
+template <class T, bool LAYERED>
 __global__ void __launch_bounds__(256) k_vel_interior_tma(const __grid_constant__ VelMaps M, Grid g, Fields<T> f,
                                                            StepConst<T> c, int kchunk, int* status) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -164,7 +165,7 @@ __global__ void __launch_bounds__(256) k_vel_interior_tma(const __grid_constant_
     __shared__ __align__(8) uint64_t bars[TMA_NS];
     tma_ring_init(bars);
     unsigned pc = 0;
-    vel_interior_tma_body<T>(M, g, f, c, kchunk, blockIdx.x, blockIdx.y, blockIdx.z, ring, bars, pc, status);
+    vel_interior_tma_body<T, LAYERED>(M, g, f, c, kchunk, blockIdx.x, blockIdx.y, blockIdx.z, ring, bars, pc, status);
 }
 
 // Stress slot layout (elements)
@@ -178,24 +179,24 @@ struct StrSlot {
     static constexpr int LOADED = 3520;
 };
 
-template <class T>
+template <class T, bool LAYERED>
 __device__ __forceinline__ void str_issue(const StrMaps& M, T* slot, uint32_t bar, int x0, int y0, int k) {
-    mbar_expect_tx(bar, StrSlot::LOADED * sizeof(T));
+    mbar_expect_tx(bar, (StrSlot::LOADED - (LAYERED ? 256 + 288 : 0)) * sizeof(T));
     const int z = k - 1;
     tma_load_3d(smem_addr(slot + StrSlot::U), &M.u, x0 - 4, y0 - 2, z, bar);
     tma_load_3d(smem_addr(slot + StrSlot::V), &M.v, x0 - 4, y0 - 2, z, bar);
     tma_load_3d(smem_addr(slot + StrSlot::W), &M.w, x0 - 4, y0 - 2, z, bar);
-    tma_load_3d(smem_addr(slot + StrSlot::LAM), &M.lam, x0, y0, z, bar);
+    if (!LAYERED) tma_load_3d(smem_addr(slot + StrSlot::LAM), &M.lam, x0, y0, z, bar);
     tma_load_3d(smem_addr(slot + StrSlot::XX), &M.xx, x0, y0, z, bar);
     tma_load_3d(smem_addr(slot + StrSlot::YY), &M.yy, x0, y0, z, bar);
     tma_load_3d(smem_addr(slot + StrSlot::ZZ), &M.zz, x0, y0, z, bar);
     tma_load_3d(smem_addr(slot + StrSlot::XY), &M.xy, x0, y0, z, bar);
     tma_load_3d(smem_addr(slot + StrSlot::XZ), &M.xz, x0, y0, z, bar);
     tma_load_3d(smem_addr(slot + StrSlot::YZ), &M.yz, x0, y0, z, bar);
-    tma_load_3d(smem_addr(slot + StrSlot::MU), &M.mu, x0, y0, z, bar);
+    if (!LAYERED) tma_load_3d(smem_addr(slot + StrSlot::MU), &M.mu, x0, y0, z, bar);
 }
 
-template <class T>
+template <class T, bool LAYERED = false>
 __device__ __forceinline__ bool str_interior_tma_body(const StrMaps& M, const Grid& g, const Fields<T>& f,
                                                       const StepConst<T>& c, int kchunk, int bx_, int by_, int bz_,
                                                       T* ring, uint64_t* bars, unsigned& pc, int* status) {
@@ -211,7 +212,7 @@ __device__ __forceinline__ bool str_interior_tma_body(const StrMaps& M, const Gr
     if (leader)
         for (int k = kb; k <= min(ke, kb + TMA_NS - 1); ++k) {
             const unsigned n = p0 + (unsigned)(k - kb);
-            str_issue<T>(M, ring + (size_t)ring_slot(n) * StrSlot::ELEMS, smem_addr(&bars[ring_slot(n)]), x0, y0, k);
+            str_issue<T, LAYERED>(M, ring + (size_t)ring_slot(n) * StrSlot::ELEMS, smem_addr(&bars[ring_slot(n)]), x0, y0, k);
         }
     const int ic = min(i, g.nxt - 1), jc = min(j, g.nyt - 1);  // keeps the (i+1,j+1) tap in range
     const long long sy = g.px, sz = g.plane;
@@ -221,7 +222,7 @@ __device__ __forceinline__ bool str_interior_tma_body(const StrMaps& M, const Gr
     T uq0, uq1 = u[pcol - sz], uq2 = u[pcol], uq3 = u[pcol + sz], nu = u[pcol + 2 * sz];
     T vq0, vq1 = v[pcol - sz], vq2 = v[pcol], vq3 = v[pcol + sz], nv = v[pcol + 2 * sz];
     T wq0, wq1 = w[pcol - 2 * sz], wq2 = w[pcol - sz], wq3 = w[pcol], nw = w[pcol + sz];
-    T mq1 = mu[pcol + sz], pmd = mu[pcol + 1 + sy + sz];
+    T mq1 = LAYERED ? (T)0 : mu[pcol + sz], pmd = LAYERED ? (T)0 : mu[pcol + 1 + sy + sz];
     const T c1 = c.c1, c2 = c.c2, dth = c.dth;
     for (int k = kb; k <= ke; ++k) {
         const int n = k - kb;
@@ -235,8 +236,11 @@ __device__ __forceinline__ bool str_interior_tma_body(const StrMaps& M, const Gr
         if (k < ke) {
             const long long pn = pk + sz;
             nu = u[pn + 2 * sz]; nv = v[pn + 2 * sz]; nw = w[pn + sz];
-            mq1 = mu[pn + sz]; pmd = mu[pn + 1 + sy + sz];
+            if (!LAYERED) { mq1 = mu[pn + sz]; pmd = mu[pn + 1 + sy + sz]; }
         }
+        // 1-D medium: lam, mu of plane k and mu of plane k+1 (every (i,j) of a plane is equal)
+        const T lk = LAYERED ? f.lay[k - 1] : (T)0, mk = LAYERED ? f.lay[g.nzt + k - 1] : (T)0;
+        const T mk1 = LAYERED ? f.lay[g.nzt + k] : (T)0;
         if (!mbar_wait(smem_addr(&bars[s]), ring_parity(gn))) {
             atomicOr(status, ST_TIMEOUT);
             tma_drain_pc(bars, p0, k, ke, kb);
@@ -248,7 +252,7 @@ __device__ __forceinline__ bool str_interior_tma_body(const StrMaps& M, const Gr
             const T* sv = sl + StrSlot::V + (ty + 2) * 40 + tx + 4;
             const T* sw = sl + StrSlot::W + (ty + 2) * 40 + tx + 4;
             const int o = ty * 32 + tx;
-            const T xl = sl[StrSlot::LAM + o], xm = sl[StrSlot::MU + o];
+            const T xl = LAYERED ? lk : sl[StrSlot::LAM + o], xm = LAYERED ? mk : sl[StrSlot::MU + o];
             const T a = xl + (T)2 * xm, b = xl;
             const T dxu1 = c1 * (su[1] - su[0]), dxu2 = c2 * (su[2] - su[-1]);
             const T dyv1 = c1 * (sv[0] - sv[-40]), dyv2 = c2 * (sv[40] - sv[-80]);
@@ -256,27 +260,27 @@ __device__ __forceinline__ bool str_interior_tma_body(const StrMaps& M, const Gr
             f.xx[pk] = sl[StrSlot::XX + o] + dth * a * (dxu1 + dxu2) + dth * b * (dyv1 + dyv2 + dzw1 + dzw2);
             f.yy[pk] = sl[StrSlot::YY + o] + dth * a * (dyv1 + dyv2) + dth * b * (dxu1 + dxu2 + dzw1 + dzw2);
             f.zz[pk] = sl[StrSlot::ZZ + o] + dth * a * (dzw1 + dzw2) + dth * b * (dxu1 + dxu2 + dyv1 + dyv2);
-            T xmu = (T)0.5 * (xm + sl[StrSlot::MU + o + 32]);
+            T xmu = (T)0.5 * (xm + (LAYERED ? mk : sl[StrSlot::MU + o + 32]));
             f.xy[pk] = sl[StrSlot::XY + o] + dth * xmu * (c1 * (su[40] - su[0]) + c2 * (su[80] - su[-40]) +
                                                           c1 * (sv[0] - sv[-1]) + c2 * (sv[1] - sv[-2]));
-            xmu = (T)0.5 * (xm + cm1);
+            xmu = (T)0.5 * (xm + (LAYERED ? mk1 : cm1));
             f.xz[pk] = sl[StrSlot::XZ + o] + dth * xmu * (c1 * (uq2 - uq1) + c2 * (uq3 - uq0) +
                                                           c1 * (sw[0] - sw[-1]) + c2 * (sw[1] - sw[-2]));
-            xmu = (T)0.5 * (xm + cmd);
+            xmu = (T)0.5 * (xm + (LAYERED ? mk1 : cmd));
             f.yz[pk] = sl[StrSlot::YZ + o] + dth * xmu * (c1 * (vq2 - vq1) + c2 * (vq3 - vq0) +
                                                           c1 * (sw[40] - sw[0]) + c2 * (sw[80] - sw[-40]));
         }
         __syncthreads();
         if (leader && k + TMA_NS <= ke) {
             fence_proxy_async_smem();
-            str_issue<T>(M, ring + (size_t)s * StrSlot::ELEMS, smem_addr(&bars[s]), x0, y0, k + TMA_NS);
+            str_issue<T, LAYERED>(M, ring + (size_t)s * StrSlot::ELEMS, smem_addr(&bars[s]), x0, y0, k + TMA_NS);
         }
     }
     pc = p0 + (unsigned)(ke - kb + 1);
     return true;
 }
 
-template <class T>
+template <class T, bool LAYERED>
 __global__ void __launch_bounds__(256) k_str_interior_tma(const __grid_constant__ StrMaps M, Grid g, Fields<T> f,
                                                            StepConst<T> c, int kchunk, int* status) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -285,7 +289,7 @@ __global__ void __launch_bounds__(256) k_str_interior_tma(const __grid_constant_
     __shared__ __align__(8) uint64_t bars[TMA_NS];
     tma_ring_init(bars);
     unsigned pc = 0;
-    str_interior_tma_body<T>(M, g, f, c, kchunk, blockIdx.x, blockIdx.y, blockIdx.z, ring, bars, pc, status);
+    str_interior_tma_body<T, LAYERED>(M, g, f, c, kchunk, blockIdx.x, blockIdx.y, blockIdx.z, ring, bars, pc, status);
 }
 
 // dynamic shared memory of a CTA that runs both sweeps through one ring
