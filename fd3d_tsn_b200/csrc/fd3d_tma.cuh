@@ -24,7 +24,10 @@ namespace fd3d {
 struct VelMaps { CUtensorMap xx, xy, yy, xz, yz, d, u, v, w; };
 struct StrMaps { CUtensorMap u, v, w, lam, mu, xx, yy, zz, xy, xz, yz; };
 
-constexpr int TMA_NS = 3;            // ring slots: plane k computed, k+1 and k+2 in flight
+#ifndef FD3D_TMA_NS
+#define FD3D_TMA_NS 3
+#endif
+constexpr int TMA_NS = FD3D_TMA_NS;  // ring slots: plane k computed, the next ones in flight
 constexpr int TMA_SMEM_PAD = 128;  // alignment slack of the dynamic ring
 
 __device__ __forceinline__ void tma_load_3d(uint32_t dst, const CUtensorMap* map, int x, int y, int z, uint32_t bar) {
