@@ -26,7 +26,7 @@ HIST_NAMES = ["sliprateX", "sliprateZ", "shearstressX", "shearstressZ", "psi"]
 FIELDS = {"u": 0, "v": 1, "w": 2, "xx": 3, "yy": 4, "zz": 5, "xy": 6, "yz": 7, "xz": 8}
 PLANES = {"tx": 0, "tz": 1, "slipX": 2, "slipZ": 3, "ruptime": 4, "rise": 5, "sliptime": 6,
           "distX": 7, "distZ": 8, "psiX": 9, "psiZ": 10, "T0X": 11, "T0Z": 12,
-          "schangeX": 13, "schangeZ": 14}
+          "schangeX": 13, "schangeZ": 14, "rvel": 15, "czone": 16}
 NKERNELS = 8
 KERNEL_NAMES = ["vel_interior", "vel_fault", "vel_pml", "vel_fs",
                 "str_interior", "str_fault", "str_pml", "fault_bc"]
@@ -148,6 +148,8 @@ def load_library(path: str | None = None) -> C.CDLL:
         "fd3d_read_deck": (i, [C.c_char_p, C.POINTER(Params), C.POINTER(dp), C.POINTER(dp), C.POINTER(dp)]),
         "fd3d_free": (None, [vp]),
         "fd3d_check_division": (i, [fp, i, C.POINTER(C.c_ulonglong), C.POINTER(C.c_uint)]),
+        "fd3d_fetch_moment_rate": (i, [vp, i, i, dp]),
+        "fd3d_post_process": (i, [vp, dp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

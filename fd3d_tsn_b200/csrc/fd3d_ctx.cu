@@ -15,6 +15,7 @@
 #include "fd3d_common.cuh"
 #include "fd3d_kernels.cuh"
 #include "fd3d_opt.cuh"
+#include "fd3d_post.cuh"
 #include "fd3d_setup.h"
 #include "fd3d_host.h"
 
@@ -87,6 +88,8 @@ struct CtxBase {
     virtual int enqueue_step() = 0;
     virtual int fetch_field(int, void*, int) = 0;
     virtual int fetch_plane(int, double*) = 0;
+    virtual int moment_rate(int rec0, int nrec, double* host) = 0;
+    virtual int post(double* out4) = 0;
     virtual size_t elem() const = 0;
 };
 
@@ -112,6 +115,10 @@ struct Ctx : CtxBase {
     size_t block_bytes = 0, block_used = 0;
     T* dlay = nullptr;      // 1-D medium profile (Fields::lay) when the medium is layered
     int* lflag = nullptr;   // result word of the layered-medium check
+    // fault-plane observables (fd3d_post.cuh): rupture velocity and cohesive-zone planes,
+    // partial and final sums of the post-loop quantities, moment rate of ring records
+    static constexpr int POST_BLOCKS = 148;
+    double *rvel_d = nullptr, *czone_d = nullptr, *part_d = nullptr, *sums_d = nullptr, *mrate_d = nullptr;
     static size_t carve(size_t bytes) { return (std::max<size_t>(bytes, 1) + 255) & ~(size_t)255; }
     template <class U> int dalloc(U** ptr, size_t n) {
         const size_t bytes = carve(n * sizeof(U));
@@ -167,7 +174,9 @@ struct Ctx : CtxBase {
                           carve(prof.size() * sizeof(Damp<T>)) + 2 * carve(sizeof(int)) +
                           carve((size_t)cap * nf * plane * sizeof(T)) +
                           carve((size_t)cap * std::max(1, p.nstations) * 3 * sizeof(T)) +
-                          carve((size_t)3 * p.nzt * sizeof(T)) + carve(sizeof(int));
+                          carve((size_t)3 * p.nzt * sizeof(T)) + carve(sizeof(int)) + 2 * carve(n2 * sizeof(double)) +
+                          carve((size_t)POST_BLOCKS * POST_NSUM * sizeof(double)) + carve(POST_NSUM * sizeof(double)) +
+                          carve((size_t)cap * sizeof(double));
             void* v = nullptr;
             if (cudaMalloc(&v, block_bytes) != cudaSuccess) { cudaGetLastError(); return FD3D_ERR_NOMEM; }
             block = (char*)v;
@@ -208,6 +217,9 @@ struct Ctx : CtxBase {
         seis = sg;
         if (dalloc(&dlay, (size_t)3 * p.nzt)) return FD3D_ERR_NOMEM;
         if (dalloc(&lflag, 1)) return FD3D_ERR_NOMEM;
+        if (dalloc(&rvel_d, n2) || dalloc(&czone_d, n2) || dalloc(&part_d, (size_t)POST_BLOCKS * POST_NSUM) ||
+            dalloc(&sums_d, POST_NSUM) || dalloc(&mrate_d, (size_t)cap))
+            return FD3D_ERR_NOMEM;
         CK(cudaStreamSynchronize(st));
         return FD3D_OK;
     }
@@ -477,6 +489,7 @@ struct Ctx : CtxBase {
             case FD3D_PLANE_PSIX: ds = q.psiX; break;        case FD3D_PLANE_PSIZ: ds = q.psiZ; break;
             case FD3D_PLANE_T0X: ts = q.T0X; break;          case FD3D_PLANE_T0Z: ts = q.T0Z; break;
             case FD3D_PLANE_SCHANGEX: ts = q.schangeX; break; case FD3D_PLANE_SCHANGEZ: ts = q.schangeZ; break;
+            case FD3D_PLANE_RVEL: ds = rvel_d; break;        case FD3D_PLANE_CZONE: ds = czone_d; break;
             default: return FD3D_ERR_ARG;
         }
         if (ds) {
@@ -488,6 +501,33 @@ struct Ctx : CtxBase {
             CK(cudaStreamSynchronize(st));
             for (size_t k = 0; k < n2; ++k) host[k] = (double)v[k];
         }
+        return FD3D_OK;
+    }
+
+    int moment_rate(int rec0, int nrec, double* host) override {
+        for (int r0 = 0; r0 < nrec; r0 += hist_cap) {  // at most one ring of records per pass
+            const int n = std::min(hist_cap, nrec - r0);
+            k_moment_rate<T><<<n, POST_THREADS, 0, st>>>(g, f, (const T*)ring, hist_cap, nf, rec0 + r0, (double)c.dh,
+                                                         mrate_d);
+            CK(cudaGetLastError());
+            CK(cudaMemcpyAsync(host + r0, mrate_d, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, st));
+            CK(cudaStreamSynchronize(st));
+        }
+        return FD3D_OK;
+    }
+
+    int post(double* out4) override {
+        const double dh2 = (double)(c.dh * c.dh);  // dh*dh in the field type, as the reference
+        k_post<T><<<POST_BLOCKS, POST_THREADS, 0, st>>>(g, f, q, (double)c.dh, dh2, rvel_d, czone_d, part_d);
+        k_post_sum<<<1, POST_THREADS, 0, st>>>(part_d, POST_BLOCKS, sums_d);
+        CK(cudaGetLastError());
+        double s[POST_NSUM];
+        CK(cudaMemcpyAsync(s, sums_d, sizeof(s), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        out4[0] = s[3] / s[4];                          // average rupture speed (tint / tint2)
+        out4[1] = s[0];                                 // seismic moment M0
+        out4[2] = 0.0;                                  // rupture area: never set by the reference
+        out4[3] = s[2] != 0.0 ? -(s[1] / s[2]) : 0.0;   // average stress drop
         return FD3D_OK;
     }
 };
@@ -743,6 +783,19 @@ int fd3d_fetch_plane(fd3d_ctx* ctx, int plane, double* host) {
     if (!ctx || !host) return FD3D_ERR_ARG;
     CK(cudaStreamSynchronize(ctx->impl->st));
     return ctx->impl->fetch_plane(plane, host);
+}
+
+int fd3d_fetch_moment_rate(fd3d_ctx* ctx, int rec0, int nrec, double* host) {
+    if (!ctx || !host || nrec < 0 || rec0 < 0) return FD3D_ERR_ARG;
+    CtxBase* c = ctx->impl;
+    const int have = c->steps_done / c->p.history_stride;
+    if (rec0 + nrec > have || rec0 < have - c->hist_cap) return FD3D_ERR_ARG;  // overwritten or not yet made
+    return c->moment_rate(rec0, nrec, host);
+}
+
+int fd3d_post_process(fd3d_ctx* ctx, double* out4) {
+    if (!ctx || !out4) return FD3D_ERR_ARG;
+    return ctx->impl->post(out4);
 }
 
 int fd3d_fetch_final(fd3d_ctx* ctx, double* slipX, double* slipZ, double* ruptime, double* rise, double* sliptime) {

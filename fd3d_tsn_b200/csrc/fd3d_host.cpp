@@ -99,17 +99,56 @@ int write_results(fd3d_ctx* ctx, const fd3d_params& p, int nf, int& rec_written,
         struct Out { const char* name; std::vector<double>* v; const std::vector<double>* minus; };
         Out outs[] = {{"risetime.res", &ri, nullptr}, {"ruptime.res", &rt, nullptr}, {"slipX.res", &sx, nullptr},
                       {"slipZ.res", &sz, nullptr}, {"stressdropX.res", &cx, &t0x}, {"stressdropZ.res", &cz, &t0z}};
+        const bool f32 = p.precision == FD3D_PREC_F32;
         for (const Out& o : outs) {
             FILE* fp = std::fopen(path(dir, o.name).c_str(), "w");
             if (!fp) return FD3D_ERR_IO;
             for (int k = p.nabc + 1; k <= p.nzt - p.nfs; ++k)
                 for (int i = p.nabc + 1; i <= p.nxt - p.nabc; ++i) {
                     const size_t q = (size_t)(i - 1) + (size_t)p.nxt * (k - 1);
-                    double v = (*o.v)[q] - (o.minus ? (*o.minus)[q] : 0.0);
+                    double v = (*o.v)[q];
+                    if (o.minus)  // SCHANGE - T0 in `real` (fd3d_theo.f90:604-605)
+                        v = f32 ? (double)((float)v - (float)(*o.minus)[q]) : v - (*o.minus)[q];
                     std::fprintf(fp, " %23.15E\n", v);
                 }
             std::fclose(fp);
         }
+        // rupture contour, cohesive zone and rupture velocity (fd3d_theo.f90:710-749),
+        // the last two computed on the device by fd3d_post_process
+        double summary[4];
+        std::vector<double> rvel(n2), czone(n2);
+        if (fd3d_post_process(ctx, summary) || fd3d_fetch_plane(ctx, FD3D_PLANE_RVEL, rvel.data()) ||
+            fd3d_fetch_plane(ctx, FD3D_PLANE_CZONE, czone.data()))
+            return FD3D_ERR_CUDA;
+        FILE* fc = std::fopen(path(dir, "contour.res").c_str(), "w");
+        FILE* fz = std::fopen(path(dir, "czone.res").c_str(), "w");
+        FILE* fv = std::fopen(path(dir, "rvel.res").c_str(), "w");
+        if (!fc || !fz || !fv) {
+            if (fc) std::fclose(fc);
+            if (fz) std::fclose(fz);
+            if (fv) std::fclose(fv);
+            return FD3D_ERR_IO;
+        }
+        std::fprintf(fc, " j k t\n");
+        for (int k = p.nabc + 1; k <= p.nzt - p.nfs; ++k)
+            for (int i = p.nabc + 1; i <= p.nxt - p.nabc; ++i) {
+                const size_t q = (size_t)(i - 1) + (size_t)p.nxt * (k - 1);
+                double x, z;
+                if (f32) {
+                    const float dh = (float)p.dh;
+                    x = (double)(((float)(i - p.nabc - 1) - (float)(p.nxt - 2 * p.nabc) / 2.f) * dh);
+                    z = (double)((float)(p.nzt - k - p.nabc - 1) * dh);
+                } else {
+                    x = ((double)(i - p.nabc - 1) - (double)(p.nxt - 2 * p.nabc) / 2.) * p.dh;
+                    z = (double)(p.nzt - k - p.nabc - 1) * p.dh;
+                }
+                std::fprintf(fc, " %23.15E %23.15E %23.15E\n", x, z, rt[q]);
+                std::fprintf(fz, " %23.15E\n", czone[q]);
+                std::fprintf(fv, " %23.15E\n", rvel[q]);
+            }
+        std::fclose(fc);
+        std::fclose(fz);
+        std::fclose(fv);
     }
     return FD3D_OK;
 }

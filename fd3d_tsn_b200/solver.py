@@ -138,6 +138,25 @@ class Solver:
             "fd3d_fetch_plane")
         return out
 
+    def moment_rate(self, rec0: int = 0, nrec: int | None = None) -> np.ndarray:
+        """Moment rate of the history records still in the device ring
+        (MomentRate of fd3d_theo.f90:574-578 with the seismogram step equal to dt)."""
+        if nrec is None:
+            nrec = self.history_records() - rec0
+        out = np.empty(nrec)
+        _ck(lib().fd3d_fetch_moment_rate(self.h, rec0, nrec, out.ctypes.data_as(C.POINTER(C.c_double))),
+            "fd3d_fetch_moment_rate")
+        return out
+
+    def post_process(self) -> dict:
+        """The reference's post-loop block on the device: average rupture speed, seismic
+        moment, rupture area (0, as the reference leaves it) and average stress drop, and
+        the rupture-velocity and cohesive-zone planes."""
+        out = np.empty(4)
+        _ck(lib().fd3d_post_process(self.h, out.ctypes.data_as(C.POINTER(C.c_double))), "fd3d_post_process")
+        return dict(rupture_speed=out[0], moment=out[1], area=out[2], stress_drop=out[3],
+                    rvel=self.plane("rvel"), czone=self.plane("czone"))
+
     def final(self) -> dict:
         shp = (self.model["nxt"], self.model["nzt"])
         out = {k: np.empty(shp, order="F") for k in ("slipX", "slipZ", "ruptime", "rise", "sliptime")}

@@ -97,7 +97,9 @@ extern "C" {
 #define FD3D_PLANE_T0Z      12
 #define FD3D_PLANE_SCHANGEX 13
 #define FD3D_PLANE_SCHANGEZ 14
-#define FD3D_PLANE_NPLANES  15
+#define FD3D_PLANE_RVEL     15   /* rupture velocity (rvel.res), after fd3d_post_process */
+#define FD3D_PLANE_CZONE    16   /* cohesive zone (czone.res), after fd3d_post_process   */
+#define FD3D_PLANE_NPLANES  17
 
 #define FD3D_MAX_STATIONS 10  /* units 31..40 of the reference (fd3d_theo.f90:117-128) */
 
@@ -184,6 +186,16 @@ int fd3d_fetch_plane(fd3d_ctx* ctx, int plane, double* host);                  /
 int fd3d_fetch_final(fd3d_ctx* ctx, double* slipX, double* slipZ, double* ruptime,
                      double* rise, double* sliptime);
 int fd3d_write_results(fd3d_ctx* ctx, const char* dir, int real_kind);
+/* Moment rate of history records rec0..rec0+nrec-1 (still in the device ring): the sum
+ * over the interior fault plane of |slip rate| * mu(i,nyt,k) * dh^2, reduced on the
+ * device in FP64 -- MomentRate of fd3d_theo.f90:574-578 with the seismogram step equal
+ * to dt (for a coarser step the reference averages consecutive records). */
+int fd3d_fetch_moment_rate(fd3d_ctx* ctx, int rec0, int nrec, double* host);
+/* The post-loop quantities of fd3d_theo.f90:604-749 on the device: fills the
+ * FD3D_PLANE_RVEL and FD3D_PLANE_CZONE planes and out4 = {average rupture speed,
+ * seismic moment M0, rupture area (0: the reference never assigns it), average
+ * stress drop}. */
+int fd3d_post_process(fd3d_ctx* ctx, double* out4);
 /* host-visible timing of the last fd3d_run span, CUDA events on the ctx stream */
 int fd3d_last_run_ms(fd3d_ctx* ctx, float* ms);
 /* per-kernel timing over the last run when profiling is switched on */

@@ -85,6 +85,7 @@ struct Oracle {
     std::vector<A> distX, distZ, slipX, slipZ, ruptime, rise, sliptime;
     std::vector<F> sliprateoutX, sliprateoutZ, schangeX, schangeZ;
     std::vector<A> psiout;
+    std::vector<A> moment_rate;  // per step (fd3d_theo.f90:574-578, dtseis = dt)
     std::vector<F> seis;  // nst*3 of the last step
     A Sn = 0, v0 = 0, f0 = 0, fw = 0, uini = 0, wini = 0;
     int nucleation = 0;
@@ -128,6 +129,7 @@ struct Oracle {
         for (auto* a : {&u1, &v1, &w1, &xx, &yy, &zz, &xy, &yz, &xz}) std::fill(a->begin(), a->end(), (F)0);
         for (auto* a : {&tx, &tz, &v1t, &avdx, &avdz, &RFx, &RFz, &au1, &av1, &aw1, &uZ, &wX, &sliprateoutX,
                         &sliprateoutZ, &schangeX, &schangeZ}) std::fill(a->begin(), a->end(), (F)0);
+        moment_rate.clear();
         std::fill(ruptime.begin(), ruptime.end(), (A)1.e4);
         std::fill(rise.begin(), rise.end(), (A)0);
         std::fill(sliptime.begin(), sliptime.end(), (A)1.e4);
@@ -847,6 +849,63 @@ struct Oracle {
         dvel(); bnd2d(); tasuw(); pml_uvw(); fuvw();
         dstres(); strbnd(); tasxz_tasii(); pml_xyz(); fres();
         traction(); friction(time); nucleate(time);
+        // MomentRate(k) += sqrt(srX^2 + srZ^2)*mu1(i,nysc,j)*dh*dh/(dtseis/dt), with dtseis = dt
+        // one bin per step (fd3d_theo.f90:560,574-578), in the accumulator type
+        A mr = 0;
+        for (int j = nabc + 1; j <= nzt - nfs; ++j)
+            for (int i = nabc + 1; i <= nxt - nabc; ++i) {
+                const A x = (A)sliprateoutX[I2(i, j)], z = (A)sliprateoutZ[I2(i, j)];
+                mr = mr + std::sqrt(x * x + z * z) * (A)mu1[I3(i, nysc, j)] * (A)dh * (A)dh;
+            }
+        moment_rate.push_back(mr);
+    }
+
+    // post-loop quantities  fd3d_theo.f90:604-605, 660-686, 710-749:
+    // out = {average rupture speed, seismic moment, rupture area (never assigned by the
+    // reference, 0), average stress drop}; rvel, czone planes (nxt*nzt, 0 outside)
+    void post(double* out, double* rvel, double* czone) const {
+        const A d = (A)dh;
+        A m0 = 0, numer = 0, denom = 0, sd = 0;
+        std::fill(rvel, rvel + tx.size(), 0.0);
+        std::fill(czone, czone + tx.size(), 0.0);
+        for (int k = nabc + 1; k <= nzt - nfs; ++k)
+            for (int i = nabc + 1; i <= nxt - nabc; ++i) {
+                const size_t p = I2(i, k);
+                const A slip = std::sqrt(slipX[p] * slipX[p] + slipZ[p] * slipZ[p]);
+                m0 = m0 + slip * (A)mu1[I3(i, nysc, k)] * (A)(dh * dh);  // dh*dh in `real`
+                const A dzs = (A)(F)(schangeZ[p] - T0Z[p]), dxs = (A)(F)(schangeX[p] - T0X[p]);
+                numer = numer + dzs * slipZ[p] + dxs * slipX[p];
+                denom = denom + slip;
+                sd = (denom != 0) ? -(numer / denom) : (A)0;
+            }
+        A tint = 0, tint2 = 0;
+        const A none = (A)1.e4;
+        for (int k = nabc + 1; k <= nzt - nfs; ++k)
+            for (int i = nabc + 1; i <= nxt - nabc; ++i) {
+                const size_t p = I2(i, k);
+                A cz = 0, rv = 0;
+                const A r0 = ruptime[p], rxp = ruptime[I2(i + 1, k)], rzp = ruptime[I2(i, k + 1)];
+                const A rxm = ruptime[I2(i - 1, k)], rzm = ruptime[I2(i, k - 1)];
+                if (r0 != none && rxp != none && rzp != none && rxm != none && rzm != none) {
+                    if (sliptime[p] != none) {
+                        const A den = std::sqrt((rxp - r0) * (rxp - r0) + (rzp - r0) * (rzp - r0)) +
+                                      std::sqrt((r0 - rxm) * (r0 - rxm) + (r0 - rzm) * (r0 - rzm));
+                        if (den != 0) {
+                            rv = (A)2 * d / den;
+                            const A slip = std::sqrt(slipX[p] * slipX[p] + slipZ[p] * slipZ[p]);
+                            tint = tint + rv * slip;
+                            tint2 = tint2 + slip;
+                        }
+                        cz = rv * (sliptime[p] - r0);
+                    }
+                }
+                rvel[p] = (double)rv;
+                czone[p] = (double)cz;
+            }
+        out[0] = (double)(tint / tint2);
+        out[1] = (double)m0;
+        out[2] = 0.0;
+        out[3] = (double)sd;
     }
 };
 
@@ -982,6 +1041,24 @@ int oracle_get_plane(void* hv, int plane, double* out) {
         }
     });
     return rc;
+}
+
+// moment rate of steps [from, from+n) (one value per step)
+int oracle_moment_rate(void* hv, int from, int n, double* out) {
+    Handle* h = (Handle*)hv;
+    int rc = 0;
+    DISPATCH(h, {
+        if (from < 0 || from + n > (int)o->moment_rate.size()) rc = FD3D_ERR_ARG;
+        else for (int q = 0; q < n; ++q) out[q] = (double)o->moment_rate[(size_t)(from + q)];
+    });
+    return rc;
+}
+
+// post-loop quantities (see Oracle::post)
+int oracle_post(void* hv, double* out4, double* rvel, double* czone) {
+    Handle* h = (Handle*)hv;
+    DISPATCH(h, o->post(out4, rvel, czone));
+    return 0;
 }
 
 int oracle_steps_done(void* hv) {

@@ -43,6 +43,9 @@ def lib():
         L.oracle_get_field.argtypes = [vp, C.c_int, dp]
         L.oracle_get_plane.argtypes = [vp, C.c_int, dp]
         L.oracle_steps_done.argtypes = [vp]
+        L.oracle_steps_done.restype = C.c_int
+        L.oracle_moment_rate.argtypes = [vp, C.c_int, C.c_int, dp]
+        L.oracle_post.argtypes = [vp, dp, dp, dp]
         L.oracle_num_threads.restype = C.c_int
         L.oracle_set_threads.argtypes = [C.c_int]
         _LIB = L
@@ -102,6 +105,28 @@ class Oracle:
         out = {k: self.plane(k) for k in ("slipX", "slipZ", "ruptime", "rise", "sliptime")}
         out["rise"] = out["rise"] - out["ruptime"]
         return out
+
+    def steps_done(self) -> int:
+        return int(lib().oracle_steps_done(self.h))
+
+    def moment_rate(self, first: int = 0, n: int | None = None) -> np.ndarray:
+        """Moment rate per step (fd3d_theo.f90:574-578 with dtseis = dt)."""
+        n = self.steps_done() - first if n is None else n
+        out = np.empty(n)
+        rc = lib().oracle_moment_rate(self.h, first, n, out.ctypes.data_as(C.POINTER(C.c_double)))
+        if rc:
+            raise ValueError("oracle_moment_rate: bad range")
+        return out
+
+    def post(self):
+        """Post-loop quantities (fd3d_theo.f90:604-749): summary (average rupture speed,
+        seismic moment, rupture area = 0, average stress drop) and the rvel, czone planes."""
+        n2 = self.model["nxt"] * self.model["nzt"]
+        out, rv, cz = np.empty(4), np.empty(n2), np.empty(n2)
+        dp = C.POINTER(C.c_double)
+        lib().oracle_post(self.h, out.ctypes.data_as(dp), rv.ctypes.data_as(dp), cz.ctypes.data_as(dp))
+        shp = (self.model["nxt"], self.model["nzt"])
+        return out, rv.reshape(shp, order="F"), cz.reshape(shp, order="F")
 
     def close(self):
         if self.h:

@@ -224,3 +224,33 @@ def test_heterogeneous_medium_bitwise():
             np.testing.assert_array_equal(s.field(name), o.field(name), err_msg=name)
         s.close()
         o.close()
+
+
+@pytest.mark.parametrize("precision,variant", [("f32", MIXED), ("f64", F64)])
+def test_moment_rate_and_post_loop_match_oracle(precision, variant, tmp_path):
+    """Moment rate per step and the post-loop block (rupture velocity, cohesive zone,
+    average rupture speed, seismic moment, stress drop) on the device against the
+    oracle's sequential loops: the per-node planes agree to the last bit, the sums up to
+    their summation order."""
+    m = configs.tiny_sw(seed=8, nsteps=70, precision=precision)
+    o = Oracle(m, variant)
+    o.step(70, history=False)
+    s = Solver(m)
+    s.run(70)
+    s.sync()
+    mr = s.moment_rate()
+    assert mr.shape == (70,) and mr.max() > 0
+    np.testing.assert_allclose(mr, o.moment_rate(), rtol=1e-12, atol=0)
+    got = s.post_process()
+    ref, rv, cz = o.post()
+    np.testing.assert_array_equal(got["rvel"], rv)
+    np.testing.assert_array_equal(got["czone"], cz)
+    assert got["area"] == 0.0
+    np.testing.assert_allclose([got["rupture_speed"], got["moment"], got["stress_drop"]], ref[[0, 1, 3]],
+                               rtol=1e-12)
+    s.write_results(str(tmp_path), 8 if precision == "f64" else 4)
+    c = np.loadtxt(tmp_path / "contour.res", skiprows=1)
+    assert c.shape == (s.nxT * s.nzT, 3)
+    inner = (slice(m["nabc"], m["nxt"] - m["nabc"]), slice(m["nabc"], m["nzt"] - m["nfs"]))
+    np.testing.assert_allclose(np.loadtxt(tmp_path / "rvel.res"), rv[inner].ravel(order="F"), rtol=1e-14)
+    np.testing.assert_allclose(np.loadtxt(tmp_path / "czone.res"), cz[inner].ravel(order="F"), rtol=1e-14)
