@@ -55,6 +55,48 @@ __global__ void k_layer_check(Grid g, const T* lam, const T* mu, const T* d, T* 
     if (__syncthreads_or(bad) && threadIdx.x == 0) atomicOr(nonuniform, 1);
 }
 
+// inversion_modeltofd3d (fd3d_init.f90:806-835) on the device: control points (nli x
+// nwi, Fortran order) bilinearly interpolated onto the interior fault plane in the
+// field type, in the reference's operation order; striniX goes to T0Xb for the next pass
+template <class T>
+__global__ void k_model_to_fd3d(Grid g, int nli, const T* T0I, const T* TsI, const T* DcI, const T* ns, T DL, T DW,
+                                T dh, int dipslip, Fault<T> q) {
+    const int i = g.nabc + 1 + blockIdx.x * blockDim.x + threadIdx.x;
+    const int k = g.nabc + 1 + blockIdx.y * blockDim.y + threadIdx.y;
+    if (i > g.nxt - g.nabc || k > g.ks()) return;
+    const T ZS = dh * (T)(k - 1 - g.nabc);
+    const int kk = (int)(ZS / DW) + 1;
+    const T u = (ZS - DW * (T)(kk - 1)) / DW;
+    const T XS = dh * (T)(i - 1 - g.nabc);
+    const int ii = (int)(XS / DL) + 1;
+    const T t = (XS - DL * (T)(ii - 1)) / DL;
+    auto C2 = [&](const T* a, int x, int z) { return a[(x - 1) + nli * (z - 1)]; };
+    auto bil = [&](const T* a) {
+        return ((T)1 - t) * ((T)1 - u) * C2(a, ii, kk) + t * ((T)1 - u) * C2(a, ii + 1, kk) +
+               t * u * C2(a, ii + 1, kk + 1) + ((T)1 - t) * u * C2(a, ii, kk + 1);
+    };
+    const int p = g.at2(i, k);
+    const T t0 = bil(T0I);
+    if (dipslip) q.T0Z[p] = t0; else q.T0Xb[p] = t0;
+    q.peakZ[p] = bil(TsI) * ns[k - 1];
+    const T dc = bil(DcI);
+    q.Dc[p] = dc;
+    q.DcZ[p] = dc;
+}
+
+// interp_fric (fd3d_deriv.f90:3174-3189): X-node values are 4-point averages
+template <class T>
+__global__ void k_interp_fric(Grid g, Fault<T> q) {
+    const int i = 2 + blockIdx.x * blockDim.x + threadIdx.x;
+    const int k = 2 + blockIdx.y * blockDim.y + threadIdx.y;
+    if (i > g.nxt - 1 || k > g.nzt - 1) return;
+    const int a = g.at2(i, k), b = g.at2(i - 1, k), c = g.at2(i, k - 1), d = g.at2(i - 1, k - 1);
+    q.peakX[a] = (q.peakZ[a] + q.peakZ[b] + q.peakZ[c] + q.peakZ[d]) / (T)4;
+    q.dynX[a] = (q.dynZ[a] + q.dynZ[b] + q.dynZ[c] + q.dynZ[d]) / (T)4;
+    q.DcX[a] = (q.DcZ[a] + q.DcZ[b] + q.DcZ[c] + q.DcZ[d]) / (T)4;
+    q.T0X[a] = (q.T0Xb[a] + q.T0Xb[b] + q.T0Xb[c] + q.T0Xb[d]) / (T)4;
+}
+
 struct CtxBase {
     fd3d_params p;
     Grid g;
@@ -84,6 +126,7 @@ struct CtxBase {
     virtual int upload_medium(const void*, const void*, const void*, int) = 0;
     virtual int upload_medium_layers(const double*, const double*, const double*) = 0;
     virtual int upload_fault(const fd3d_fault*) = 0;
+    virtual int upload_fault_model(int, int, const double*, const double*, const double*, double, int) = 0;
     virtual int reset() = 0;
     virtual int enqueue_step() = 0;
     virtual int fetch_field(int, void*, int) = 0;
@@ -353,6 +396,41 @@ struct Ctx : CtxBase {
         rc |= up2(q.peakZ, pkZ); rc |= up2(q.dynZ, dyZ); rc |= up2(q.DcZ, DcZ); rc |= up2(q.coh, coh);
         if (rc) return FD3D_ERR_CUDA;
         CK(cudaStreamSynchronize(st));
+        fault_ok = true;
+        return reset_state(false);
+    }
+
+    int upload_fault_model(int nli, int nwi, const double* T0I, const double* TsI, const double* DcI, double dip,
+                           int dipslip) override {
+        if (law != FD3D_LAW_SW || nli < 2 || nwi < 2 || !T0I || !TsI || !DcI) return FD3D_ERR_ARG;
+        const size_t nc = (size_t)nli * nwi, n2 = (size_t)p.nxt * p.nzt;
+        // control points and the normal-stress profile (fd3d_init.f90:77-86) in the field type
+        std::vector<T> ctl(3 * nc + (size_t)p.nzt);
+        for (size_t q2 = 0; q2 < nc; ++q2) {
+            ctl[q2] = (T)T0I[q2]; ctl[nc + q2] = (T)TsI[q2]; ctl[2 * nc + q2] = (T)DcI[q2];
+        }
+        const T pi = (T)3.1415926535, dh = c.dh;
+        for (int k = 1; k <= p.nzt; ++k) {
+            const T cns = dipslip ? (T)8520. : (T)16200.;
+            ctl[3 * nc + k - 1] = std::max((T)1.e5, cns * dh * (T)(p.nzt - p.nfs - k) * (T)std::sin((T)dip / (T)180. * pi));
+        }
+        const T DL = dh * (T)(p.nxt - 2 * p.nabc) / (T)(nli - 1);
+        const T DW = dh * (T)(p.nzt - p.nfs - p.nabc) / (T)(nwi - 1);
+        T* dctl = nullptr;  // set-up scratch, released before returning
+        CK(cudaMalloc(&dctl, ctl.size() * sizeof(T)));
+        CK(cudaMemcpyAsync(dctl, ctl.data(), ctl.size() * sizeof(T), cudaMemcpyHostToDevice, st));
+        T* zero[] = {q.T0Xb, q.T0Z, q.peakZ, q.Dc, q.DcZ, q.dynZ, q.coh, q.peakX, q.dynX, q.DcX, q.T0X};
+        for (T* a : zero) CK(cudaMemsetAsync(a, 0, n2 * sizeof(T), st));
+        const dim3 b2(32, 8);
+        const int nxT = p.nxt - 2 * p.nabc, nzT = g.ks() - p.nabc;
+        k_model_to_fd3d<T><<<dim3((nxT + 31) / 32, (nzT + 7) / 8), b2, 0, st>>>(
+            g, nli, dctl, dctl + nc, dctl + 2 * nc, dctl + 3 * nc, DL, DW, dh, dipslip, q);
+        k_interp_fric<T><<<dim3((p.nxt + 31) / 32, (p.nzt + 7) / 8), b2, 0, st>>>(g, q);
+        CK(cudaGetLastError());
+        CK(cudaMemcpyAsync(q.T0Xb, q.T0X, n2 * sizeof(T), cudaMemcpyDeviceToDevice, st));
+        CK(cudaStreamSynchronize(st));
+        CK(cudaFree(dctl));
+        fs = FvwScalars{};
         fault_ok = true;
         return reset_state(false);
     }
@@ -783,6 +861,12 @@ int fd3d_fetch_plane(fd3d_ctx* ctx, int plane, double* host) {
     if (!ctx || !host) return FD3D_ERR_ARG;
     CK(cudaStreamSynchronize(ctx->impl->st));
     return ctx->impl->fetch_plane(plane, host);
+}
+
+int fd3d_upload_fault_model(fd3d_ctx* ctx, int nli, int nwi, const double* T0I, const double* TsI, const double* DcI,
+                            double dip, int dipslip) {
+    if (!ctx) return FD3D_ERR_ARG;
+    return ctx->impl->upload_fault_model(nli, nwi, T0I, TsI, DcI, dip, dipslip);
 }
 
 int fd3d_fetch_moment_rate(fd3d_ctx* ctx, int rec0, int nrec, double* host) {

@@ -73,6 +73,14 @@ class Solver:
         fb = abi.FaultBuffers(fault)
         _ck(lib().fd3d_upload_fault(self.h, C.byref(fb.s)), "fd3d_upload_fault")
 
+    def upload_fault_model(self, T0I, TsI, DcI, dip: float = 90.0, dipslip: bool = False):
+        """Fault from the control points of forwardmodel.dat (interpolated on the device)."""
+        arrs = [np.asfortranarray(a, dtype=np.float64) for a in (T0I, TsI, DcI)]
+        nli, nwi = arrs[0].shape
+        dp = C.POINTER(C.c_double)
+        _ck(lib().fd3d_upload_fault_model(self.h, nli, nwi, *(a.ctypes.data_as(dp) for a in arrs), float(dip),
+                                          int(dipslip)), "fd3d_upload_fault_model")
+
     # ------------------------------------------------------------ time loop
     def reset(self):
         _ck(lib().fd3d_reset(self.h), "fd3d_reset")

@@ -163,6 +163,15 @@ int fd3d_upload_medium(fd3d_ctx* ctx, const void* lam1, const void* mu1, const v
 /* 1-D layered medium as built by readcrustalmodel (fd3d_init.f90:241-265): one value per k */
 int fd3d_upload_medium_layers(fd3d_ctx* ctx, const double* lam_k, const double* mu_k, const double* d_k);
 int fd3d_upload_fault(fd3d_ctx* ctx, const fd3d_fault* f);
+/* Slip-weakening fault from the control points an inversion sampler writes to
+ * forwardmodel.dat (readinversionresult, fd3d_init.f90:839-857): nli x nwi arrays in
+ * Fortran order of prestress T0I, static friction TsI (scaled by the normal stress
+ * normstress(k), fd3d_init.f90:77-86, dip in degrees, dipslip selects the DIPSLIP
+ * build) and Dc.  The bilinear interpolation onto the fault plane
+ * (inversion_modeltofd3d, fd3d_init.f90:802-835) and interp_fric run on the device;
+ * dynamic friction and cohesion are 0 as there. */
+int fd3d_upload_fault_model(fd3d_ctx* ctx, int nli, int nwi, const double* T0I, const double* TsI,
+                            const double* DcI, double dip, int dipslip);
 int fd3d_reset(fd3d_ctx* ctx);                      /* zero wave field, PML and fault state (fd3d_theo.f90:59-88) */
 int fd3d_run(fd3d_ctx* ctx, int nsteps);            /* enqueue nsteps time steps; asynchronous */
 int fd3d_sync(fd3d_ctx* ctx);                       /* wait; returns first device error        */

@@ -860,6 +860,49 @@ struct Oracle {
         moment_rate.push_back(mr);
     }
 
+    // readinversionresult + inversion_modeltofd3d (fd3d_init.f90:802-857): the control
+    // points (nli x nwi, Fortran order) of prestress T0I, static strength TsI (times the
+    // normal stress) and Dc, bilinearly interpolated onto the interior fault plane in
+    // `real`; dynamic strength and cohesion 0; then interp_fric through set_fault.
+    void set_fault_model(int nli, int nwi, const double* T0Id, const double* TsId, const double* DcId, double dipd,
+                         int dipslip) {
+        const size_t n2 = tx.size();
+        std::vector<F> T0I(T0Id, T0Id + (size_t)nli * nwi), TsI(TsId, TsId + (size_t)nli * nwi),
+            DcI(DcId, DcId + (size_t)nli * nwi);
+        auto C2 = [&](const std::vector<F>& a, int ii, int kk) { return a[(size_t)(ii - 1) + (size_t)nli * (kk - 1)]; };
+        const F pi = (F)3.1415926535, dip = (F)dipd;
+        auto normstress = [&](int j) {  // fd3d_init.f90:77-86
+            const F c = dipslip ? (F)8520. : (F)16200.;
+            return std::max((F)1.e5, c * dh * (F)(nzt - nfs - j) * (F)std::sin(dip / (F)180. * pi));
+        };
+        std::vector<double> sX(n2, 0.0), sZ(n2, 0.0), pk(n2, 0.0), dy(n2, 0.0), dc(n2, 0.0), ch(n2, 0.0);
+        const F DL = dh * (F)(nxt - 2 * nabc) / (F)(nli - 1);
+        const F DW = dh * (F)(nzt - nfs - nabc) / (F)(nwi - 1);
+        for (int k = nabc + 1; k <= nzt - nfs; ++k) {
+            const F ZS = dh * (F)(k - 1 - nabc);
+            const int kk = (int)(ZS / DW) + 1;
+            const F u = (ZS - DW * (F)(kk - 1)) / DW;
+            for (int i = nabc + 1; i <= nxt - nabc; ++i) {
+                const F XS = dh * (F)(i - 1 - nabc);
+                const int ii = (int)(XS / DL) + 1;
+                const F t = (XS - DL * (F)(ii - 1)) / DL;
+                auto bil = [&](const std::vector<F>& a) {
+                    return ((F)1 - t) * ((F)1 - u) * C2(a, ii, kk) + t * ((F)1 - u) * C2(a, ii + 1, kk) +
+                           t * u * C2(a, ii + 1, kk + 1) + ((F)1 - t) * u * C2(a, ii, kk + 1);
+                };
+                const size_t p = I2(i, k);
+                const F t0 = bil(T0I);
+                if (dipslip) sZ[p] = (double)t0; else sX[p] = (double)t0;
+                pk[p] = (double)(bil(TsI) * normstress(k));
+                dc[p] = (double)bil(DcI);
+            }
+        }
+        fd3d_fault f{};
+        f.striniX = sX.data(); f.striniZ = sZ.data(); f.Dc = dc.data();
+        f.peak_xz = pk.data(); f.dyn_xz = dy.data(); f.coh = ch.data();
+        set_fault(f);
+    }
+
     // post-loop quantities  fd3d_theo.f90:604-605, 660-686, 710-749:
     // out = {average rupture speed, seismic moment, rupture area (never assigned by the
     // reference, 0), average stress drop}; rvel, czone planes (nxt*nzt, 0 outside)
@@ -1041,6 +1084,13 @@ int oracle_get_plane(void* hv, int plane, double* out) {
         }
     });
     return rc;
+}
+
+int oracle_set_fault_model(void* hv, int nli, int nwi, const double* T0I, const double* TsI, const double* DcI,
+                           double dip, int dipslip) {
+    Handle* h = (Handle*)hv;
+    DISPATCH(h, o->set_fault_model(nli, nwi, T0I, TsI, DcI, dip, dipslip));
+    return 0;
 }
 
 // moment rate of steps [from, from+n) (one value per step)

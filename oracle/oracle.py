@@ -46,6 +46,7 @@ def lib():
         L.oracle_steps_done.restype = C.c_int
         L.oracle_moment_rate.argtypes = [vp, C.c_int, C.c_int, dp]
         L.oracle_post.argtypes = [vp, dp, dp, dp]
+        L.oracle_set_fault_model.argtypes = [vp, C.c_int, C.c_int, dp, dp, dp, C.c_double, C.c_int]
         L.oracle_num_threads.restype = C.c_int
         L.oracle_set_threads.argtypes = [C.c_int]
         _LIB = L
@@ -105,6 +106,15 @@ class Oracle:
         out = {k: self.plane(k) for k in ("slipX", "slipZ", "ruptime", "rise", "sliptime")}
         out["rise"] = out["rise"] - out["ruptime"]
         return out
+
+    def set_fault_model(self, T0I, TsI, DcI, dip=90.0, dipslip=False):
+        """Fault from control points (readinversionresult + inversion_modeltofd3d)."""
+        arrs = [np.asfortranarray(a, dtype=np.float64) for a in (T0I, TsI, DcI)]
+        nli, nwi = arrs[0].shape
+        dp = C.POINTER(C.c_double)
+        lib().oracle_set_fault_model(self.h, nli, nwi, *(a.ctypes.data_as(dp) for a in arrs), float(dip),
+                                     int(dipslip))
+        lib().oracle_reset(self.h)
 
     def steps_done(self) -> int:
         return int(lib().oracle_steps_done(self.h))

@@ -254,3 +254,30 @@ def test_moment_rate_and_post_loop_match_oracle(precision, variant, tmp_path):
     inner = (slice(m["nabc"], m["nxt"] - m["nabc"]), slice(m["nabc"], m["nzt"] - m["nfs"]))
     np.testing.assert_allclose(np.loadtxt(tmp_path / "rvel.res"), rv[inner].ravel(order="F"), rtol=1e-14)
     np.testing.assert_allclose(np.loadtxt(tmp_path / "czone.res"), cz[inner].ravel(order="F"), rtol=1e-14)
+
+
+@pytest.mark.parametrize("dipslip", [False, True])
+def test_fault_from_inversion_control_points(dipslip):
+    """The control points of forwardmodel.dat interpolated onto the fault plane on the
+    device (inversion_modeltofd3d + interp_fric) give the oracle's fault and, after a
+    run, its histories, to the last bit."""
+    m = configs.tiny_sw(seed=31, nsteps=40)
+    rng = np.random.default_rng(5)
+    nli, nwi = 7, 5
+    T0I = rng.uniform(20e6, 30e6, (nli, nwi))
+    TsI = rng.uniform(0.6, 0.7, (nli, nwi))
+    TsI[3, 2] = 0.02  # a weak spot in the middle breaks at once
+    DcI = rng.uniform(0.2, 0.5, (nli, nwi))
+    o = Oracle(m, MIXED)
+    o.set_fault_model(T0I, TsI, DcI, dip=75.0, dipslip=dipslip)
+    oh, _ = o.step(40)
+    s = Solver(m)
+    s.upload_fault_model(T0I, TsI, DcI, dip=75.0, dipslip=dipslip)
+    for name in ("T0X", "T0Z"):
+        np.testing.assert_array_equal(s.plane(name), o.plane(name), err_msg=name)
+    s.run(40)
+    s.sync()
+    gh = np.stack([s.history(f) for f in range(s.nf)], axis=1)
+    assert np.abs(oh[:, 0:2]).max() > 0, "the weak spot must slip"
+    np.testing.assert_array_equal(gh, oh[:, :s.nf])
+    np.testing.assert_array_equal(s.final()["slipX"], o.plane("slipX"))
