@@ -819,6 +819,19 @@ int fd3d_fetch_history(fd3d_ctx* ctx, int field, int rec0, int nrec, void* host,
     CK(cudaStreamSynchronize(c->st));
     const size_t plane = (size_t)(c->p.nxt - 2 * c->p.nabc) * (c->p.nzt - c->p.nfs - c->p.nabc);
     const size_t es = c->elem();
+    if ((size_t)rk == es) {
+        // same element type: the records go straight to the caller's buffer, one strided
+        // copy per contiguous run of ring slots (a page-locked buffer makes it one DMA)
+        for (int r = 0; r < nrec;) {
+            const int slot = (rec0 + r) % c->hist_cap;
+            const int run = std::min(nrec - r, c->hist_cap - slot);
+            const char* src = (const char*)c->ring + ((size_t)slot * c->nf + field) * plane * es;
+            CK(cudaMemcpy2D((char*)host + (size_t)r * plane * es, plane * es, src, (size_t)c->nf * plane * es,
+                            plane * es, (size_t)run, cudaMemcpyDeviceToHost));
+            r += run;
+        }
+        return FD3D_OK;
+    }
     std::vector<char> buf(plane * es);
     for (int r = 0; r < nrec; ++r) {
         const size_t slot = (size_t)((rec0 + r) % c->hist_cap);
@@ -840,14 +853,19 @@ int fd3d_fetch_stations(fd3d_ctx* ctx, int rec0, int nrec, double* host) {
     if (rec0 + nrec > have || rec0 < have - c->hist_cap) return FD3D_ERR_ARG;
     CK(cudaStreamSynchronize(c->st));
     const int ns = c->p.nstations;
+    if (ns == 0) return FD3D_OK;
     const size_t es = c->elem();
-    std::vector<char> buf((size_t)3 * std::max(ns, 1) * es);
-    for (int r = 0; r < nrec; ++r) {
-        const size_t slot = (size_t)((rec0 + r) % c->hist_cap);
-        CK(cudaMemcpy(buf.data(), (const char*)c->seis + slot * 3 * ns * es, 3 * ns * es, cudaMemcpyDeviceToHost));
-        for (int q = 0; q < 3 * ns; ++q)
-            host[(size_t)r * 3 * ns + q] = es == 4 ? (double)((float*)buf.data())[q] : ((double*)buf.data())[q];
+    // the records are contiguous in the ring apart from its wrap: at most two copies
+    std::vector<char> buf((size_t)nrec * 3 * ns * es);
+    for (int r = 0; r < nrec;) {
+        const int slot = (rec0 + r) % c->hist_cap;
+        const int run = std::min(nrec - r, c->hist_cap - slot);
+        CK(cudaMemcpy(buf.data() + (size_t)r * 3 * ns * es, (const char*)c->seis + (size_t)slot * 3 * ns * es,
+                      (size_t)run * 3 * ns * es, cudaMemcpyDeviceToHost));
+        r += run;
     }
+    for (size_t q = 0; q < (size_t)nrec * 3 * ns; ++q)
+        host[q] = es == 4 ? (double)((const float*)buf.data())[q] : ((const double*)buf.data())[q];
     return FD3D_OK;
 }
 

@@ -166,6 +166,8 @@ def test_history_stride_and_ring():
     oh, _ = o.step(40)
     last = s.history(0, rec0=6, nrec=4)          # the ring keeps the last 4 records
     np.testing.assert_array_equal(last, oh[[27, 31, 35, 39], 0])
+    # the same records in the field type: copied straight out of the ring (which wraps here)
+    np.testing.assert_array_equal(s.history(0, rec0=6, nrec=4, real_kind=4), oh[[27, 31, 35, 39], 0].astype(np.float32))
     with pytest.raises(Fd3dError):
         s.history(0, rec0=0, nrec=1)             # overwritten
 
