@@ -55,9 +55,10 @@ struct Fields {
     T *u, *v, *w, *xx, *yy, *zz, *xy, *yz, *xz;
     const T *lam, *mu, *d;
     // The same medium as a 1-D profile when it varies with k only (the layered medium
-    // of readcrustalmodel): lam at lay[k-1], mu at lay[nzt+k-1], d at lay[2*nzt+k-1];
-    // null otherwise.  The interior sweeps then read three values per plane instead of
-    // three arrays per cell.
+    // of readcrustalmodel): lam at lay[k-1], mu at lay[nzt+k-1], d at lay[2*nzt+k-1],
+    // and dth/d (the IEEE quotient the velocity sweep forms per cell) at lay[3*nzt+k-1];
+    // null otherwise.  The interior sweeps then read values per plane instead of arrays
+    // per cell.
     const T* lay;
 };
 

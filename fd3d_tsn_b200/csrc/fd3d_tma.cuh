@@ -124,7 +124,7 @@ __device__ __forceinline__ bool vel_interior_tma_body(const VelMaps& M, const Gr
         xq0 = xq1; xq1 = xq2; xq2 = xq3; xq3 = nx;
         yq0 = yq1; yq1 = yq2; yq2 = yq3; yq3 = ny;
         if (k < ke) { nz = zz[pk + 3 * sz]; nx = xz[pk + 2 * sz]; ny = yz[pk + 2 * sz]; }
-        const T dk = LAYERED ? f.lay[2 * g.nzt + k - 1] : (T)0;  // density of plane k (1-D medium)
+        const T rk = LAYERED ? f.lay[3 * g.nzt + k - 1] : (T)0;  // dth / density of plane k (1-D medium)
         if (!mbar_wait(smem_addr(&bars[s]), ring_parity(gn))) {
             atomicOr(status, ST_TIMEOUT);
             tma_drain_pc(bars, p0, k, ke, kb);
@@ -138,7 +138,7 @@ __device__ __forceinline__ bool vel_interior_tma_body(const VelMaps& M, const Gr
             const T* sxz = sl + VelSlot::XZ + ty * 40 + tx;
             const T* syz = sl + VelSlot::YZ + (ty + 2) * 32 + tx;
             const int o = ty * 32 + tx;
-            const T r = dth / (LAYERED ? dk : sl[VelSlot::D + o]);
+            const T r = LAYERED ? rk : dth / sl[VelSlot::D + o];
             f.u[pk] = sl[VelSlot::U + o] +
                       r * (c1 * (sxx[4] - sxx[3]) + c2 * (sxx[5] - sxx[2]) + c1 * (sxy[4] - sxy[-40 + 4]) +
                            c2 * (sxy[40 + 4] - sxy[-80 + 4]) + c1 * (xq2 - xq1) + c2 * (xq3 - xq0));
