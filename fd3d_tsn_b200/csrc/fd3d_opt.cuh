@@ -317,10 +317,10 @@ struct InteriorCfg {
     // measured on B200 at 1020x410x512 (fraction of the measured HBM copy bandwidth):
     // TMA ring 97% (velocity) and 92% (stress); register-prefetch pipe 66%/67%;
     // per-point 61%/53%; tiled without prefetch 22%/26%.  With the layered medium
-    // (no media windows) 32 / 16 planes per CTA beat 16 / 8 by 2-3%.
+    // (no media windows) 32 planes per CTA beat 16 / 8 by 2-4%.
     int variant = IV_TMA;
     int kchunk = 32;      // z-planes per CTA of the velocity sweep
-    int kchunk_str = 16;  // z-planes per CTA of the stress sweep
+    int kchunk_str = 32;  // z-planes per CTA of the stress sweep
     int by = 8;          // CTA rows (IV_POINT: block = 32 x by)
 };
 
