@@ -169,7 +169,7 @@ def describe(name, m):
             "grid_padded": [m["nxt"], m["nyt"], m["nzt"]],
             "cells_padded": m["nxt"] * m["nyt"] * m["nzt"],
             "h_m": m["dh"], "dt_s": m["dt"], "law": m.get("law", "sw"),
-            "fields": "fp32", "accumulators": "fp64", "medium": "1-D layered (interior sweeps read the profile)",
+            "fields": "fp32", "accumulators": "fp64", "medium": "1-D layered",
             "history_stride": m.get("history_stride", 1),
             "l2": "inputs larger than L2 (wave field ~10 GB >> 126 MB)"}
 
