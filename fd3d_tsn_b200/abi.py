@@ -46,7 +46,7 @@ class Params(C.Structure):
         ("pml_vp", C.c_double), ("pml_fact", C.c_double), ("vp_max", C.c_double),
         ("law", C.c_int), ("precision", C.c_int), ("nstations", C.c_int),
         ("staX", C.c_int * MAX_STATIONS), ("staY", C.c_int * MAX_STATIONS), ("staZ", C.c_int * MAX_STATIONS),
-        ("history_stride", C.c_int), ("history_capacity", C.c_int),
+        ("history_stride", C.c_int), ("history_capacity", C.c_int), ("fspace", C.c_int),
     ]
 
 
@@ -77,7 +77,8 @@ def make_params(cfg: dict) -> Params:
     p = Params()
     for k in ("nxt", "nyt", "nzt", "nabc", "ntfd"):
         setattr(p, k, int(cfg[k]))
-    p.nfs = int(cfg.get("nfs", 2))
+    p.fspace = 1 if cfg.get("fspace", False) else 0
+    p.nfs = int(cfg.get("nfs", p.nabc if p.fspace else 2))
     for k in ("dh", "dt", "damp_s", "pml_vp", "pml_fact"):
         setattr(p, k, float(cfg[k]))
     p.vp_max = float(cfg.get("vp_max", 0.0))
@@ -146,6 +147,7 @@ def load_library(path: str | None = None) -> C.CDLL:
         "fd3d_set_profiling": (i, [vp, i]),
         "fd3d_kernel_times": (i, [vp, fp, C.POINTER(i)]),
         "fd3d_read_deck": (i, [C.c_char_p, C.POINTER(Params), C.POINTER(dp), C.POINTER(dp), C.POINTER(dp)]),
+        "fd3d_read_deck_ex": (i, [C.c_char_p, i, C.POINTER(Params), C.POINTER(dp), C.POINTER(dp), C.POINTER(dp)]),
         "fd3d_free": (None, [vp]),
         "fd3d_check_division": (i, [fp, i, C.POINTER(C.c_ulonglong), C.POINTER(C.c_uint)]),
         "fd3d_fetch_moment_rate": (i, [vp, i, i, dp]),

@@ -83,8 +83,11 @@ def gaussian_field(rng, nx, nz, corr_nodes, mean, std):
     return mean + std * f
 
 
-def _grid(nxT, nyT, nzT, h, dt, ntfd, nabc=NABC):
-    return dict(nxt=nxT + 2 * nabc, nyt=nyT + nabc, nzt=nzT + nabc + NFS, nabc=nabc, nfs=NFS,
+def _grid(nxT, nyT, nzT, h, dt, ntfd, nabc=NABC, fspace=False):
+    """Padded grid of fd3d_init.f90:161-169; fspace: the FSPACE build (a PML strip of
+    nabc cells above the model instead of the free surface, nfs = nabc)."""
+    nfs = nabc if fspace else NFS
+    return dict(nxt=nxT + 2 * nabc, nyt=nyT + nabc, nzt=nzT + nabc + nfs, nabc=nabc, nfs=nfs, fspace=bool(fspace),
                 dh=float(h), dt=float(dt), ntfd=int(ntfd), damp_s=DAMP_S, pml_vp=PML_VP, pml_fact=PML_FACT)
 
 
@@ -125,7 +128,7 @@ def sw_fault(m, rng, patch, sn=120e6, mus=0.68, mud=0.52, dc=0.4, t0_mean=70e6, 
 
 
 def sw_model(nxT, nyT, nzT, h, sim_time, seed, layers=None, patch_nodes=None, nstations=4, corr_m=2000.0,
-             dc_patch_m=None, dc_range=None, history_stride=1, precision="f32", ntfd=None):
+             dc_patch_m=None, dc_range=None, history_stride=1, precision="f32", ntfd=None, fspace=False):
     rng = np.random.default_rng(seed)
     if layers is None:
         layers = dict(depth=[0.0], vp=[6000.0], vs=[3464.0], rho=[2670.0])
@@ -133,8 +136,9 @@ def sw_model(nxT, nyT, nzT, h, sim_time, seed, layers=None, patch_nodes=None, ns
     vpmax = max(layers["vp"])
     dt = 0.25 * h / vpmax * (1.0 - 1e-6)  # strict CFL check of fd3d_init.f90:274-278
     nsteps = int(round(sim_time / dt)) if ntfd is None else ntfd
-    m = _grid(nxT, nyT, nzT, h, dt, nsteps)
-    lam, mu, d, vpm = crustal_medium(m["nzt"], h, dip, layers["depth"], layers["vp"], layers["vs"], layers["rho"])
+    m = _grid(nxT, nyT, nzT, h, dt, nsteps, fspace=fspace)
+    lam, mu, d, vpm = crustal_medium(m["nzt"], h, dip, layers["depth"], layers["vp"], layers["vs"], layers["rho"],
+                                     nfs=m["nfs"])
     m.update(medium=(lam, mu, d), vp_max=vpm, law="sw", precision=precision, history_stride=history_stride)
     if patch_nodes is None:
         patch_nodes = (nxT * 3 // 4, nzT // 2)
@@ -273,10 +277,25 @@ def serving_stream(n=2000, seed=4242, rate=30.0, large_frac=0.05, sim_time=8.0):
     return out
 
 
-def tiny_sw(seed=5, nxT=40, nyT=14, nzT=28, h=200.0, nsteps=60, precision="f32", nstations=3, stride=1):
+def fspace_variant(m: dict) -> dict:
+    """The same model in the FSPACE build's padding: nfs = nabc, so nabc-2 more planes on
+    top, where the fifth PML strip lies (fd3d_init.f90:161-169).  Medium and fault planes
+    keep their values for k <= nzt-nfs+2 and repeat the last plane above, so both builds
+    see the same model below the former free surface."""
+    nab = m["nabc"]
+    extra = nab - m["nfs"]
+    f = dict(m, fspace=True, nfs=nab, nzt=m["nzt"] + extra)
+    f["medium"] = tuple(np.concatenate([np.asarray(a), np.repeat(np.asarray(a)[-1:], extra)]) for a in m["medium"])
+    f["fault"] = {k: (np.concatenate([v, np.repeat(v[:, -1:], extra, axis=1)], axis=1)
+                      if isinstance(v, np.ndarray) and v.ndim == 2 else v) for k, v in m["fault"].items()}
+    return f
+
+
+def tiny_sw(seed=5, nxT=40, nyT=14, nzT=28, h=200.0, nsteps=60, precision="f32", nstations=3, stride=1,
+            fspace=False, layers=None):
     """Parity-test model: rupture starts on step 1 from an overstressed nucleation patch."""
-    return sw_model(nxT, nyT, nzT, h, 1.0, seed, patch_nodes=(nxT - 8, nzT - 8), nstations=nstations,
-                    precision=precision, ntfd=nsteps, history_stride=stride, corr_m=600.0)
+    return sw_model(nxT, nyT, nzT, h, 1.0, seed, layers=layers, patch_nodes=(nxT - 8, nzT - 8), nstations=nstations,
+                    precision=precision, ntfd=nsteps, history_stride=stride, corr_m=600.0, fspace=fspace)
 
 
 def tiny_fvw(seed=6, nxT=40, nyT=14, nzT=28, h=200.0, nsteps=60, precision="f32", stride=1):

@@ -459,12 +459,12 @@ int build_work(fd3d_batch* b) {
         const int fx = (std::max(nxT, p.nxt) + 31) / 32, fz = (nzT + 7) / 8;
         for (int y = 0; y < fz; ++y)
             for (int x = 0; x < fx; ++x) per[0].push_back(Work{tm | W_VEL_FAULT, x, y, 0});
-        const int npml = (int)((M.dev.D.cum[4] + 255) / 256);
+        const int npml = (int)((M.dev.D.cum[PML_MAXS] + 255) / 256);
         for (int x = 0; x < npml; ++x) {
             per[0].push_back(Work{tm | W_VEL_PML, x, 0, 0});
             per[2].push_back(Work{tm | W_STR_PML, x, 0, 0});
         }
-        const int sx = (p.nxt + 31) / 32, sy = (p.nyt + 7) / 8;
+        const int sx = (p.nxt + 31) / 32, sy = p.fspace ? 0 : (p.nyt + 7) / 8;  // no fuvw/fres under FSPACE
         for (int y = 0; y < sy; ++y)
             for (int x = 0; x < sx; ++x) {
                 per[1].push_back(Work{tm | W_VEL_FS, x, y, 0});

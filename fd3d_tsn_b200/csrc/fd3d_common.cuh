@@ -19,6 +19,7 @@ namespace fd3d {
 
 struct Grid {
     int nxt, nyt, nzt, nabc, nfs;
+    int fspace;      // FSPACE build: a PML strip above k = ks() instead of the free surface
     int px;          // row pitch (elements)
     int off;         // x offset of i=1 inside a row
     long long plane; // px*nyt
@@ -28,10 +29,11 @@ struct Grid {
         return (long long)off + (i - 1) + (long long)px * (j - 1) + plane * (k - 1);
     }
     __host__ __device__ __forceinline__ int at2(int i, int k) const { return (i - 1) + nxt * (k - 1); }
-    __host__ __device__ __forceinline__ int ks() const { return nzt - nfs; }  // free-surface row
+    __host__ __device__ __forceinline__ int ks() const { return nzt - nfs; }  // free-surface row (top row of the
+                                                                              // interior box under FSPACE)
 };
 
-// Split-field PML strip (strip s = 1 x-low, 2 x-high, 3 y-low, 4 z-low).
+// Split-field PML strip (strip s = 1 x-low, 2 x-high, 3 y-low, 4 z-low, 5 z-high under FSPACE).
 struct Strip {
     int nxb, nxe, nyb, nye, nzb, nze;  // reference box (v/xy/yz loops end at nye)
     int ni, nj1, nk;                   // aux dims, nj1 = nye-nyb+2

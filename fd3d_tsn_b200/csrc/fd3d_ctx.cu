@@ -499,7 +499,7 @@ struct Ctx : CtxBase {
         launch_pml<T>(false, pml_minb_vel, st, g, f, D, X, c, status);
         kend(2);
         kbeg(3);
-        k_vel_fs<T><<<dim3((p.nxt + 31) / 32, (p.nyt + 7) / 8), b2, 0, st>>>(g, f);
+        if (!p.fspace) k_vel_fs<T><<<dim3((p.nxt + 31) / 32, (p.nyt + 7) / 8), b2, 0, st>>>(g, f);  // fuvw
         kend(3);
         // stress half-step
         kbeg(4);
@@ -514,7 +514,7 @@ struct Ctx : CtxBase {
         kend(6);
         // fault boundary condition
         kbeg(7);
-        k_str_fs<T><<<dim3((p.nxt + 31) / 32, (p.nyt + 7) / 8), b2, 0, st>>>(g, f);
+        if (!p.fspace) k_str_fs<T><<<dim3((p.nxt + 31) / 32, (p.nyt + 7) / 8), b2, 0, st>>>(g, f);  // fres
         k_traction<T><<<dim3((nxT + 31) / 32, (nzT + 7) / 8), b2, 0, st>>>(g, f, q, c);
         k_friction<T><<<dim3((nxT + 31) / 32, (nzT + 7) / 8), b2, 0, st>>>(g, f, q, c, law, fs, it_dev);
         HistDesc h;

@@ -160,7 +160,11 @@ extern "C" {
 void fd3d_free(void* p) { std::free(p); }
 
 int fd3d_read_deck(const char* dir, fd3d_params* p, double** lam1, double** mu1, double** d1) {
-    if (!dir || !p) return FD3D_ERR_ARG;
+    return fd3d_read_deck_ex(dir, 0, p, lam1, mu1, d1);
+}
+
+int fd3d_read_deck_ex(const char* dir, int fspace, fd3d_params* p, double** lam1, double** mu1, double** d1) {
+    if (!dir || !p || (fspace != 0 && fspace != 1)) return FD3D_ERR_ARG;
     std::ifstream in(path(dir, "inputfd3d.dat"));
     if (!in) return FD3D_ERR_IO;
     std::vector<std::string> t;
@@ -190,7 +194,8 @@ int fd3d_read_deck(const char* dir, fd3d_params* p, double** lam1, double** mu1,
         if (!read_tokens(in, 3, t)) return FD3D_ERR_IO;
         p->staX[s] = std::atoi(t[0].c_str()); p->staY[s] = std::atoi(t[1].c_str()); p->staZ[s] = std::atoi(t[2].c_str());
     }
-    p->nfs = 2;  // fd3d_init.f90:164 (FSPACE not built)
+    p->fspace = fspace;
+    p->nfs = fspace ? p->nabc : 2;  // fd3d_init.f90:161-165
     p->nxt = nxtT + 2 * p->nabc;
     p->nyt = nytT + p->nabc;
     p->nzt = nztT + p->nabc + p->nfs;

@@ -79,8 +79,9 @@ __device__ __forceinline__ void vel_fault_body(Grid g, Fields<T> f, Fault<T> q, 
     if (ii == 0 && kk == 0) atomicAdd(it_dev, 1);  // step counter read by the fault BC launches
     const int ks = g.ks();
     const long long sy = g.px, sz = g.plane;
-    // ghost row k=ks+1: v(:,nyt,ks+1) = v(:,nyt-1,ks+1)  (bnd2d mirror, fd3d_deriv.f90:225-232)
-    if (kk == 0 && ii < g.nxt) {
+    // ghost row k=ks+1: v(:,nyt,ks+1) = v(:,nyt-1,ks+1)  (bnd2d mirror, fd3d_deriv.f90:225-232);
+    // under FSPACE that row belongs to the top PML strip, whose tiles mirror it
+    if (!g.fspace && kk == 0 && ii < g.nxt) {
         const long long p = g.at(ii + 1, g.nyt - 1, ks + 1);
         f.v[p + sy] = f.v[p];
     }
@@ -150,14 +151,16 @@ __device__ __forceinline__ void vel_fault_body(Grid g, Fields<T> f, Fault<T> q, 
     }
 }
 
+constexpr int PML_MAXS = 5;  // strips 1-4, and 5 (the top) under FSPACE
 struct PmlDesc {
-    Strip s[4];
-    long long cum[5];  // cumulative cell counts of the u/w loop ranges over the strips
+    Strip s[PML_MAXS];
+    long long cum[PML_MAXS + 1];  // cumulative cell counts of the u/w loop ranges (an absent strip adds 0)
+    int ns;                       // strips present: 4, or 5 under FSPACE
 };
 
 // PML auxiliary components (the 24 split fields that init_pml allocates per strip,
-// fd3d_deriv.f90:1330-1406) are indexed by the compact cell index t of the u/w loop
-// ranges of the 4 strips (strip s holds t in [cum[s], cum[s+1])) and stored in blocks
+// fd3d_deriv.f90:1330-1406, 1413-1437) are indexed by the compact cell index t of the
+// u/w loop ranges of the strips (strip s holds t in [cum[s], cum[s+1])) and stored in blocks
 // of 32 cells: inside a block the 32 values of one component are contiguous and the
 // components of a group follow each other.  The velocity group (u,v,w splits, 9
 // components) and the stress group (xx,yy,zz,xy,xz,yz splits, 15) are separate spans,
@@ -165,7 +168,7 @@ struct PmlDesc {
 // one bulk copy brings a tile's range into shared memory and one writes it back.
 constexpr int AUX_NV = 9, AUX_NS = 15;
 constexpr int PML_TILE = 256;
-inline long long pml_aux_cells(const PmlDesc& D) { return (D.cum[4] + PML_TILE - 1) / PML_TILE * PML_TILE; }
+inline long long pml_aux_cells(const PmlDesc& D) { return (D.cum[PML_MAXS] + PML_TILE - 1) / PML_TILE * PML_TILE; }
 inline size_t pml_aux_elems(const PmlDesc& D) { return (size_t)pml_aux_cells(D) * (AUX_NV + AUX_NS); }
 
 // One entry of a damping profile (init_pml's omega at one index): the factors
@@ -195,8 +198,8 @@ __device__ __forceinline__ int aux_sm(int l, int ncomp, int c) { return (l >> 5)
 
 // locate strip and (i,j,k) of compact cell index t (u/w loop range of every strip)
 __device__ __forceinline__ bool pml_locate(const PmlDesc& D, long long t, int& s, int& i, int& j, int& k) {
-    if (t >= D.cum[4]) return false;
-    s = (t >= D.cum[1]) + (t >= D.cum[2]) + (t >= D.cum[3]);
+    if (t >= D.cum[PML_MAXS]) return false;
+    s = (t >= D.cum[1]) + (t >= D.cum[2]) + (t >= D.cum[3]) + (t >= D.cum[4]);
     const Strip& S = D.s[s];
     // strip-local index fits 32 bits (a strip is ni*nj*nk cells)
     unsigned r = (unsigned)(t - D.cum[s]);
@@ -450,7 +453,7 @@ __device__ __forceinline__ bool str_pml_tile(const Grid& g, const Fields<T>& f, 
         const Strip& S = D.s[s];
         p = g.at(i, j, k);
         dxy = (j <= S.nye);
-        top = (s <= 2) && (k == S.nze);  // xz/yz aux zeroed at the top row, strips 1-3
+        top = !g.fspace && (s <= 2) && (k == S.nze);  // xz/yz aux zeroed at the top row, strips 1-3 (not FSPACE)
         xl = f.lam[p]; xm = f.mu[p]; mz = f.mu[p + sz];
         up = f.u[p]; ux = f.u[p + 1]; uz = f.u[p + sz];
         vp = f.v[p]; vy = f.v[p - sy];
@@ -467,9 +470,9 @@ __device__ __forceinline__ bool str_pml_tile(const Grid& g, const Fields<T>& f, 
         const int i2 = i - S.nxb, j2 = j - S.nyb, k2 = k - S.nzb;
         const Damp<T> ox = X.prof[S.ox_off + i2], oxS = X.prof[S.oxS_off + i2];
         const Damp<T> oy = X.prof[S.oy_off + j2], oz = X.prof[S.oz_off + k2];
-        // xy, yz use omegayS in strips 3,4; xz, yz use omegazS in strip 4
+        // xy, yz use omegayS in strips 3-5; xz, yz use omegazS in strips 4, 5
         const Damp<T> oyxy = X.prof[(s >= 2 ? S.oyS_off : S.oy_off) + j2];
-        const Damp<T> ozxz = X.prof[(s == 3 ? S.ozS_off : S.oz_off) + k2];
+        const Damp<T> ozxz = X.prof[(s >= 3 ? S.ozS_off : S.oz_off) + k2];
         const T dt = c.dt, dh = c.dh, rdh = c.rdh;
         const T a = xl + (T)2 * xm, b = xl;
         const T diff1 = ux - up, diff2 = vp - vy, diff3 = wp - wz;
@@ -535,7 +538,8 @@ __device__ __forceinline__ void str_fs_body(Grid g, Fields<T> f, int bx_, int by
 }
 
 // ---------------------------------------------------------------- fault BC
-// trial traction, damping, RF (fd3d_theo.f90:233-308, non-FSPACE)
+// trial traction, damping, RF (fd3d_theo.f90:233-308).  Under FSPACE the top row k = ks
+// takes the interior formula and no ghost row is written (fd3d_theo.f90:260-283).
 template <class T>
 __device__ __forceinline__ void traction_body(Grid g, Fields<T> f, Fault<T> q, StepConst<T> c, int bx_, int by_, int bz_) {
     const int i = g.nabc + 1 + bx_ * blockDim.x + threadIdx.x;
@@ -547,8 +551,9 @@ __device__ __forceinline__ void traction_body(Grid g, Fields<T> f, Fault<T> q, S
     const int n2 = g.at2(i, k);
     const T c1 = c.c1, c2 = c.c2, dht = c.dht, ds = c.damp_s;
     const T* xx = f.xx; const T* xz = f.xz; const T* zz = f.zz;
+    const bool inner = (k < ks) || g.fspace;
     T pdz;
-    if (k < ks)
+    if (inner)
         pdz = (c1 * (xz[p + 1] - xz[p]) + c2 * (xz[p + 2] - xz[p - 1])) / (T)2 +
               (c1 * (zz[p + sz] - zz[p]) + c2 * (zz[p + 2 * sz] - zz[p - sz])) / (T)2 - f.yz[p - sy];
     else
@@ -558,7 +563,7 @@ __device__ __forceinline__ void traction_body(Grid g, Fields<T> f, Fault<T> q, S
     T rf = pdz + av;
     q.RFz[n2] = rf;
     T tzv;
-    if (k < ks) tzv = -rf - (T)0.5 * f.d[p] * dht * f.w[p];
+    if (inner) tzv = -rf - (T)0.5 * f.d[p] * dht * f.w[p];
     else        tzv = -rf - (T)0.5 * f.d[p] * dht * f.w[p] / (T)2;
     q.tzt[n2] = tzv;
     q.avdz[n2] = pdz;
@@ -571,8 +576,8 @@ __device__ __forceinline__ void traction_body(Grid g, Fields<T> f, Fault<T> q, S
     q.txt[n2] = txv;
     q.avdx[n2] = pdx;
     // ghost row nzt-1 (fd3d_theo.f90:304-307); with nfs=2: nzt-1 = ks+1, nzt-2 = ks, nzt-3 = ks-1
-    if (k == ks) q.txt[g.at2(i, ks + 1)] = +txv;
-    if (k == ks - 1) q.tzt[g.at2(i, ks + 1)] = -tzv;
+    if (!g.fspace && k == ks) q.txt[g.at2(i, ks + 1)] = +txv;
+    if (!g.fspace && k == ks - 1) q.tzt[g.at2(i, ks + 1)] = -tzv;
 }
 
 // |T| at staggered nodes, friction law, slip, rupture time (fd3d_theo.f90:313-410)
@@ -801,7 +806,7 @@ __global__ void __launch_bounds__(PML_TILE, MINB) k_str_pml(Grid g, Fields<T> f,
 template <class T>
 inline void launch_pml(bool stress, int minb, cudaStream_t st, const Grid& g, const Fields<T>& f, const PmlDesc& D,
                        const PmlAux<T>& X, const StepConst<T>& c, int* status) {
-    const unsigned nblk = (unsigned)((D.cum[4] + PML_TILE - 1) / PML_TILE);
+    const unsigned nblk = (unsigned)((D.cum[PML_MAXS] + PML_TILE - 1) / PML_TILE);
     if (nblk == 0) return;
 #define FD3D_PML_CASE(MB)                                                               \
     case MB:                                                                            \

@@ -12,7 +12,8 @@ namespace fd3d {
 inline
 int validate_params(const fd3d_params* p) {
     if (!p) return FD3D_ERR_ARG;
-    if (p->nabc < 3 || p->nfs != 2) return FD3D_ERR_ARG;
+    if (p->nabc < 3 || (p->fspace != 0 && p->fspace != 1)) return FD3D_ERR_ARG;
+    if (p->nfs != (p->fspace ? p->nabc : 2)) return FD3D_ERR_ARG;  // fd3d_init.f90:161-165
     if (p->nxt < 2 * p->nabc + 4 || p->nyt < p->nabc + 4 || p->nzt < p->nabc + p->nfs + 4) return FD3D_ERR_ARG;
     if (!(p->dh > 0) || !(p->dt > 0)) return FD3D_ERR_ARG;
     if (p->law != FD3D_LAW_SW && p->law != FD3D_LAW_FVW) return FD3D_ERR_ARG;
@@ -30,6 +31,7 @@ int validate_params(const fd3d_params* p) {
 inline Grid make_grid(const fd3d_params& p) {
     Grid g;
     g.nxt = p.nxt; g.nyt = p.nyt; g.nzt = p.nzt; g.nabc = p.nabc; g.nfs = p.nfs;
+    g.fspace = p.fspace;
     g.off = (32 - (p.nabc % 32)) % 32;
     g.px = ((p.nxt + g.off + 31) / 32) * 32;
     g.plane = (long long)g.px * p.nyt;
@@ -41,15 +43,23 @@ inline Grid make_grid(const fd3d_params& p) {
 template <class T>
 void make_pml(const fd3d_params& p, PmlDesc& D, std::vector<Damp<T>>& prof) {
     const int nxt = p.nxt, nyt = p.nyt, nzt = p.nzt, nabc = p.nabc, nfs = p.nfs;
-    const int bx[4][6] = {{2, nabc, nabc + 1, nyt - 1, nabc + 1, nzt - nfs},
-                          {nxt - nabc + 1, nxt - 1, nabc + 1, nyt - 1, nabc + 1, nzt - nfs},
-                          {2, nxt - 1, 2, nabc, nabc + 1, nzt - nfs},
-                          {2, nxt - 1, 2, nyt - 1, 2, nabc}};
+    const int bx[PML_MAXS][6] = {{2, nabc, nabc + 1, nyt - 1, nabc + 1, nzt - nfs},
+                                 {nxt - nabc + 1, nxt - 1, nabc + 1, nyt - 1, nabc + 1, nzt - nfs},
+                                 {2, nxt - 1, 2, nabc, nabc + 1, nzt - nfs},
+                                 {2, nxt - 1, 2, nyt - 1, 2, nabc},
+                                 {2, nxt - 1, 2, nyt - 1, nzt - nabc + 1, nzt - 1}};  // FSPACE top strip
     long long base = 0;
     prof.clear();
+    D.ns = p.fspace ? 5 : 4;
     D.cum[0] = 0;
-    std::vector<std::vector<T>> ox(4), oxS(4), oy(4), oyS(4), oz(4), ozS(4);
-    for (int s = 0; s < 4; ++s) {
+    std::vector<std::vector<T>> ox(PML_MAXS), oxS(PML_MAXS), oy(PML_MAXS), oyS(PML_MAXS), oz(PML_MAXS), ozS(PML_MAXS);
+    for (int s = 0; s < PML_MAXS; ++s) {
+        if (s >= D.ns) {  // absent strip: empty range
+            D.s[s] = D.s[s - 1];
+            D.s[s].ncells = 0;
+            D.cum[s + 1] = D.cum[s];
+            continue;
+        }
         Strip& S = D.s[s];
         S.nxb = bx[s][0]; S.nxe = bx[s][1]; S.nyb = bx[s][2]; S.nye = bx[s][3]; S.nzb = bx[s][4]; S.nze = bx[s][5];
         S.ni = S.nxe - S.nxb + 1; S.nk = S.nze - S.nzb + 1; S.nj1 = S.nye - S.nyb + 2;
@@ -85,8 +95,14 @@ void make_pml(const fd3d_params& p, PmlDesc& D, std::vector<Damp<T>>& prof) {
         oy[3][i - 1] = omR[i - 1];
         ozS[3][i - 1] = omRM[i - 1]; oxS[3][i - 1] = omRM[i - 1]; oxS[3][nxt - i - 2] = om[i - 1];
         oyS[3][i - 1] = omRM[i - 1];
+        if (D.ns == 5) {  // fd3d_deriv.f90:1481-1490
+            oz[4][i - 1] = omM[i - 1];  ox[4][i - 1] = omR[i - 1];  ox[4][nxt - i - 2] = omM[i - 1];
+            oy[4][i - 1] = omR[i - 1];
+            ozS[4][i - 1] = om[i - 1];  oxS[4][i - 1] = omRM[i - 1]; oxS[4][nxt - i - 2] = om[i - 1];
+            oyS[4][i - 1] = omRM[i - 1];
+        }
     }
-    for (int s = 0; s < 4; ++s) {
+    for (int s = 0; s < D.ns; ++s) {
         Strip& S = D.s[s];
         auto put = [&](const std::vector<T>& v) {
             const int o = (int)prof.size();

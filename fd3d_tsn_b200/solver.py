@@ -195,12 +195,14 @@ class Solver:
             pass
 
 
-def read_deck(path: str):
-    """fd3d_init + readcrustalmodel through the C ABI: (params dict, lam1, mu1, d1)."""
+def read_deck(path: str, fspace: bool = False):
+    """fd3d_init + readcrustalmodel through the C ABI: (params dict, lam1, mu1, d1);
+    fspace reads the deck as the FSPACE build does (nfs = nabc)."""
     p = abi.Params()
     dp = C.POINTER(C.c_double)
     bl, bm, bd = dp(), dp(), dp()
-    _ck(lib().fd3d_read_deck(path.encode(), C.byref(p), C.byref(bl), C.byref(bm), C.byref(bd)), "fd3d_read_deck")
+    _ck(lib().fd3d_read_deck_ex(path.encode(), int(fspace), C.byref(p), C.byref(bl), C.byref(bm), C.byref(bd)),
+        "fd3d_read_deck_ex")
     n = p.nxt * p.nyt * p.nzt
     arrs = []
     for b in (bl, bm, bd):

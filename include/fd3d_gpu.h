@@ -111,7 +111,7 @@ extern "C" {
 typedef struct fd3d_params {
     int    nxt, nyt, nzt;      /* padded grid                                     */
     int    nabc;               /* PML thickness (cells)                           */
-    int    nfs;                /* rows above the free surface (2; FSPACE is not built) */
+    int    nfs;                /* rows above the free surface: 2, or nabc with fspace */
     int    ntfd;               /* number of time steps of a full solve            */
     double dh, dt;             /* grid step [m], time step [s]                    */
     double damp_s;             /* damping near the fault                          */
@@ -123,6 +123,11 @@ typedef struct fd3d_params {
     int    staX[FD3D_MAX_STATIONS], staY[FD3D_MAX_STATIONS], staZ[FD3D_MAX_STATIONS]; /* 1-based */
     int    history_stride;     /* keep history planes every n-th step (>=1)       */
     int    history_capacity;   /* device ring capacity in records (0 = default)   */
+    int    fspace;             /* 1: the FSPACE build (fd3d_init.f90:161-165): nfs = nabc and a
+                                  fifth PML strip above k = nzt-nfs instead of the free surface
+                                  (fd3d_deriv.f90:1413-1493, 2223-2293, 2996-3143); no fuvw/fres,
+                                  the top fault row uses the full 4th-order traction
+                                  (fd3d_theo.f90:213-227, 260-283); 0: free surface        */
 } fd3d_params;
 
 /*
@@ -270,6 +275,9 @@ int fd3d_check_division(const float* divisors, int n, unsigned long long* mismat
 /* Reads inputfd3d.dat and crustal.dat from dir (fd3d_init.f90:145-173, 211-279),
  * fills p and returns lam1/mu1/d1 (caller frees with fd3d_free). */
 int fd3d_read_deck(const char* dir, fd3d_params* p, double** lam1, double** mu1, double** d1);
+/* The same for the build selected by fspace (1: FSPACE, nfs = nabc, as the reference's
+ * compile switch does in fd3d_init.f90:161-165; 0: as fd3d_read_deck). */
+int fd3d_read_deck_ex(const char* dir, int fspace, fd3d_params* p, double** lam1, double** mu1, double** d1);
 void fd3d_free(void* p);
 
 #ifdef __cplusplus

@@ -4,6 +4,7 @@
 //   src/fd3d_deriv.f90  dvel/uxx1/vyy1/wzz1, bnd2d/uxx0a/vyy0a/wzz0a, dstres,
 //                       strbnd/sxx/sxy0/sxz0/syz0, sxz1 (tasxz), tasii, tasu1, tasw1,
 //                       fuvw, fres, init_pml, pml_uvw, pml_xyz, interp_fric
+//                       (with the FSPACE build's top PML strip, fspace = 1)
 //   src/fd3d_theo.f90   fd3d(): initialisation, loop order, traction, friction,
 //                       output planes, stations, TPV103/104 nucleation ramp
 // Every region keeps the reference's index ranges, evaluation order of sums and
@@ -66,6 +67,8 @@ template <class F, class A>
 struct Oracle {
     // ---------------- parameters (fd3dparam_com, pml_com, traction_com)
     int nxt, nyt, nzt, nabc, nfs, nysc, ntfd;
+    int fspace = 0;  // FSPACE build (fd3d_init.f90:161-165): PML strip 5 above, no free surface
+    int nstrip = 4;  // PML strips: 4, or 5 under FSPACE
     F dh, dt, damp_s, omegaM_pml;
     A dtA;
     int law;
@@ -91,14 +94,14 @@ struct Oracle {
     int nucleation = 0;
     A hx0 = 0, hz0 = 0, perturb = 0, RR2 = 0, TT2 = 0, strinixI = 0;
 
-    // ---------------- PML (pml_com), per strip s=1..4
+    // ---------------- PML (pml_com), per strip s=1..4 (5 under FSPACE)
     struct Strip {
         int nxb, nxe, nyb, nye, nzb, nze;
         int ni, nj1, nk;  // nj1 = nye-nyb+2 (the "+1" arrays)
         std::vector<F> u[3], v[3], w[3], sxx[3], syy[3], szz[3], sxy[2], sxz[2], syz[2];
         std::vector<F> ox, oy, oz, oxS, oyS, ozS;  // damping profiles (index 1-based -> [i-1])
         size_t at(int i2, int j2, int k2) const { return (size_t)(i2 - 1) + (size_t)ni * ((size_t)(j2 - 1) + (size_t)nj1 * (size_t)(k2 - 1)); }
-    } S[5];
+    } S[6];  // 1-based
     std::vector<F> omega_pml, omegaR_pml, omega_pmlM, omegaR_pmlM;  // 1-based by [i-1]
 
     inline size_t I3(int i, int j, int k) const { return (size_t)(i - 1) + (size_t)nxt * ((size_t)(j - 1) + (size_t)nyt * (size_t)(k - 1)); }
@@ -106,6 +109,7 @@ struct Oracle {
 
     explicit Oracle(const fd3d_params& p) {
         nxt = p.nxt; nyt = p.nyt; nzt = p.nzt; nabc = p.nabc; nfs = p.nfs; nysc = nyt; ntfd = p.ntfd;
+        fspace = p.fspace; nstrip = fspace ? 5 : 4;
         dh = (F)p.dh; dt = (F)p.dt; damp_s = (F)p.damp_s; dtA = (A)p.dt;
         law = p.law;
         // omegaM_pml=pml_fact*pml_vp/(2.*dh*(nabc-1))  fd3d_init.f90:171
@@ -137,7 +141,7 @@ struct Oracle {
         F t0 = law == FD3D_LAW_FVW ? (F)1 : (F)0;  // FVW: tabsX=tabsZ=1 (fd3d_theo.f90:78-82)
         std::fill(tabsX.begin(), tabsX.end(), t0);
         std::fill(tabsZ.begin(), tabsZ.end(), t0);
-        for (int s = 1; s <= 4; ++s) {
+        for (int s = 1; s <= nstrip; ++s) {
             Strip& st = S[s];
             for (auto& a : st.u) std::fill(a.begin(), a.end(), (F)0);
             for (auto& a : st.v) std::fill(a.begin(), a.end(), (F)0);
@@ -154,14 +158,15 @@ struct Oracle {
         it = 0; newton_fail = 0;
     }
 
-    // init_pml  fd3d_deriv.f90:1319-1493 (FSPACE strip 5 not built)
+    // init_pml  fd3d_deriv.f90:1319-1493 (strip 5: the FSPACE top strip, :1413-1437)
     void init_pml() {
-        const int bx[5][6] = {{0, 0, 0, 0, 0, 0},
+        const int bx[6][6] = {{0, 0, 0, 0, 0, 0},
                               {2, nabc, nabc + 1, nyt - 1, nabc + 1, nzt - nfs},
                               {nxt - nabc + 1, nxt - 1, nabc + 1, nyt - 1, nabc + 1, nzt - nfs},
                               {2, nxt - 1, 2, nabc, nabc + 1, nzt - nfs},
-                              {2, nxt - 1, 2, nyt - 1, 2, nabc}};
-        for (int s = 1; s <= 4; ++s) {
+                              {2, nxt - 1, 2, nyt - 1, 2, nabc},
+                              {2, nxt - 1, 2, nyt - 1, nzt - nabc + 1, nzt - 1}};
+        for (int s = 1; s <= nstrip; ++s) {
             Strip& st = S[s];
             st.nxb = bx[s][0]; st.nxe = bx[s][1]; st.nyb = bx[s][2]; st.nye = bx[s][3]; st.nzb = bx[s][4]; st.nze = bx[s][5];
             st.ni = st.nxe - st.nxb + 1; st.nk = st.nze - st.nzb + 1;
@@ -209,6 +214,16 @@ struct Oracle {
             S[4].oxS[i - 1] = omegaR_pmlM[i - 1];
             S[4].oxS[nxt - i - 1 - 1] = omega_pml[i - 1];
             S[4].oyS[i - 1] = omegaR_pmlM[i - 1];
+            if (fspace) {  // fd3d_deriv.f90:1481-1490
+                S[5].oz[i - 1] = omega_pmlM[i - 1];
+                S[5].ox[i - 1] = omegaR_pml[i - 1];
+                S[5].ox[nxt - i - 1 - 1] = omega_pmlM[i - 1];
+                S[5].oy[i - 1] = omegaR_pml[i - 1];
+                S[5].ozS[i - 1] = omega_pml[i - 1];
+                S[5].oxS[i - 1] = omegaR_pmlM[i - 1];
+                S[5].oxS[nxt - i - 1 - 1] = omega_pml[i - 1];
+                S[5].oyS[i - 1] = omegaR_pmlM[i - 1];
+            }
         }
     }
 
@@ -384,9 +399,9 @@ struct Oracle {
             }
     }
 
-    // pml_uvw  fd3d_deriv.f90:1927-2299
+    // pml_uvw  fd3d_deriv.f90:1927-2299 (strip 5: :2223-2293)
     void pml_uvw() {
-        for (int s = 1; s <= 4; ++s) {
+        for (int s = 1; s <= nstrip; ++s) {
             Strip& st = S[s];
             const bool y3 = (s == 3);
             const int jue = y3 ? st.nye : st.nye + 1;  // u,w loops run to nye+1 except in strip 3
@@ -552,14 +567,14 @@ struct Oracle {
             }
     }
 
-    // pml_xyz  fd3d_deriv.f90:2304-2992 (FSPACE parts not built)
+    // pml_xyz  fd3d_deriv.f90:2304-2992 (strip 5: :2996-3143)
     void pml_xyz() {
-        for (int s = 1; s <= 4; ++s) {
+        for (int s = 1; s <= nstrip; ++s) {
             Strip& st = S[s];
             const bool y3 = (s == 3);
             const int jn = y3 ? st.nye : st.nye + 1;  // normal-stress and xz loops reach nye+1 except in strip 3
-            const std::vector<F>& oyxy = (s >= 3) ? st.oyS : st.oy;   // xy: omegay in strips 1,2; omegayS in 3,4
-            const std::vector<F>& ozxz = (s == 4) ? st.ozS : st.oz;   // xz,yz: omegazS in strip 4
+            const std::vector<F>& oyxy = (s >= 3) ? st.oyS : st.oy;   // xy: omegay in strips 1,2; omegayS in 3-5
+            const std::vector<F>& ozxz = (s >= 4) ? st.ozS : st.oz;   // xz,yz: omegazS in strips 4, 5
             par_for(st.nzb, st.nze, [&](int k) {
                 for (int j = st.nyb; j <= jn; ++j)
                     for (int i = st.nxb; i <= st.nxe; ++i) {
@@ -628,8 +643,8 @@ struct Oracle {
                         yz[I3(i, j, k)] = st.syz[0][q] + st.syz[1][q];
                     }
             });
-            // zero xz/yz aux at the top row (fd3d_deriv.f90:2471-2491, 2649-2669, 2826-2846)
-            if (s <= 3) {
+            // zero xz/yz aux at the top row (fd3d_deriv.f90:2471-2491, 2649-2669, 2826-2846), not under FSPACE
+            if (s <= 3 && !fspace) {
                 int k2 = st.nze - st.nzb + 1;
                 for (int i2 = 1; i2 <= st.ni; ++i2) {
                     for (int j2 = 1; j2 <= (y3 ? st.nye - st.nyb + 1 : st.nye - st.nyb + 2); ++j2) {
@@ -660,7 +675,7 @@ struct Oracle {
     }
 
     // ------------------------------------------------------------------ fault BC
-    // traction  fd3d_theo.f90:233-308 (non-FSPACE branch)
+    // traction  fd3d_theo.f90:233-308 (FSPACE top row :260-283)
     void traction() {
         const F c1 = (F)9 / (F)8, c2 = (F)-1 / (F)24, dht = dh / dt;
         const int j = nysc;
@@ -689,6 +704,10 @@ struct Oracle {
         };
         for (int k = nabc + 1; k <= nzt - nfs - 1; ++k)
             for (int i = nabc + 1; i <= nxt - nabc; ++i) trac(i, k, false);
+        if (fspace) {  // FSPACE: the top row takes the interior formula, no ghost row (fd3d_theo.f90:260-283)
+            for (int i = nabc + 1; i <= nxt - nabc; ++i) trac(i, nzt - nfs, false);
+            return;
+        }
         for (int i = nabc + 1; i <= nxt - nabc; ++i) trac(i, nzt - nfs, true);
         for (int i = nabc + 1; i <= nxt - nabc; ++i) {
             tx[I2(i, nzt - 1)] = +tx[I2(i, nzt - 2)];
@@ -846,8 +865,10 @@ struct Oracle {
         std::fill(schangeX.begin(), schangeX.end(), (F)0);
         std::fill(schangeZ.begin(), schangeZ.end(), (F)0);
         std::fill(psiout.begin(), psiout.end(), (A)0);
-        dvel(); bnd2d(); tasuw(); pml_uvw(); fuvw();
-        dstres(); strbnd(); tasxz_tasii(); pml_xyz(); fres();
+        dvel(); bnd2d(); tasuw(); pml_uvw();
+        if (!fspace) fuvw();  // fd3d_theo.f90:213-215
+        dstres(); strbnd(); tasxz_tasii(); pml_xyz();
+        if (!fspace) fres();  // fd3d_theo.f90:225-227
         traction(); friction(time); nucleate(time);
         // MomentRate(k) += sqrt(srX^2 + srZ^2)*mu1(i,nysc,j)*dh*dh/(dtseis/dt), with dtseis = dt
         // one bin per step (fd3d_theo.f90:560,574-578), in the accumulator type
@@ -976,6 +997,7 @@ extern "C" {
 
 void* oracle_create(const fd3d_params* p, int variant) {
     if (!p || p->nxt < 2 * p->nabc + 5 || p->nyt < p->nabc + 5 || p->nzt < p->nabc + p->nfs + 5 || p->nabc < 3) return nullptr;
+    if ((p->fspace != 0 && p->fspace != 1) || p->nfs != (p->fspace ? p->nabc : 2)) return nullptr;
     Handle* h = new Handle{variant, nullptr};
     if (variant == 0) h->o = new Oracle<float, double>(*p);
     else if (variant == 1) h->o = new Oracle<double, double>(*p);

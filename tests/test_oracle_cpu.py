@@ -101,3 +101,49 @@ def test_reset_is_exact(variant):
     om.lib().oracle_reset(o.h)
     h2, _ = o.step(20)
     np.testing.assert_array_equal(h1, h2)
+
+
+def _fspace_pair(nsteps):
+    m = configs.sw_model(40, 14, 40, 200.0, 1.0, 7, patch_nodes=(8, 8), nstations=2, ntfd=nsteps, corr_m=600.0)
+    return m, configs.fspace_variant(m)
+
+
+def test_fspace_equals_free_surface_until_the_waves_reach_the_top():
+    """The FSPACE build (PML strip above instead of the free surface) runs the same
+    arithmetic below the top: its histories follow the free-surface build's until the
+    waves from the patch (16 cells below the top) reach it, and part ways afterwards."""
+    m, mf = _fspace_pair(200)
+    assert mf["nzt"] == m["nzt"] + m["nabc"] - 2 and mf["nfs"] == m["nabc"]
+    a, b = Oracle(m, MIXED), Oracle(mf, MIXED)
+    ha, _ = a.step(40)
+    hb, _ = b.step(40)
+    assert np.abs(ha[:, 0]).max() > 0.1, "the patch must slip"
+    for f in range(4):
+        assert np.linalg.norm(ha[:, f] - hb[:, f]) <= 1e-8 * np.linalg.norm(ha[:, f]), f
+    a.step(110, history=False)
+    b.step(110, history=False)
+    ha, _ = a.step(50)
+    hb, _ = b.step(50)
+    assert np.linalg.norm(ha[:, 0] - hb[:, 0]) > 0.05 * np.linalg.norm(ha[:, 0])
+
+
+@pytest.mark.parametrize("fspace", [False, True])
+def test_top_boundary_energy(fspace):
+    """A rupture confined to a small patch radiates; with the FSPACE strip the energy
+    leaves through all sides, and it never grows without bound in either build."""
+    m, mf = _fspace_pair(500)
+    o = Oracle(mf if fspace else m, F64)
+    energies, top = [], 0.0
+    ks = m["nzt"] - m["nfs"]
+    for _ in range(25):
+        o.step(20, history=False)
+        u = o.field("u")
+        energies.append(sum(float((o.field(c) ** 2).sum()) for c in ("u", "v", "w")))
+        top = max(top, float(np.abs(u[:, :, ks + 1:]).max()))  # k >= ks+2: u of the top strip / never set
+    peak = max(energies)
+    assert np.isfinite(energies).all()
+    assert energies[-1] < 0.05 * peak, (fspace, energies[-1], peak)
+    if fspace:
+        assert top > 1e-3  # the top strip carries the wave field it absorbs
+    else:
+        assert top == 0.0  # fuvw sets u on the first ghost row only
