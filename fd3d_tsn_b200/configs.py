@@ -357,6 +357,167 @@ def write_deck(model: dict, outdir: str, crustal: dict):
             f.write(f"{float(dpt) / 1e3!r} {float(vp) / 1e3!r} {float(vs) / 1e3!r} {float(rho) / 1e3!r} 800. 400.\n")
 
 
+def _scec_sw(scec_path):
+    """The scecmodel.dat of the slip-weakening SCEC set-ups (forwardspecialTPV5/8/9,
+    src/fd3d_init.f90:549-558, 630-639, 719-728)."""
+    lines = open(scec_path).read().splitlines()
+    t = _tokens(lines[0], 7)
+    r = dict(no0=int(t[0]))
+    r.update(zip(("hx0", "hz0", "h1x0", "h1z0", "h2x0", "h2z0"), (float(x) for x in t[1:])))
+    r["hdelta"] = float(_tokens(lines[1], 1)[0])
+    r.update(zip(("T0", "T0n", "T0h1", "T0h2"), (float(x) for x in _tokens(lines[2], 4))))
+    r["sn"] = float(_tokens(lines[3], 1)[0])
+    r["mus"], r["muso"] = (float(x) for x in _tokens(lines[4], 2))
+    r["mud"] = float(_tokens(lines[5], 1)[0])
+    r["d0h"] = float(_tokens(lines[6], 1)[0])
+    return r
+
+
+def _in_box(x, z, cx, cz, hdelta):
+    return (x - cx >= -hdelta / 2) & (x - cx <= hdelta / 2) & (z - cz >= -hdelta / 2) & (z - cz <= hdelta / 2)
+
+
+def _tpv89_fault(m, scec_path, dip_slip):
+    """forwardspecialTPV8 (src/fd3d_init.f90:706-783) and forwardspecialTPV9 (:619-704):
+    depth-dependent normal stress sigma_n = sn*dh*(nzt-2-k) (+0.5 for TPV8), cohesion
+    1 MPa, prestress T0*sigma_n (strike slip in TPV8, dip slip in TPV9) with a
+    nucleation square at T0n*mus*sigma_n + coh, the TPV9 surface row at 1/4 and the
+    ghost rows mirrored with a sign change of the prestress.  In FP64 (the -r8 build)."""
+    r = _scec_sw(scec_path)
+    nxt, nzt, dh = m["nxt"], m["nzt"], float(m["dh"])
+    shape = (nxt, nzt)
+    peak, dyn, Dc, T = (np.zeros(shape) for _ in range(4))
+    coh = np.full(shape, 1.e6)
+    i = np.arange(1, nxt + 1, dtype=np.float64)[:, None]
+    k = np.arange(2, nzt - 1, dtype=np.float64)[None, :]  # k = 2..nzt-2
+    sig = r["sn"] * dh * ((nzt - 2 - k) + (0.0 if dip_slip else 0.5))
+    ks = slice(1, nzt - 2)
+    peak[:, ks] = sig * r["muso"]
+    dyn[:, ks] = sig * r["mud"]
+    nuc = _in_box((i - 1.0) * dh, (k - 1.0) * dh, r["hx0"], r["hz0"], r["hdelta"])
+    T[:, ks] = np.where(nuc, r["T0n"] * r["mus"] * sig + 1.e6, r["T0"] * sig)
+    Dc[:, ks] = r["d0h"]
+    no0 = r["no0"]
+    peak[no0:nxt - no0, no0:nzt - 2] = (sig * r["mus"] + 0.0 * i)[no0:nxt - no0, no0 - 1:]
+    if dip_slip:  # TPV9: the surface row k = nzt-2 at a quarter (src/fd3d_init.f90:670-675)
+        for a in (peak, dyn, T):
+            a[:, nzt - 3] = 0.25 * a[:, nzt - 4]
+        Dc[:, nzt - 3] = r["d0h"]
+    for a in (peak, dyn, Dc):
+        a[:, nzt - 2] = a[:, nzt - 3]
+        a[:, nzt - 1] = a[:, nzt - 4]
+    T[:, nzt - 2] = -T[:, nzt - 3]
+    T[:, nzt - 1] = -T[:, nzt - 4]
+    zero = np.zeros(shape)
+    sX, sZ = (zero, T) if dip_slip else (T, zero)
+    return dict(law="sw", striniX=sX, striniZ=sZ, Dc=Dc, peak_xz=peak, dyn_xz=dyn, coh=coh)
+
+
+def tpv8_fault(m, scec_path):
+    return _tpv89_fault(m, scec_path, dip_slip=False)
+
+
+def tpv9_fault(m, scec_path):
+    """TPV9 is built with -DDIPSLIP (examples/TPV9/compile.sh)."""
+    return _tpv89_fault(m, scec_path, dip_slip=True)
+
+
+def tpv10x_fault(m, scec_path, variant=104):
+    """forwardspecialTPV103 / forwardspecialTPV104 (src/fd3d_init.f90:283-501): rate-and-state
+    fast-velocity-weakening fault whose a and Vw rise outside a smooth box
+    B(x)B(z) (tanh transition of width trans), steady-state psi for the initial slip
+    rate, and the TPV103/104 nucleation ramp.  TPV104 tapers only below the
+    hypocentre row (its z test is one-sided, the tanh argument uses |z - z0| as there).
+    In FP64 (the -r8 build)."""
+    lines = open(scec_path).read().splitlines()
+    wfx, wfz, hx0t, hz0t, trans, fringe = (float(x) for x in _tokens(lines[0], 6))
+    val = [float(_tokens(lines[q], 1)[0]) for q in range(1, 15)]
+    f0, v0, a0, b, d0h, fw, vw0, vwd, vini, Tini, Sn, perturb, RRini, TT2 = val
+    nxt, nzt, dh, nabc = m["nxt"], m["nzt"], float(m["dh"]), m["nabc"]
+    hx0 = hx0t + fringe + nabc * dh
+    hz0 = hz0t + fringe + nabc * dh
+
+    def box(d, w, one_sided_dist=None):
+        t = np.abs(d) if one_sided_dist is None else one_sided_dist
+        ad = np.abs(d)
+        mid = (t > w) & (t < w + trans)
+        with np.errstate(divide="ignore", invalid="ignore"):
+            ramp = 0.5 * (1.0 + np.tanh(trans / (ad - w - trans) + trans / (ad - w)))
+        return np.where(t >= w + trans, 0.0, np.where(mid, ramp, 1.0))
+
+    def taper(off):
+        hx = np.arange(1, nxt + 1, dtype=np.float64)[:, None] * dh + off
+        hz = np.arange(1, nzt + 1, dtype=np.float64)[None, :] * dh + off
+        bx = box(hx - hx0, wfx)
+        bz = box(hz - hz0, wfz, -(hz - hz0) if variant == 104 else None)
+        return bx * bz
+
+    shape = (nxt, nzt)
+    T = np.full(shape, Tini)
+    Bz_, Bx_ = taper(0.0), taper(dh / 2)
+    a = a0 + a0 * (1.0 - Bz_)
+    vw = vw0 + vwd * (1.0 - Bz_)
+    aX = a0 + a0 * (1.0 - Bx_)
+    vwX = vw0 + vwd * (1.0 - Bx_)
+    psi = a * (np.log(2 * v0 / (2 * vini)) + np.log(np.sinh(T / (a * Sn))))
+    psiX = aX * (np.log(2 * v0 / (2 * vini)) + np.log(np.sinh(T / (aX * Sn))))
+    return dict(law="fvw", striniX=T, striniZ=np.zeros(shape), Dc=np.full(shape, d0h), a=a, b=np.full(shape, b),
+                psi=psi, vw=vw, aX=aX, bX=np.full(shape, b), psiX=psiX, vwX=vwX, Sn=Sn, v0=v0, f0=f0, fw=fw,
+                uini=vini, wini=0.0, nucleation=1, hx0=hx0, hz0=hz0, perturb=perturb, RR2=RRini * RRini, TT2=TT2,
+                strinixI=Tini)
+
+
+def read_forward_model(deck_dir):
+    """inversion_init + readinversionresult (src/fd3d_init.f90:786-800, 839-857): the
+    NLI x NWI control points of prestress T0I, static friction TsI and Dc from
+    forwardmodel.dat (the first two values are skipped as there), Fortran order."""
+    lines = open(os.path.join(deck_dir, "inputinv.dat")).read().splitlines()
+    nli, nwi = (int(x) for x in _tokens(lines[1], 2))
+    vals = [float(x.replace("d", "e").replace("D", "e"))
+            for x in open(os.path.join(deck_dir, "forwardmodel.dat")).read().split()]
+    n = nli * nwi
+    if len(vals) < 2 + 3 * n:
+        raise ValueError(f"forwardmodel.dat holds {len(vals)} values, {2 + 3 * n} needed")
+    T0I, TsI, DcI = (np.asarray(vals[2 + q * n:2 + (q + 1) * n]).reshape((nli, nwi), order="F") for q in range(3))
+    return T0I, TsI, DcI
+
+
+def inversion_example(deck_dir, dipslip=False, precision="f32"):
+    """A model as dynamicsolver builds it without -DSCEC (src/dynamicsolver.f90:56-58):
+    the deck's grid and medium, and the fault from the control points of forwardmodel.dat,
+    which Solver uploads with fd3d_upload_fault_model (interpolation on the device)."""
+    m = read_inputfd3d(os.path.join(deck_dir, "inputfd3d.dat"))
+    cr = read_crustal(os.path.join(deck_dir, "crustal.dat"))
+    lam, mu, d, vpm = crustal_medium(m["nzt"], m["dh"], m["dip"], cr["depth"], cr["vp"], cr["vs"], cr["rho"])
+    T0I, TsI, DcI = read_forward_model(deck_dir)
+    m.update(medium=(lam, mu, d), vp_max=vpm, precision=precision, history_stride=1, law="sw",
+             fault_model=dict(T0I=T0I, TsI=TsI, DcI=DcI, dip=m["dip"], dipslip=dipslip))
+    return m
+
+
+SCEC_SETUPS = {"TPV5": None, "TPV8": tpv8_fault, "TPV9": tpv9_fault,
+               "TPV103": lambda m, p: tpv10x_fault(m, p, 103), "TPV104": lambda m, p: tpv10x_fault(m, p, 104)}
+
+
+def reference_example(deck_dir, setup, precision="f32", fspace=False):
+    """A model from one of the reference's example directories (inputfd3d.dat,
+    crustal.dat, scecmodel.dat), as dynamicsolver builds it with -DSCEC -D<setup>
+    (src/dynamicsolver.f90:39-57): fd3d_init, readcrustalmodel and forwardspecial<setup>."""
+    m = read_inputfd3d(os.path.join(deck_dir, "inputfd3d.dat"))
+    if fspace:
+        nab = m["nabc"]
+        m.update(fspace=True, nfs=nab, nzt=m["nzt"] + nab - NFS)
+    cr = read_crustal(os.path.join(deck_dir, "crustal.dat"))
+    lam, mu, d, vpm = crustal_medium(m["nzt"], m["dh"], m["dip"], cr["depth"], cr["vp"], cr["vs"], cr["rho"],
+                                     nfs=m["nfs"])
+    m.update(medium=(lam, mu, d), vp_max=vpm, precision=precision, history_stride=1)
+    scec = os.path.join(deck_dir, "scecmodel.dat")
+    fault = tpv5_fault(m, scec) if setup == "TPV5" else SCEC_SETUPS[setup](m, scec)
+    m["fault"] = fault
+    m["law"] = fault["law"]
+    return m
+
+
 def tpv5_fault(m, scec_path):
     """forwardspecialTPV5 (src/fd3d_init.f90:535-617) from scecmodel.dat."""
     lines = open(scec_path).read().splitlines()

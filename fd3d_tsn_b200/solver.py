@@ -50,7 +50,10 @@ class Solver:
         self.nzT = model["nzt"] - model["nfs"] - model["nabc"]
         self.nf = 5 if model.get("law", "sw") == "fvw" else 4
         self.upload_medium(medium3d)
-        self.upload_fault(model["fault"])
+        if "fault_model" in model:  # control points of forwardmodel.dat (readinversionresult)
+            self.upload_fault_model(**model["fault_model"])
+        else:
+            self.upload_fault(model["fault"])
 
     # ------------------------------------------------------------ inputs
     def upload_medium(self, medium3d: bool = False):

@@ -67,8 +67,13 @@ class Oracle:
                       for a in model["medium"])
         dp = C.POINTER(C.c_double)
         lib().oracle_set_medium(self.h, lam.ctypes.data_as(dp), mu.ctypes.data_as(dp), d.ctypes.data_as(dp))
-        fb = abi.FaultBuffers(model["fault"])
-        lib().oracle_set_fault(self.h, C.byref(fb.s))
+        if "fault_model" in model:  # control points of forwardmodel.dat
+            fm = model["fault_model"]
+            self.set_fault_model(fm["T0I"], fm["TsI"], fm["DcI"], dip=fm.get("dip", 90.0),
+                                 dipslip=fm.get("dipslip", False))
+        else:
+            fb = abi.FaultBuffers(model["fault"])
+            lib().oracle_set_fault(self.h, C.byref(fb.s))
         lib().oracle_reset(self.h)
         self.nxT = model["nxt"] - 2 * model["nabc"]
         self.nzT = model["nzt"] - model["nfs"] - model["nabc"]
