@@ -113,6 +113,13 @@ struct CtxBase {
     void* ring = nullptr;
     void* seis = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    // Side stream of the step: the fault-band and PML sweeps of each half-step run beside
+    // the interior sweep (disjoint cells, both read only the other half-step's fields), so
+    // the latency-bound PML tiles can take SM slots the interior sweep leaves free
+    // (FD3D_OVERLAP=0 puts everything on one stream).
+    cudaStream_t st2 = nullptr;
+    cudaEvent_t evf[4] = {};
+    int overlap = 1;
     float last_ms = 0.f;
     bool profiling = false;
     int pml_minb_vel = 1, pml_minb_str = 4;  // register caps of the PML sweeps (CTAs per SM)
@@ -186,11 +193,16 @@ struct Ctx : CtxBase {
         for (auto e : kev) cudaEventDestroy(e);
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
+        for (auto e : evf) if (e) cudaEventDestroy(e);
+        if (st2) cudaStreamDestroy(st2);
         if (st) cudaStreamDestroy(st);
     }
 
     int alloc() override {
         CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+        if (const char* e = std::getenv("FD3D_OVERLAP")) overlap = std::atoi(e);
+        CK(cudaStreamCreateWithFlags(&st2, cudaStreamNonBlocking));
+        for (auto& e : evf) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
         CK(cudaEventCreate(&ev0));
         CK(cudaEventCreate(&ev1));
         kev.resize(2 * FD3D_NKERNELS);
@@ -487,31 +499,39 @@ struct Ctx : CtxBase {
         const int nxT = p.nxt - 2 * p.nabc;
         const int nzT = g.ks() - p.nabc;
         const dim3 b2(32, 8);
+        const bool ov = overlap > 0 && !profiling;
+        cudaStream_t sp = ov ? st2 : st;  // fault band and PML
+        auto fork = [&](int e) { cudaEventRecord(evf[e], st); cudaStreamWaitEvent(st2, evf[e], 0); };
+        auto join = [&](int e) { cudaEventRecord(evf[e], st2); cudaStreamWaitEvent(st, evf[e], 0); };
         // velocity half-step
+        if (ov) fork(0);
         kbeg(0);
         if (icfg.variant == IV_TMA) launch_vel_interior_tma<T>(vmaps, icfg, g, f, c, status, st);
         else launch_vel_interior<T>(icfg, g, f, c, st);
         kend(0);
         kbeg(1);
-        k_vel_fault<T><<<dim3((std::max(nxT, p.nxt) + 31) / 32, (nzT + 7) / 8), b2, 0, st>>>(g, f, q, c, law, fs, it_dev, status);
+        k_vel_fault<T><<<dim3((std::max(nxT, p.nxt) + 31) / 32, (nzT + 7) / 8), b2, 0, sp>>>(g, f, q, c, law, fs, it_dev, status);
         kend(1);
         kbeg(2);
-        launch_pml<T>(false, pml_minb_vel, st, g, f, D, X, c, status);
+        launch_pml<T>(false, pml_minb_vel, sp, g, f, D, X, c, status);
         kend(2);
+        if (ov) join(1);
         kbeg(3);
         if (!p.fspace) k_vel_fs<T><<<dim3((p.nxt + 31) / 32, (p.nyt + 7) / 8), b2, 0, st>>>(g, f);  // fuvw
         kend(3);
         // stress half-step
+        if (ov) fork(2);
         kbeg(4);
         if (icfg.variant == IV_TMA) launch_str_interior_tma<T>(smaps, icfg, g, f, c, status, st);
         else launch_str_interior<T>(icfg, g, f, c, st);
         kend(4);
         kbeg(5);
-        k_str_fault<T><<<dim3((nxT + 31) / 32, (nzT + 7) / 8), b2, 0, st>>>(g, f, q, c);
+        k_str_fault<T><<<dim3((nxT + 31) / 32, (nzT + 7) / 8), b2, 0, sp>>>(g, f, q, c);
         kend(5);
         kbeg(6);
-        launch_pml<T>(true, pml_minb_str, st, g, f, D, X, c, status);
+        launch_pml<T>(true, pml_minb_str, sp, g, f, D, X, c, status);
         kend(6);
+        if (ov) join(3);
         // fault boundary condition
         kbeg(7);
         if (!p.fspace) k_str_fs<T><<<dim3((p.nxt + 31) / 32, (p.nyt + 7) / 8), b2, 0, st>>>(g, f);  // fres
