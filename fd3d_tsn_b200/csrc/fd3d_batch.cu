@@ -368,7 +368,7 @@ size_t model_bytes(const fd3d_params& p, const Grid& g, const PmlDesc& D, int pr
     add((size_t)prof_n * sizeof(Damp<float>));
     add((size_t)cap * nf * plane * 4);
     add((size_t)cap * std::max(1, p.nstations) * 3 * 4);
-    add((size_t)4 * p.nzt * 4);
+    add((size_t)LAY_N * p.nzt * 4);
     add(64);
     return b + 256;
 }
@@ -845,7 +845,7 @@ int fd3d_batch_add(fd3d_batch* b, const fd3d_params* pin, const double* lam_k, c
     const size_t plane = (size_t)(p.nxt - 2 * p.nabc) * (p.nzt - p.nfs - p.nabc);
     float* ring = bp.take<float>((size_t)M.cap * M.nf * plane);
     float* seis = bp.take<float>((size_t)M.cap * std::max(1, p.nstations) * 3);
-    float* layers = bp.take<float>((size_t)4 * p.nzt);
+    float* layers = bp.take<float>((size_t)LAY_N * p.nzt);
     d.f.lay = layers;  // batch models always carry a 1-D medium
     d.it_dev = bp.take<int>(1);
     d.status = bp.take<int>(1);
@@ -860,10 +860,11 @@ int fd3d_batch_add(fd3d_batch* b, const fd3d_params* pin, const double* lam_k, c
     }
     // whole block to zero, then medium, fault planes and profiles
     BCK(cudaMemsetAsync(b->arena_base + M.off, 0, bp.used, b->sst));
-    std::vector<float> lay(4 * (size_t)p.nzt);
+    std::vector<float> lay(LAY_N * (size_t)p.nzt);
     for (int k = 0; k < p.nzt; ++k) {
         lay[k] = (float)lam_k[k]; lay[p.nzt + k] = (float)mu_k[k]; lay[2 * p.nzt + k] = (float)d_k[k];
-        lay[3 * p.nzt + k] = d.c.dth / lay[2 * p.nzt + k];  // the IEEE quotient the sweep would form
+        lay[3 * p.nzt + k] = d.c.dth / lay[2 * p.nzt + k];  // the IEEE quotients the sweeps would form
+        lay[4 * p.nzt + k] = d.c.dt / lay[2 * p.nzt + k];
     }
     BCK(cudaMemcpyAsync(layers, lay.data(), lay.size() * sizeof(float), cudaMemcpyHostToDevice, b->sst));
     k_fill_layers<<<1024, 256, 0, b->sst>>>(d.g, lam, mu, dd, layers, layers + p.nzt, layers + 2 * p.nzt);

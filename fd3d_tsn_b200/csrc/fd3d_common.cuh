@@ -58,11 +58,13 @@ struct Fields {
     const T *lam, *mu, *d;
     // The same medium as a 1-D profile when it varies with k only (the layered medium
     // of readcrustalmodel): lam at lay[k-1], mu at lay[nzt+k-1], d at lay[2*nzt+k-1],
-    // and dth/d (the IEEE quotient the velocity sweep forms per cell) at lay[3*nzt+k-1];
-    // null otherwise.  The interior sweeps then read values per plane instead of arrays
-    // per cell.
+    // dth/d (the IEEE quotient the interior velocity sweep forms per cell) at
+    // lay[3*nzt+k-1] and dt/d (the PML velocity sweep's) at lay[4*nzt+k-1]; null
+    // otherwise.  The interior and PML sweeps then read values per plane instead of
+    // arrays per cell.
     const T* lay;
 };
+constexpr int LAY_N = 5;  // profile entries per plane
 
 // Fault-plane state.  F = field type, double = accumulators (slip, slip path,
 // rupture time, rise, slip time, psi).

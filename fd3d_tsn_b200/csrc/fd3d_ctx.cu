@@ -37,7 +37,7 @@ namespace fd3d {
 // (1,1,k) in all three arrays (sets *nonuniform otherwise); the profile of column (1,1)
 // goes to tab (lam, mu, d and dth/d, nzt values each).
 template <class T>
-__global__ void k_layer_check(Grid g, const T* lam, const T* mu, const T* d, T dth, T* tab, int* nonuniform) {
+__global__ void k_layer_check(Grid g, const T* lam, const T* mu, const T* d, T dth, T dt, T* tab, int* nonuniform) {
     const long long n = (long long)g.nxt * g.nyt * g.nzt;
     int bad = 0;
     for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
@@ -51,6 +51,7 @@ __global__ void k_layer_check(Grid g, const T* lam, const T* mu, const T* d, T d
             tab[g.nzt + k - 1] = mu[p0];
             tab[2 * g.nzt + k - 1] = d[p0];
             tab[3 * g.nzt + k - 1] = dth / d[p0];
+            tab[4 * g.nzt + k - 1] = dt / d[p0];
         }
     }
     if (__syncthreads_or(bad) && threadIdx.x == 0) atomicOr(nonuniform, 1);
@@ -230,7 +231,7 @@ struct Ctx : CtxBase {
                           carve(prof.size() * sizeof(Damp<T>)) + 2 * carve(sizeof(int)) +
                           carve((size_t)cap * nf * plane * sizeof(T)) +
                           carve((size_t)cap * std::max(1, p.nstations) * 3 * sizeof(T)) +
-                          carve((size_t)4 * p.nzt * sizeof(T)) + carve(sizeof(int)) + 2 * carve(n2 * sizeof(double)) +
+                          carve((size_t)LAY_N * p.nzt * sizeof(T)) + carve(sizeof(int)) + 2 * carve(n2 * sizeof(double)) +
                           carve((size_t)POST_BLOCKS * POST_NSUM * sizeof(double)) + carve(POST_NSUM * sizeof(double)) +
                           carve((size_t)cap * sizeof(double));
             void* v = nullptr;
@@ -271,7 +272,7 @@ struct Ctx : CtxBase {
         T* sg = nullptr;
         if (dalloc(&sg, (size_t)cap * std::max(1, p.nstations) * 3)) return FD3D_ERR_NOMEM;
         seis = sg;
-        if (dalloc(&dlay, (size_t)4 * p.nzt)) return FD3D_ERR_NOMEM;
+        if (dalloc(&dlay, (size_t)LAY_N * p.nzt)) return FD3D_ERR_NOMEM;
         if (dalloc(&lflag, 1)) return FD3D_ERR_NOMEM;
         if (dalloc(&rvel_d, n2) || dalloc(&czone_d, n2) || dalloc(&part_d, (size_t)POST_BLOCKS * POST_NSUM) ||
             dalloc(&sums_d, POST_NSUM) || dalloc(&mrate_d, (size_t)cap))
@@ -285,7 +286,7 @@ struct Ctx : CtxBase {
     int medium_uploaded() {
         int nonuni = 0;
         CK(cudaMemsetAsync(lflag, 0, sizeof(int), st));
-        k_layer_check<T><<<1024, 256, 0, st>>>(g, f.lam, f.mu, f.d, c.dth, dlay, lflag);
+        k_layer_check<T><<<1024, 256, 0, st>>>(g, f.lam, f.mu, f.d, c.dth, c.dt, dlay, lflag);
         CK(cudaGetLastError());
         CK(cudaMemcpyAsync(&nonuni, lflag, sizeof(int), cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));

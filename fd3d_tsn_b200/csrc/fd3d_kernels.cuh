@@ -254,7 +254,7 @@ __device__ __forceinline__ bool vel_pml_tile(const Grid& g, const Fields<T>& f, 
     pml_tile_begin(sm, gaux, AUX_NV, bar);
     int s = 0, i = 0, j = 0, k = 0;
     const bool act = pml_locate(D, t0 + l, s, i, j, k);
-    T d = 1, xx0 = 0, xx1 = 0, xy0 = 0, xy1 = 0, xz0 = 0, xz1 = 0, xz2 = 0, yz0 = 0, yz1 = 0, zz0 = 0, zz1 = 0;
+    T d = 1, rl = 0, xx0 = 0, xx1 = 0, xy0 = 0, xy1 = 0, xz0 = 0, xz1 = 0, xz2 = 0, yz0 = 0, yz1 = 0, zz0 = 0, zz1 = 0;
     T xy2 = 0, yy0 = 0, yy1 = 0, yz2 = 0, vold = 0;
     Damp<T> ox{}, oxS{}, oy{}, oz{};
     long long p = 0;
@@ -267,7 +267,8 @@ __device__ __forceinline__ bool vel_pml_tile(const Grid& g, const Fields<T>& f, 
         oy = X.prof[S.oy_off + j2]; oz = X.prof[S.oz_off + k2];
         p = g.at(i, j, k);
         dov = (j <= S.nye);
-        d = f.d[p];
+        if (f.lay) rl = f.lay[4 * g.nzt + k - 1];  // dt/d of the plane (1-D medium)
+        else d = f.d[p];
         xx0 = f.xx[p]; xx1 = f.xx[p - 1]; xy0 = f.xy[p]; xy1 = f.xy[p - sy]; xz0 = f.xz[p]; xz1 = f.xz[p - sz];
         xz2 = f.xz[p + 1]; yz0 = f.yz[p]; yz1 = f.yz[p - sy]; zz0 = f.zz[p]; zz1 = f.zz[p + sz];
         if (dov) {
@@ -278,7 +279,7 @@ __device__ __forceinline__ bool vel_pml_tile(const Grid& g, const Fields<T>& f, 
     if (!pml_tile_wait(bar, parity, status)) return false;
     if (act) {
         const T dt = c.dt, dh = c.dh, rdh = c.rdh;
-        const T r = dt / d;
+        const T r = f.lay ? rl : dt / d;
         // p = (p*(1 - omega) + (dt/d)*diff/dh) / (1 + omega), every division rounded as IEEE
         // Where omega is 0 (most split directions of a strip) a*(1-0) = a and x/(1+0) = x
         // exactly, so the branch skips a multiply and a division without changing a bit.
@@ -454,12 +455,17 @@ __device__ __forceinline__ bool str_pml_tile(const Grid& g, const Fields<T>& f, 
         p = g.at(i, j, k);
         dxy = (j <= S.nye);
         top = !g.fspace && (s <= 2) && (k == S.nze);  // xz/yz aux zeroed at the top row, strips 1-3 (not FSPACE)
-        xl = f.lam[p]; xm = f.mu[p]; mz = f.mu[p + sz];
+        if (f.lay) {  // 1-D medium: mu(i,j+1,k) = mu(i,j,k), mu(i+1,j+1,k+1) = mu(i,j,k+1)
+            xl = f.lay[k - 1]; xm = f.lay[g.nzt + k - 1]; mz = f.lay[g.nzt + k];
+        } else {
+            xl = f.lam[p]; xm = f.mu[p]; mz = f.mu[p + sz];
+        }
         up = f.u[p]; ux = f.u[p + 1]; uz = f.u[p + sz];
         vp = f.v[p]; vy = f.v[p - sy];
         wp = f.w[p]; wz = f.w[p - sz]; wx = f.w[p - 1];
         if (dxy) {
-            my = f.mu[p + sy]; md = f.mu[p + 1 + sy + sz];
+            if (f.lay) { my = xm; md = mz; }
+            else { my = f.mu[p + sy]; md = f.mu[p + 1 + sy + sz]; }
             uy = f.u[p + sy]; vx = f.v[p - 1]; vz = f.v[p + sz]; wy = f.w[p + sy];
             if (j == g.nyt - 1) { xyo = f.xy[p]; yzo = f.yz[p]; }
         }
