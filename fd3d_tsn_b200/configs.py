@@ -83,6 +83,13 @@ def gaussian_field(rng, nx, nz, corr_nodes, mean, std):
     return mean + std * f
 
 
+def fortran_planes(fault: dict) -> dict:
+    """Fault planes in Fortran order (x fastest), as a Fortran host holds them: the C ABI
+    takes them without a copy."""
+    return {k: (np.asfortranarray(v, dtype=np.float64) if isinstance(v, np.ndarray) and v.ndim == 2 else v)
+            for k, v in fault.items()}
+
+
 def _grid(nxT, nyT, nzT, h, dt, ntfd, nabc=NABC, fspace=False):
     """Padded grid of fd3d_init.f90:161-169; fspace: the FSPACE build (a PML strip of
     nabc cells above the model instead of the free surface, nfs = nabc)."""
@@ -146,8 +153,8 @@ def sw_model(nxT, nyT, nzT, h, sim_time, seed, layers=None, patch_nodes=None, ns
     nab = m["nabc"]
     i0 = nab + 1 + (nxT - px) // 2
     k0 = nab + 1 + (nzT - pz) // 2
-    m["fault"] = sw_fault(m, rng, (i0, i0 + px - 1, k0, k0 + pz - 1), corr_m=corr_m, dc_patch_m=dc_patch_m,
-                          dc_range=dc_range)
+    m["fault"] = fortran_planes(sw_fault(m, rng, (i0, i0 + px - 1, k0, k0 + pz - 1), corr_m=corr_m,
+                                         dc_patch_m=dc_patch_m, dc_range=dc_range))
     m["stations"] = _stations(rng, m, nstations)
     m["seed"] = seed
     return m
@@ -222,7 +229,7 @@ def fvw_model(nxT, nyT, nzT, h, sim_time, seed, fault_m=(48e3, 24e3), dt=None, h
                  fwZ=fw, fwX=fw.copy(), Sn=Sn, v0=v0, f0=f0, fw=0.15, uini=uini, wini=0.0,
                  nucleation=2, hx0=(i0 + fx // 2) * h, hz0=(k1 - fz // 2) * h, perturb=perturb, RR2=R * R,
                  TT2=TT, strinixI=float(np.mean(tau)))
-    m["fault"] = fault
+    m["fault"] = fortran_planes(fault)
     m["stations"] = _stations(rng, m, nstations)
     m["seed"] = seed
     return m
@@ -286,8 +293,9 @@ def fspace_variant(m: dict) -> dict:
     extra = nab - m["nfs"]
     f = dict(m, fspace=True, nfs=nab, nzt=m["nzt"] + extra)
     f["medium"] = tuple(np.concatenate([np.asarray(a), np.repeat(np.asarray(a)[-1:], extra)]) for a in m["medium"])
-    f["fault"] = {k: (np.concatenate([v, np.repeat(v[:, -1:], extra, axis=1)], axis=1)
-                      if isinstance(v, np.ndarray) and v.ndim == 2 else v) for k, v in m["fault"].items()}
+    f["fault"] = fortran_planes({k: (np.concatenate([v, np.repeat(v[:, -1:], extra, axis=1)], axis=1)
+                                     if isinstance(v, np.ndarray) and v.ndim == 2 else v)
+                                 for k, v in m["fault"].items()})
     return f
 
 
@@ -513,7 +521,7 @@ def reference_example(deck_dir, setup, precision="f32", fspace=False):
     m.update(medium=(lam, mu, d), vp_max=vpm, precision=precision, history_stride=1)
     scec = os.path.join(deck_dir, "scecmodel.dat")
     fault = tpv5_fault(m, scec) if setup == "TPV5" else SCEC_SETUPS[setup](m, scec)
-    m["fault"] = fault
+    m["fault"] = fortran_planes(fault)
     m["law"] = fault["law"]
     return m
 

@@ -86,6 +86,19 @@ __global__ void k_model_to_fd3d(Grid g, int nli, const T* T0I, const T* TsI, con
     q.DcZ[p] = dc;
 }
 
+// A contiguous Fortran-order (nxt,nyt,nzt) array, staged on the device, into the padded
+// layout (element type converted when the host's real kind differs from the field type)
+template <class T, class S>
+__global__ void k_repack(Grid g, const S* __restrict__ src, T* __restrict__ dst) {
+    const long long n = (long long)g.nxt * g.nyt * g.nzt;
+    for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
+        const int i = 1 + (int)(q % g.nxt);
+        const long long r = q / g.nxt;
+        const int j = 1 + (int)(r % g.nyt), k = 1 + (int)(r / g.nyt);
+        dst[g.at(i, j, k)] = (T)src[q];
+    }
+}
+
 // interp_fric (fd3d_deriv.f90:3174-3189): X-node values are 4-point averages
 template <class T>
 __global__ void k_interp_fric(Grid g, Fault<T> q) {
@@ -302,10 +315,24 @@ struct Ctx : CtxBase {
         const size_t n = (size_t)p.nxt * p.nyt * p.nzt;
         const void* src[3] = {l, m, d};
         T* dst[3] = {(T*)f.lam, (T*)f.mu, (T*)f.d};
+        for (int a = 0; a < 3; ++a)
+            if (!src[a]) return FD3D_ERR_ARG;
+        if (steps_done == 0 && n * (size_t)rk <= (size_t)g.n3 * 9 * sizeof(T)) {
+            // The wave field is still zero: use it as the staging buffer of one contiguous
+            // copy per array (the host array as it lies), repack on the device, zero it again.
+            for (int a = 0; a < 3; ++a) {
+                CK(cudaMemcpyAsync(fieldpool, src[a], n * (size_t)rk, cudaMemcpyHostToDevice, st));
+                if (rk == 8) k_repack<T, double><<<1184, 256, 0, st>>>(g, (const double*)fieldpool, dst[a]);
+                else k_repack<T, float><<<1184, 256, 0, st>>>(g, (const float*)fieldpool, dst[a]);
+                CK(cudaGetLastError());
+            }
+            CK(cudaMemsetAsync(fieldpool, 0, n * (size_t)rk, st));
+            CK(cudaStreamSynchronize(st));
+            return medium_uploaded();
+        }
         if ((size_t)rk == sizeof(T)) {
             // same element type: one pitched copy per array straight into the padded rows
             for (int a = 0; a < 3; ++a) {
-                if (!src[a]) return FD3D_ERR_ARG;
                 CK(cudaMemcpy2DAsync(dst[a] + g.off, (size_t)g.px * sizeof(T), src[a], (size_t)p.nxt * sizeof(T),
                                      (size_t)p.nxt * sizeof(T), (size_t)p.nyt * p.nzt, cudaMemcpyHostToDevice, st));
             }
@@ -314,7 +341,6 @@ struct Ctx : CtxBase {
         }
         std::vector<T> row((size_t)g.px * p.nyt * 16);
         for (int a = 0; a < 3; ++a) {
-            if (!src[a]) return FD3D_ERR_ARG;
             // pack k-slabs into the padded layout on the host, one copy per slab
             const int kb = 16;
             for (int k0 = 0; k0 < p.nzt; k0 += kb) {
@@ -376,9 +402,7 @@ struct Ctx : CtxBase {
         if (!fl->striniX || !fl->Dc) return FD3D_ERR_ARG;
         std::vector<T> sX = cp(fl->striniX, 0), sZ = cp(fl->striniZ, 0), Dc = cp(fl->Dc, 0);
         std::vector<T> zero(n2, (T)0);
-        std::vector<T> pkX = zero, dyX = zero, DcX = zero, T0X = zero;
         std::vector<T> pkZ = zero, dyZ = zero, DcZ = zero, T0Z = sZ, coh = zero;
-        auto I2 = [&](int i, int k) { return (size_t)(i - 1) + (size_t)nxt * (k - 1); };
         int rc = 0;
         if (law == FD3D_LAW_FVW) {
             if (!fl->a || !fl->b || !fl->psi || !fl->vw || !fl->aX || !fl->bX || !fl->psiX || !fl->vwX) return FD3D_ERR_ARG;
@@ -396,19 +420,16 @@ struct Ctx : CtxBase {
             pkZ = cp(fl->peak_xz, 0); dyZ = cp(fl->dyn_xz, 0); DcZ = Dc; coh = cp(fl->coh, 0);
             fs = FvwScalars{};
         }
-        for (int i = 2; i <= nxt - 1; ++i)
-            for (int k = 2; k <= nzt - 1; ++k) {
-                if (law != FD3D_LAW_FVW) {
-                    pkX[I2(i, k)] = (pkZ[I2(i, k)] + pkZ[I2(i - 1, k)] + pkZ[I2(i, k - 1)] + pkZ[I2(i - 1, k - 1)]) / (T)4;
-                    dyX[I2(i, k)] = (dyZ[I2(i, k)] + dyZ[I2(i - 1, k)] + dyZ[I2(i, k - 1)] + dyZ[I2(i - 1, k - 1)]) / (T)4;
-                    DcX[I2(i, k)] = (DcZ[I2(i, k)] + DcZ[I2(i - 1, k)] + DcZ[I2(i, k - 1)] + DcZ[I2(i - 1, k - 1)]) / (T)4;
-                }
-                T0X[I2(i, k)] = (sX[I2(i, k)] + sX[I2(i - 1, k)] + sX[I2(i, k - 1)] + sX[I2(i - 1, k - 1)]) / (T)4;
-            }
-        rc |= up2(q.Dc, Dc); rc |= up2(q.T0X, T0X); rc |= up2(q.T0Xb, T0X); rc |= up2(q.T0Z, T0Z);
-        rc |= up2(q.peakX, pkX); rc |= up2(q.dynX, dyX); rc |= up2(q.DcX, DcX);
+        // Z-node planes up; X-node planes (4-point averages, zero on the border) by
+        // k_interp_fric on the device, T0X from striniX staged in T0Xb
+        rc |= up2(q.Dc, Dc); rc |= up2(q.T0Xb, sX); rc |= up2(q.T0Z, T0Z);
         rc |= up2(q.peakZ, pkZ); rc |= up2(q.dynZ, dyZ); rc |= up2(q.DcZ, DcZ); rc |= up2(q.coh, coh);
         if (rc) return FD3D_ERR_CUDA;
+        T* xnodes[] = {q.peakX, q.dynX, q.DcX, q.T0X};
+        for (T* a : xnodes) CK(cudaMemsetAsync(a, 0, n2 * sizeof(T), st));
+        k_interp_fric<T><<<dim3((p.nxt + 31) / 32, (p.nzt + 7) / 8), dim3(32, 8), 0, st>>>(g, q);
+        CK(cudaGetLastError());
+        CK(cudaMemcpyAsync(q.T0Xb, q.T0X, n2 * sizeof(T), cudaMemcpyDeviceToDevice, st));
         CK(cudaStreamSynchronize(st));
         fault_ok = true;
         return reset_state(false);
