@@ -341,13 +341,18 @@ def end_to_end(m, steps, local):
     t0 = time.perf_counter()
     s.upload_medium_arrays(*host, real_kind=4)
     s.upload_fault(m["fault"])
+    # Chunks of steps are enqueued one ahead: the records of a chunk are read back while
+    # the next chunk runs (a read waits only for the run that made its records).
     done = got = 0
-    while done < steps:
-        n = min(chunk, steps - done)
-        s.run(n)
-        s.sync()
-        done += n
-        have = done // stride
+    ready = 0                    # steps of the chunks enqueued before the latest one
+    while got < nrec or done < steps:
+        if done < steps:
+            n = min(chunk, steps - done)
+            s.run(n)
+            done += n
+        else:
+            ready = done
+        have = ready // stride
         if have > got:
             for f in range(nf):
                 rc = lib().fd3d_fetch_history(s.h, f, got, have - got, hist[f, got:have].ctypes.data, 4)
@@ -359,6 +364,8 @@ def end_to_end(m, steps, local):
                 if rc:
                     raise abi.Fd3dError(rc, "fd3d_fetch_stations")
             got = have
+        ready = done
+    s.sync()
     dt = time.perf_counter() - t0
     s.close()
     fault_bytes = 6 * m["nxt"] * m["nzt"] * 8

@@ -133,6 +133,25 @@ struct CtxBase {
     // (FD3D_OVERLAP=0 puts everything on one stream).
     cudaStream_t st2 = nullptr;
     cudaEvent_t evf[4] = {};
+    // Completion marks of the last runs: a history or station read waits for the run that
+    // made its records only, so the runs enqueued after it keep the GPU busy meanwhile.
+    static constexpr int NMARK = 8;
+    cudaEvent_t mark_ev[NMARK] = {};
+    int mark_steps[NMARK] = {};
+    int nmark = 0, next_mark = 0;
+    void mark_run() {
+        if (cudaEventRecord(mark_ev[next_mark], st) != cudaSuccess) { cudaGetLastError(); return; }
+        mark_steps[next_mark] = steps_done;
+        next_mark = (next_mark + 1) % NMARK;
+        nmark = std::min(nmark + 1, NMARK);
+    }
+    // wait until the first `steps` steps have completed
+    cudaError_t wait_steps(int steps) {
+        int best = -1;
+        for (int m = 0; m < nmark; ++m)
+            if (mark_steps[m] >= steps && (best < 0 || mark_steps[m] < mark_steps[best])) best = m;
+        return best < 0 ? cudaStreamSynchronize(st) : cudaEventSynchronize(mark_ev[best]);
+    }
     int overlap = 1;
     float last_ms = 0.f;
     bool profiling = false;
@@ -208,6 +227,7 @@ struct Ctx : CtxBase {
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
         for (auto e : evf) if (e) cudaEventDestroy(e);
+        for (auto e : mark_ev) if (e) cudaEventDestroy(e);
         if (st2) cudaStreamDestroy(st2);
         if (st) cudaStreamDestroy(st);
     }
@@ -217,6 +237,7 @@ struct Ctx : CtxBase {
         if (const char* e = std::getenv("FD3D_OVERLAP")) overlap = std::atoi(e);
         CK(cudaStreamCreateWithFlags(&st2, cudaStreamNonBlocking));
         for (auto& e : evf) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        for (auto& e : mark_ev) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
         CK(cudaEventCreate(&ev0));
         CK(cudaEventCreate(&ev1));
         kev.resize(2 * FD3D_NKERNELS);
@@ -498,6 +519,7 @@ struct Ctx : CtxBase {
         CK(cudaStreamSynchronize(st));
         steps_done = 0;
         rec_written = 0;
+        nmark = 0;
         return FD3D_OK;
     }
 
@@ -800,6 +822,7 @@ int fd3d_run(fd3d_ctx* ctx, int nsteps) {
     CK(cudaGetLastError());
     CK(cudaEventRecord(c->ev1, c->st));
     c->steps_done += nsteps;
+    c->mark_run();
     return FD3D_OK;
 }
 
@@ -859,7 +882,7 @@ int fd3d_fetch_history(fd3d_ctx* ctx, int field, int rec0, int nrec, void* host,
     if (field < 0 || field >= c->nf) return FD3D_ERR_ARG;
     const int have = c->steps_done / c->p.history_stride;
     if (rec0 + nrec > have || rec0 < have - c->hist_cap) return FD3D_ERR_ARG;  // overwritten or not yet made
-    CK(cudaStreamSynchronize(c->st));
+    CK(c->wait_steps((rec0 + nrec) * c->p.history_stride));
     const size_t plane = (size_t)(c->p.nxt - 2 * c->p.nabc) * (c->p.nzt - c->p.nfs - c->p.nabc);
     const size_t es = c->elem();
     if ((size_t)rk == es) {
@@ -894,7 +917,7 @@ int fd3d_fetch_stations(fd3d_ctx* ctx, int rec0, int nrec, double* host) {
     CtxBase* c = ctx->impl;
     const int have = c->steps_done / c->p.history_stride;
     if (rec0 + nrec > have || rec0 < have - c->hist_cap) return FD3D_ERR_ARG;
-    CK(cudaStreamSynchronize(c->st));
+    CK(c->wait_steps((rec0 + nrec) * c->p.history_stride));
     const int ns = c->p.nstations;
     if (ns == 0) return FD3D_OK;
     const size_t es = c->elem();
@@ -1031,6 +1054,7 @@ int run_noalloc_t(Ctx<T>* c, int nsteps, void* scratch) {
     CK(cudaGetLastError());
     CK(cudaEventRecord(c->ev1, c->st));
     c->steps_done += nsteps;
+    c->mark_run();
     return FD3D_OK;
 }
 }  // namespace

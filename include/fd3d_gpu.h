@@ -192,6 +192,10 @@ int fd3d_sync(fd3d_ctx* ctx);                       /* wait; returns first devic
  * calls whose work overlaps on one GPU (contexts on different streams) race on it. */
 int fd3d_run_noalloc(fd3d_ctx* ctx, int nsteps);
 int fd3d_steps_done(fd3d_ctx* ctx, int* it);
+/* Records rec0..rec0+nrec-1 of one history plane (x fastest per record).  Waits only for
+ * the fd3d_run that made the last of them: runs enqueued after it keep the GPU busy while
+ * the records are copied (they must still be in the ring, which holds history_capacity
+ * records counted back from the last enqueued step).  fd3d_fetch_stations likewise. */
 int fd3d_fetch_history(fd3d_ctx* ctx, int field, int rec0, int nrec, void* host, int real_kind);
 int fd3d_history_records(fd3d_ctx* ctx, int* nrec);  /* records held in the device ring */
 int fd3d_fetch_stations(fd3d_ctx* ctx, int rec0, int nrec, double* host /* nrec*nst*3 */);

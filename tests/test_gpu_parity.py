@@ -283,3 +283,24 @@ def test_fault_from_inversion_control_points(dipslip):
     assert np.abs(oh[:, 0:2]).max() > 0, "the weak spot must slip"
     np.testing.assert_array_equal(gh, oh[:, :s.nf])
     np.testing.assert_array_equal(s.final()["slipX"], o.plane("slipX"))
+
+
+def test_history_read_while_next_run_is_queued():
+    """fd3d_fetch_history waits only for the run that made the records it reads: the
+    records of one run come back while the next run is still queued, and both sets are
+    the oracle's."""
+    m = configs.tiny_sw(seed=19, nsteps=60)
+    m["history_capacity"] = 40
+    oh, os_ = Oracle(m, MIXED).step(60)
+    s = Solver(m)
+    s.run(20)
+    s.run(20)                       # queued behind the first run
+    first = np.stack([s.history(f, rec0=0, nrec=20) for f in range(4)], axis=1)
+    st = s.stations(rec0=0, nrec=20)
+    s.run(20)
+    second = np.stack([s.history(f, rec0=20, nrec=20) for f in range(4)], axis=1)
+    s.sync()
+    third = np.stack([s.history(f, rec0=40, nrec=20) for f in range(4)], axis=1)
+    np.testing.assert_array_equal(np.concatenate([first, second, third]), oh[:, :4])
+    np.testing.assert_array_equal(st, os_[:20])
+    s.close()
