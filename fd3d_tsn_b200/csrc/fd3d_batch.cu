@@ -124,7 +124,10 @@ struct ModelMaps {  // TMA descriptors of one model's interior sweeps (global me
     StrMaps s;
 };
 
-constexpr int BATCH_MIN_CTAS = 3;  // register cap so that 3 CTAs of 256 threads fit an SM
+#ifndef FD3D_BATCH_MINB
+#define FD3D_BATCH_MINB 3
+#endif
+constexpr int BATCH_MIN_CTAS = FD3D_BATCH_MINB;  // register cap so that this many CTAs of 256 threads fit an SM
 
 __global__ void __launch_bounds__(256, BATCH_MIN_CTAS)
 k_batch(const ModelDev* __restrict__ models, const ModelMaps* __restrict__ maps, const Work* __restrict__ work,
