@@ -185,7 +185,8 @@ def sw_large(seed=2, **kw):
 
 
 def fvw_model(nxT, nyT, nzT, h, sim_time, seed, fault_m=(48e3, 24e3), dt=None, history_stride=5,
-              precision="f32", nstations=4, border_m=3000.0, perturb=45e6, R=3000.0, TT=1.0, ntfd=None):
+              precision="f32", nstations=4, border_m=3000.0, perturb=45e6, R=3000.0, TT=1.0, ntfd=None,
+              fspace=False):
     """Fast-velocity-weakening model: a uniform in [0.008,0.012] inside, ramping to 0.02
     over the border; b=0.014; L in [0.2,0.5]; f0=0.6; V0=1e-6; fw in [0.1,0.2]; Vw 0.1
     ramping to 1.0 in the border; initial slip rate 1e-16 (uini = 0.5e-16, as the TPV104
@@ -195,8 +196,8 @@ def fvw_model(nxT, nyT, nzT, h, sim_time, seed, fault_m=(48e3, 24e3), dt=None, h
     vp, vs, rho = 6000.0, 3464.0, 2670.0
     dt = dt if dt is not None else 0.002 * h / 100.0
     nsteps = int(round(sim_time / dt)) if ntfd is None else ntfd
-    m = _grid(nxT, nyT, nzT, h, dt, nsteps)
-    lam, mu, d, vpm = crustal_medium(m["nzt"], h, 90.0, [0.0], [vp], [vs], [rho])
+    m = _grid(nxT, nyT, nzT, h, dt, nsteps, fspace=fspace)
+    lam, mu, d, vpm = crustal_medium(m["nzt"], h, 90.0, [0.0], [vp], [vs], [rho], nfs=m["nfs"])
     m.update(medium=(lam, mu, d), vp_max=vpm, law="fvw", precision=precision, history_stride=history_stride)
     nxt, nzt = m["nxt"], m["nzt"]
     nab = m["nabc"]
@@ -205,7 +206,7 @@ def fvw_model(nxT, nyT, nzT, h, sim_time, seed, fault_m=(48e3, 24e3), dt=None, h
     fx, fz = int(round(fault_m[0] / h)), int(round(fault_m[1] / h))
     fx, fz = min(fx, nxT), min(fz, nzT)
     i0 = nab + 1 + (nxT - fx) // 2
-    k1 = nzt - NFS
+    k1 = nzt - m["nfs"]
     k0 = k1 - fz + 1
     bw = border_m / h
 
@@ -306,9 +307,9 @@ def tiny_sw(seed=5, nxT=40, nyT=14, nzT=28, h=200.0, nsteps=60, precision="f32",
                     precision=precision, ntfd=nsteps, history_stride=stride, corr_m=600.0, fspace=fspace)
 
 
-def tiny_fvw(seed=6, nxT=40, nyT=14, nzT=28, h=200.0, nsteps=60, precision="f32", stride=1):
+def tiny_fvw(seed=6, nxT=40, nyT=14, nzT=28, h=200.0, nsteps=60, precision="f32", stride=1, fspace=False):
     return fvw_model(nxT, nyT, nzT, h, 1.0, seed, fault_m=(6000.0, 4000.0), dt=0.004, history_stride=stride,
-                     precision=precision, ntfd=nsteps, border_m=800.0, R=1200.0, TT=0.1)
+                     precision=precision, ntfd=nsteps, border_m=800.0, R=1200.0, TT=0.1, fspace=fspace)
 
 
 # ---------------------------------------------------------------- reference decks

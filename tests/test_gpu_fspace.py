@@ -93,3 +93,19 @@ def test_fspace_model_in_a_batch(schedule):
             np.testing.assert_array_equal(fb[k], fs[k], err_msg=k)
         np.testing.assert_array_equal(b.history(slot, 0, 0, steps), s.history(0, 0, steps))
         s.close()
+
+
+@pytest.mark.parametrize("precision,variant,tol", [("f32", MIXED, 1e-5), ("f64", F64, 1e-9)])
+def test_fspace_fvw_matches_oracle(precision, variant, tol):
+    """Rate-and-state friction with the top PML strip (the fault reaches the top row)."""
+    m = configs.tiny_fvw(nsteps=60, precision=precision, fspace=True)
+    o = Oracle(m, variant)
+    oh, _ = o.step(60)
+    s = Solver(m)
+    s.run(60)
+    s.sync()
+    assert np.abs(oh[:, 0]).max() > 1e-3
+    for f in range(5):
+        g = s.history(f)
+        assert np.linalg.norm(g - oh[:, f]) <= tol * max(np.linalg.norm(oh[:, f]), 1e-30), f
+    s.close()
