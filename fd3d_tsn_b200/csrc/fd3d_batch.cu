@@ -384,6 +384,9 @@ struct Model {
     int steps = 0;      // steps done
     int nf = 4;
     int cap = 0;
+    // this model's work items per phase, for the interior tile depth items_kchunk
+    std::vector<Work> items[NPHASE];
+    int items_kchunk = -1;
 };
 
 enum { MODE_PERSISTENT = FD3D_BATCH_PERSISTENT, MODE_GRAPH = FD3D_BATCH_GRAPH };
@@ -436,60 +439,118 @@ struct fd3d_batch {
     int** d_stptr = nullptr;     // status words of the live models (k_or_status)
     int n_stptr = 0;
     int* d_status_or = nullptr;
+    Work* h_stage = nullptr;     // page-locked staging of the work lists
+    size_t stage_cap = 0;
+    bool work_t_ok = false;      // the type-sorted list matches the work list
 };
 
 namespace {
 
-int build_work(fd3d_batch* b) {
-    b->work.clear();
-    std::vector<std::vector<Work>> per(NPHASE);
-    const int kch = b->tun.kchunk;
-    for (size_t m = 0; m < b->models.size(); ++m) {
-        const Model& M = b->models[m];
-        if (!M.live) continue;
-        const fd3d_params& p = M.p;
-        const Grid& g = M.dev.g;
-        const int tm = (int)m << 8;
-        const int nxT = p.nxt - 2 * p.nabc, nyI = p.nyt - 2 - p.nabc, nzT = g.ks() - p.nabc;
-        const int kc = std::max(1, std::min(kch, nzT));
-        const int gx = (nxT + 31) / 32, gy = (nyI + 7) / 8, gz = (nzT + kc - 1) / kc;
-        for (int z = 0; z < gz; ++z)
-            for (int y = 0; y < gy; ++y)
-                for (int x = 0; x < gx; ++x) {
-                    per[0].push_back(Work{tm | W_VEL_INT, x, y, z});
-                    per[2].push_back(Work{tm | W_STR_INT, x, y, z});
-                }
-        const int fx = (std::max(nxT, p.nxt) + 31) / 32, fz = (nzT + 7) / 8;
-        for (int y = 0; y < fz; ++y)
-            for (int x = 0; x < fx; ++x) per[0].push_back(Work{tm | W_VEL_FAULT, x, y, 0});
-        const int npml = (int)((M.dev.D.cum[PML_MAXS] + 255) / 256);
-        for (int x = 0; x < npml; ++x) {
-            per[0].push_back(Work{tm | W_VEL_PML, x, 0, 0});
-            per[2].push_back(Work{tm | W_STR_PML, x, 0, 0});
-        }
-        const int sx = (p.nxt + 31) / 32, sy = p.fspace ? 0 : (p.nyt + 7) / 8;  // no fuvw/fres under FSPACE
-        for (int y = 0; y < sy; ++y)
-            for (int x = 0; x < sx; ++x) {
-                per[1].push_back(Work{tm | W_VEL_FS, x, y, 0});
-                per[3].push_back(Work{tm | W_STR_FS, x, y, 0});
+// the work items of model m for interior tile depth kch, per phase
+void build_model_items(Model& M, int m, int kch) {
+    std::vector<Work>* per = M.items;
+    for (int ph = 0; ph < NPHASE; ++ph) per[ph].clear();
+    const fd3d_params& p = M.p;
+    const Grid& g = M.dev.g;
+    const int tm = m << 8;
+    const int nxT = p.nxt - 2 * p.nabc, nyI = p.nyt - 2 - p.nabc, nzT = g.ks() - p.nabc;
+    const int kc = std::max(1, std::min(kch, nzT));
+    const int gx = (nxT + 31) / 32, gy = (nyI + 7) / 8, gz = (nzT + kc - 1) / kc;
+    for (int z = 0; z < gz; ++z)
+        for (int y = 0; y < gy; ++y)
+            for (int x = 0; x < gx; ++x) {
+                per[0].push_back(Work{tm | W_VEL_INT, x, y, z});
+                per[2].push_back(Work{tm | W_STR_INT, x, y, z});
             }
-        const int px = (nxT + 31) / 32;
-        for (int y = 0; y < fz; ++y)
-            for (int x = 0; x < px; ++x) {
-                per[2].push_back(Work{tm | W_STR_FAULT, x, y, 0});
-                per[4].push_back(Work{tm | W_TRAC, x, y, 0});
-                per[5].push_back(Work{tm | W_FRIC, x, y, 0});
-                per[6].push_back(Work{tm | W_OUT, x, y, 0});
-            }
-        if (M.p.law == FD3D_LAW_FVW && M.dev.fs.nucleation) {
-            const int ni = (p.nxt - p.nabc) - (p.nabc - 1) + 1, nk = g.ks() - (p.nabc - 1) + 1;
-            for (int y = 0; y < (nk + 7) / 8; ++y)
-                for (int x = 0; x < (ni + 31) / 32; ++x) per[6].push_back(Work{tm | W_NUC, x, y, 0});
-        }
+    const int fx = (std::max(nxT, p.nxt) + 31) / 32, fz = (nzT + 7) / 8;
+    for (int y = 0; y < fz; ++y)
+        for (int x = 0; x < fx; ++x) per[0].push_back(Work{tm | W_VEL_FAULT, x, y, 0});
+    const int npml = (int)((M.dev.D.cum[PML_MAXS] + 255) / 256);
+    for (int x = 0; x < npml; ++x) {
+        per[0].push_back(Work{tm | W_VEL_PML, x, 0, 0});
+        per[2].push_back(Work{tm | W_STR_PML, x, 0, 0});
     }
+    const int sx = (p.nxt + 31) / 32, sy = p.fspace ? 0 : (p.nyt + 7) / 8;  // no fuvw/fres under FSPACE
+    for (int y = 0; y < sy; ++y)
+        for (int x = 0; x < sx; ++x) {
+            per[1].push_back(Work{tm | W_VEL_FS, x, y, 0});
+            per[3].push_back(Work{tm | W_STR_FS, x, y, 0});
+        }
+    const int px = (nxT + 31) / 32;
+    for (int y = 0; y < fz; ++y)
+        for (int x = 0; x < px; ++x) {
+            per[2].push_back(Work{tm | W_STR_FAULT, x, y, 0});
+            per[4].push_back(Work{tm | W_TRAC, x, y, 0});
+            per[5].push_back(Work{tm | W_FRIC, x, y, 0});
+            per[6].push_back(Work{tm | W_OUT, x, y, 0});
+        }
+    if (M.p.law == FD3D_LAW_FVW && M.dev.fs.nucleation) {
+        const int ni = (p.nxt - p.nabc) - (p.nabc - 1) + 1, nk = g.ks() - (p.nabc - 1) + 1;
+        for (int y = 0; y < (nk + 7) / 8; ++y)
+            for (int x = 0; x < (ni + 31) / 32; ++x) per[6].push_back(Work{tm | W_NUC, x, y, 0});
+    }
+    M.items_kchunk = kch;
+}
+
+// page-locked staging of n items (grown by half again when short)
+int stage_items(fd3d_batch* b, size_t n) {
+    if (n <= b->stage_cap) return FD3D_OK;
+    if (b->h_stage) cudaFreeHost(b->h_stage);
+    b->h_stage = nullptr;
+    b->stage_cap = n + n / 2 + 1024;
+    BCK(cudaHostAlloc((void**)&b->h_stage, b->stage_cap * sizeof(Work), cudaHostAllocDefault));
+    return FD3D_OK;
+}
+
+// The items of the live models grouped by type, for the graph schedule (built when a
+// graph run needs them after the work list changed)
+int build_work_t(fd3d_batch* b) {
+    std::vector<std::vector<Work>> byt(NTYPES);
+    for (const Work& w : b->work) byt[w.tm & 255].push_back(w);
+    b->work_t.clear();
+    for (int t = 0; t < NTYPES; ++t) {
+        b->tbeg[t] = (int)b->work_t.size();
+        b->work_t.insert(b->work_t.end(), byt[t].begin(), byt[t].end());
+    }
+    b->tbeg[NTYPES] = (int)b->work_t.size();
+    if (b->work_t.size() > b->work_t_cap) {
+        if (b->d_work_t) cudaFree(b->d_work_t);
+        b->work_t_cap = b->work_t.size() + b->work_t.size() / 2 + 64;
+        BCK(cudaMalloc(&b->d_work_t, b->work_t_cap * sizeof(Work)));
+    }
+    if (!b->work_t.empty()) {
+        if (stage_items(b, b->work_t.size())) return FD3D_ERR_CUDA;
+        std::memcpy(b->h_stage, b->work_t.data(), b->work_t.size() * sizeof(Work));
+        BCK(cudaMemcpyAsync(b->d_work_t, b->h_stage, b->work_t.size() * sizeof(Work), cudaMemcpyHostToDevice, b->st));
+    }
+    for (cudaGraphExec_t& g : b->gx)
+        if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+    BCK(cudaStreamSynchronize(b->st));  // the staging buffer is reused by the next build
+    b->work_t_ok = true;
+    return FD3D_OK;
+}
+
+// The work list of the live models, phase by phase: each model's items are built once
+// (and again when the tile depth changes), so a change of the resident set only
+// concatenates them.
+int build_work(fd3d_batch* b) {
+    const int kch = b->tun.kchunk;
+    size_t n = 0;
+    for (size_t m = 0; m < b->models.size(); ++m) {
+        Model& M = b->models[m];
+        if (!M.live) continue;
+        if (M.items_kchunk != kch) build_model_items(M, (int)m, kch);
+        for (int ph = 0; ph < NPHASE; ++ph) n += M.items[ph].size();
+    }
+    b->work.resize(n);
+    size_t at = 0;
     for (int ph = 0; ph < NPHASE; ++ph) {
-        b->pbeg[ph] = (int)b->work.size();
-        b->work.insert(b->work.end(), per[ph].begin(), per[ph].end());
+        b->pbeg[ph] = (int)at;
+        for (const Model& M : b->models)
+            if (M.live && !M.items[ph].empty()) {
+                std::memcpy(b->work.data() + at, M.items[ph].data(), M.items[ph].size() * sizeof(Work));
+                at += M.items[ph].size();
+            }
     }
     {   // status words of the live models
         std::vector<int*> sp;
@@ -499,36 +560,24 @@ int build_work(fd3d_batch* b) {
         if (!sp.empty())
             BCK(cudaMemcpyAsync(b->d_stptr, sp.data(), sp.size() * sizeof(int*), cudaMemcpyHostToDevice, b->st));
     }
-    {   // the same items grouped by type for the graph schedule
-        std::vector<std::vector<Work>> byt(NTYPES);
-        for (const Work& w : b->work) byt[w.tm & 255].push_back(w);
-        b->work_t.clear();
-        for (int t = 0; t < NTYPES; ++t) {
-            b->tbeg[t] = (int)b->work_t.size();
-            b->work_t.insert(b->work_t.end(), byt[t].begin(), byt[t].end());
-        }
-        b->tbeg[NTYPES] = (int)b->work_t.size();
-        if (b->work_t.size() > b->work_t_cap) {
-            if (b->d_work_t) cudaFree(b->d_work_t);
-            b->work_t_cap = b->work_t.size() + b->work_t.size() / 2 + 64;
-            BCK(cudaMalloc(&b->d_work_t, b->work_t_cap * sizeof(Work)));
-        }
-        if (!b->work_t.empty())
-            BCK(cudaMemcpyAsync(b->d_work_t, b->work_t.data(), b->work_t.size() * sizeof(Work),
-                                cudaMemcpyHostToDevice, b->st));
-        for (cudaGraphExec_t& g : b->gx)
-            if (g) { cudaGraphExecDestroy(g); g = nullptr; }
-    }
+    b->work_t_ok = false;
     b->pbeg[NPHASE] = (int)b->work.size();
     if (b->work.size() > b->work_cap) {
         if (b->d_work) cudaFree(b->d_work);
         b->work_cap = b->work.size() + b->work.size() / 2 + 64;
         BCK(cudaMalloc(&b->d_work, b->work_cap * sizeof(Work)));
     }
-    if (!b->work.empty())
-        BCK(cudaMemcpyAsync(b->d_work, b->work.data(), b->work.size() * sizeof(Work), cudaMemcpyHostToDevice, b->st));
+    if (!b->work.empty()) {
+        if (stage_items(b, b->work.size())) return FD3D_ERR_CUDA;
+        std::memcpy(b->h_stage, b->work.data(), b->work.size() * sizeof(Work));
+        BCK(cudaMemcpyAsync(b->d_work, b->h_stage, b->work.size() * sizeof(Work), cudaMemcpyHostToDevice, b->st));
+    }
     BCK(cudaMemcpyAsync(b->d_pbeg, b->pbeg, sizeof(b->pbeg), cudaMemcpyHostToDevice, b->st));
     BCK(cudaStreamSynchronize(b->st));
+    if (b->tun.mode == MODE_GRAPH) {
+        int rc = build_work_t(b);
+        if (rc) return rc;
+    }
     b->dirty = false;
     b->built_kchunk = b->tun.kchunk;
     return FD3D_OK;
@@ -607,6 +656,10 @@ int get_batch_graph(fd3d_batch* b, int g, cudaGraphExec_t* out) {
 }
 
 int launch_graphs(fd3d_batch* b, int nsteps) {
+    if (!b->work_t_ok) {
+        int rc = build_work_t(b);
+        if (rc) return rc;
+    }
     BCK(cudaMemsetAsync(b->d_run_step, 0, sizeof(int), b->st));
     int left = nsteps;
     for (int g = 0; g < fd3d_batch::NGRAPH && left > 0; ++g) {
@@ -763,6 +816,7 @@ int fd3d_batch_destroy(fd3d_batch* b) {
     cudaFree(b->d_status);
     cudaFree(b->d_work);
     cudaFree(b->d_work_t);
+    if (b->h_stage) cudaFreeHost(b->h_stage);
     cudaFree(b->d_run_step);
     cudaFree(b->d_stptr);
     cudaFree(b->d_status_or);
