@@ -135,7 +135,7 @@ def sw_fault(m, rng, patch, sn=120e6, mus=0.68, mud=0.52, dc=0.4, t0_mean=70e6, 
 
 
 def sw_model(nxT, nyT, nzT, h, sim_time, seed, layers=None, patch_nodes=None, nstations=4, corr_m=2000.0,
-             dc_patch_m=None, dc_range=None, history_stride=1, precision="f32", ntfd=None, fspace=False):
+             dc_patch_m=None, dc_range=None, history_stride=1, precision="f32", ntfd=None, fspace=False, nabc=NABC):
     rng = np.random.default_rng(seed)
     if layers is None:
         layers = dict(depth=[0.0], vp=[6000.0], vs=[3464.0], rho=[2670.0])
@@ -143,7 +143,7 @@ def sw_model(nxT, nyT, nzT, h, sim_time, seed, layers=None, patch_nodes=None, ns
     vpmax = max(layers["vp"])
     dt = 0.25 * h / vpmax * (1.0 - 1e-6)  # strict CFL check of fd3d_init.f90:274-278
     nsteps = int(round(sim_time / dt)) if ntfd is None else ntfd
-    m = _grid(nxT, nyT, nzT, h, dt, nsteps, fspace=fspace)
+    m = _grid(nxT, nyT, nzT, h, dt, nsteps, nabc=nabc, fspace=fspace)
     lam, mu, d, vpm = crustal_medium(m["nzt"], h, dip, layers["depth"], layers["vp"], layers["vs"], layers["rho"],
                                      nfs=m["nfs"])
     m.update(medium=(lam, mu, d), vp_max=vpm, law="sw", precision=precision, history_stride=history_stride)
@@ -301,10 +301,10 @@ def fspace_variant(m: dict) -> dict:
 
 
 def tiny_sw(seed=5, nxT=40, nyT=14, nzT=28, h=200.0, nsteps=60, precision="f32", nstations=3, stride=1,
-            fspace=False, layers=None):
+            fspace=False, layers=None, nabc=NABC):
     """Parity-test model: rupture starts on step 1 from an overstressed nucleation patch."""
     return sw_model(nxT, nyT, nzT, h, 1.0, seed, layers=layers, patch_nodes=(nxT - 8, nzT - 8), nstations=nstations,
-                    precision=precision, ntfd=nsteps, history_stride=stride, corr_m=600.0, fspace=fspace)
+                    precision=precision, ntfd=nsteps, history_stride=stride, corr_m=600.0, fspace=fspace, nabc=nabc)
 
 
 def tiny_fvw(seed=6, nxT=40, nyT=14, nzT=28, h=200.0, nsteps=60, precision="f32", stride=1, fspace=False):
