@@ -147,3 +147,22 @@ def test_top_boundary_energy(fspace):
         assert top > 1e-3  # the top strip carries the wave field it absorbs
     else:
         assert top == 0.0  # fuvw sets u on the first ghost row only
+
+
+def test_symmetric_setup_gives_symmetric_rupture():
+    """A homogeneous model with uniform prestress and friction and a nucleation square
+    centred in x ruptures symmetrically: the rupture times on the Z nodes mirror exactly
+    about the centre of the interior plane."""
+    m = configs.tiny_sw(nsteps=120, nxT=40, nzT=28)
+    f = m["fault"]
+    nab, nxt, nzt = m["nabc"], m["nxt"], m["nzt"]
+    T = np.full((nxt, nzt), 70e6)
+    T[nab + 16:nab + 24, nab + 10:nab + 18] = 0.68 * 120e6 * 1.02   # nodes nab+17..nab+24 in x
+    plane = lambda v: np.asfortranarray(np.full((nxt, nzt), v))
+    f.update(striniX=np.asfortranarray(T), peak_xz=plane(0.68 * 120e6), dyn_xz=plane(0.52 * 120e6), Dc=plane(0.4),
+             coh=plane(0.0))
+    o = Oracle(m, F64)
+    o.step(120)
+    rt = o.final()["ruptime"][nab:nxt - nab, nab:nzt - m["nfs"]]
+    assert (rt < 1e4).sum() > 100
+    np.testing.assert_array_equal(rt, rt[::-1, :])
