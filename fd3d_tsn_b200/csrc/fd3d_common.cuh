@@ -8,7 +8,7 @@
 //     128-byte boundary (fp32) and px (a multiple of 32) keeps every row aligned.
 //   * fault-plane arrays (i,k) at (i-1) + nxt*(k-1), the reference's own layout.
 //   * PML auxiliary (split) components of init_pml (src/fd3d_deriv.f90:1319-1410): one
-//     pool indexed by the compact cell index of the 4 strips, in 32-cell blocks per
+//     pool indexed by the compact cell index of the strips (4, or 5 under FSPACE), in 32-cell blocks per
 //     group of components (PmlAux, fd3d_kernels.cuh).
 #pragma once
 #include <cmath>

@@ -6,7 +6,7 @@
 //   1 vel_interior  uxx1/vyy1/wzz1 (fd3d_deriv.f90:50-193)
 //   2 vel_fault     uxx0a/vyy0a/wzz0a at j=nyt-1 + v mirror (fd3d_deriv.f90:198-508),
 //                   tasu1/tasw1 at j=nyt (fd3d_deriv.f90:1109-1234)
-//   3 vel_pml       pml_uvw, 4 strips (fd3d_deriv.f90:1927-2299)
+//   3 vel_pml       pml_uvw, 4 strips, 5 under FSPACE (fd3d_deriv.f90:1927-2299)
 //   4 vel_fs        fuvw (fd3d_deriv.f90:1018-1062)
 //   5 str_interior  dstres (fd3d_deriv.f90:513-622)
 //   6 str_fault     sxx/sxy0/sxz0/syz0 at j=nyt-1 + xy/yz mirror, sxz1, tasii
@@ -249,7 +249,7 @@ __device__ __forceinline__ bool pml_tile_wait(uint32_t bar, uint32_t parity, int
     }
     return true;
 }
-// pml_uvw: split-field PML velocity in the 4 strips (fd3d_deriv.f90:1927-2218), one
+// pml_uvw: split-field PML velocity in the strips (fd3d_deriv.f90:1927-2293), one
 // tile of PML_TILE consecutive cells per CTA of PML_TILE threads.  Returns false if the
 // staging copy timed out.
 template <class T>
@@ -442,7 +442,7 @@ __device__ __forceinline__ void str_fault_body(Grid g, Fields<T> f, Fault<T> q, 
     }
 }
 
-// pml_xyz in the 4 strips (fd3d_deriv.f90:2304-2992), one tile per CTA as vel_pml_tile
+// pml_xyz in the strips (fd3d_deriv.f90:2304-3143), one tile per CTA as vel_pml_tile
 template <class T>
 __device__ __forceinline__ bool str_pml_tile(const Grid& g, const Fields<T>& f, const PmlDesc& D, const PmlAux<T>& X,
                                              const StepConst<T>& c, int tile, T* sm, uint32_t bar, uint32_t parity,
