@@ -304,3 +304,38 @@ def test_history_read_while_next_run_is_queued():
     np.testing.assert_array_equal(np.concatenate([first, second, third]), oh[:, :4])
     np.testing.assert_array_equal(st, os_[:20])
     s.close()
+
+
+def test_medium_upload_paths_agree():
+    """fd3d_upload_medium stages the host arrays in the still-zero wave field (before the
+    first step) or copies them row by row into the padded arrays (after steps, when the wave
+    field is live): FP32 and FP64 host arrays, before and after steps, give the same run."""
+    m = configs.tiny_sw(seed=17, nxT=37, nyT=13, nzT=25, nsteps=30)
+    lam, mu, d = configs.medium_3d(m)
+    rng = np.random.default_rng(8)
+    arrs = [np.asfortranarray((a * (1.0 + 0.05 * rng.uniform(-1.0, 1.0, a.shape))).astype(np.float32))
+            for a in (lam, mu, d)]
+    runs = []
+    for rk in (4, 8):
+        s = Solver(m)
+        s.upload_medium_arrays(*(a if rk == 4 else a.astype(np.float64) for a in arrs), real_kind=rk)
+        s.run(30)
+        s.sync()
+        runs.append((s.history(0), s.field("xz")))
+        s.close()
+    s = Solver(m)                      # medium replaced mid-run with the same values
+    s.upload_medium_arrays(*arrs, real_kind=4)
+    s.run(10)
+    s.sync()
+    s.upload_medium_arrays(*arrs, real_kind=4)
+    s.run(20)
+    s.sync()
+    runs.append((s.history(0), s.field("xz")))
+    s.close()
+    for h, xz in runs[1:]:
+        np.testing.assert_array_equal(h, runs[0][0])
+        np.testing.assert_array_equal(xz, runs[0][1])
+    o = Oracle(m, MIXED)
+    o.set_medium_arrays(*(a.astype(np.float64) for a in arrs))
+    oh, _ = o.step(30)
+    np.testing.assert_array_equal(runs[0][0], oh[:, 0])
