@@ -193,6 +193,23 @@ k_batch(const ModelDev* __restrict__ models, const ModelMaps* __restrict__ maps,
     }
 }
 
+// ---------------------------------------------------------------- self-test of the waits
+// An mbarrier phase that no copy or arrival completes, and a grid barrier that one CTA
+// never reaches: both waits must give up by their bound, record ST_TIMEOUT and return,
+// leaving the context usable (failure detection without a hung or faulted GPU).
+__global__ void k_check_mbar_wait(int* status) {
+    __shared__ __align__(8) uint64_t bar;
+    if (threadIdx.x == 0) { mbar_init(smem_addr(&bar), 1); fence_mbar_init(); }
+    __syncthreads();
+    const bool done = mbar_wait(smem_addr(&bar), 0u);  // nothing ever arrives on this phase
+    if (__syncthreads_or(!done) && threadIdx.x == 0) atomicOr(status, ST_TIMEOUT);
+}
+
+__global__ void k_check_grid_barrier(BatchSync* sync, int* status) {
+    if (blockIdx.x == gridDim.x - 1) return;  // this CTA never arrives
+    grid_barrier(sync, gridDim.x, status);
+}
+
 // ---------------------------------------------------------------- graph schedule
 // The same items as k_batch, one kernel per region and step, every CTA one item.
 // A CUDA graph holds a chunk of steps: per step the interior, fault-band and PML
@@ -744,6 +761,31 @@ int reset_model(fd3d_batch* b, Model& M, cudaStream_t st) {
 }  // namespace
 
 extern "C" {
+
+int fd3d_check_waits(int* mbar_status, int* barrier_status) {
+    if (!mbar_status || !barrier_status) return FD3D_ERR_ARG;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) { cudaGetLastError(); return FD3D_ERR_NODEV; }
+    int* st = nullptr;
+    BatchSync* sync = nullptr;
+    if (cudaMalloc(&st, 2 * sizeof(int)) != cudaSuccess) return FD3D_ERR_NOMEM;
+    if (cudaMalloc(&sync, sizeof(BatchSync)) != cudaSuccess) { cudaFree(st); return FD3D_ERR_NOMEM; }
+    int rc = FD3D_OK, h[2] = {0, 0};
+    if (cudaMemset(st, 0, 2 * sizeof(int)) != cudaSuccess || cudaMemset(sync, 0, sizeof(BatchSync)) != cudaSuccess)
+        rc = FD3D_ERR_CUDA;
+    if (rc == FD3D_OK) {
+        k_check_mbar_wait<<<1, 64>>>(st);
+        k_check_grid_barrier<<<2, 64>>>(sync, st + 1);
+        if (cudaGetLastError() != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess ||
+            cudaMemcpy(h, st, sizeof(h), cudaMemcpyDeviceToHost) != cudaSuccess)
+            rc = FD3D_ERR_CUDA;
+    }
+    cudaFree(st);
+    cudaFree(sync);
+    *mbar_status = h[0];
+    *barrier_status = h[1];
+    return rc;
+}
 
 int fd3d_batch_create(size_t arena_bytes, int max_models, fd3d_batch** out) {
     if (!out || max_models < 1 || arena_bytes < (1u << 20)) return FD3D_ERR_ARG;

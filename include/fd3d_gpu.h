@@ -274,6 +274,12 @@ int fd3d_batch_autotune(fd3d_batch* b, int steps, const char* cache_path, const 
  * of dividends whose quotients differ (0 expected) and the first such bit pattern
  * (0xffffffff if none). */
 int fd3d_check_division(const float* divisors, int n, unsigned long long* mismatches, unsigned* first_bad);
+/* Self-test of the bounded device waits (no counterpart in the reference, whose GPU
+ * regions never wait on each other): a kernel waits on an mbarrier phase that nothing
+ * completes and a grid barrier that one CTA never reaches.  Both waits must give up after
+ * their bound and record the timeout bit (4) in the status word returned here; the device
+ * stays usable.  Takes about a second. */
+int fd3d_check_waits(int* mbar_status, int* barrier_status);
 
 /* ---- input decks (the reference's own files) --------------------------- */
 /* Reads inputfd3d.dat and crustal.dat from dir (fd3d_init.f90:145-173, 211-279),
