@@ -151,6 +151,8 @@ def load_library(path: str | None = None) -> C.CDLL:
         "fd3d_free": (None, [vp]),
         "fd3d_check_division": (i, [fp, i, C.POINTER(C.c_ulonglong), C.POINTER(C.c_uint)]),
         "fd3d_check_waits": (i, [C.POINTER(i), C.POINTER(i)]),
+        "fd3d_checkpoint": (i, [vp, C.c_char_p]),
+        "fd3d_restore": (i, [C.c_char_p, C.POINTER(vp)]),
         "fd3d_fetch_moment_rate": (i, [vp, i, i, dp]),
         "fd3d_post_process": (i, [vp, dp]),
         "fd3d_upload_fault_model": (i, [vp, i, i, dp, dp, dp, C.c_double, i]),

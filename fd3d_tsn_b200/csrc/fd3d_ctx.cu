@@ -175,6 +175,8 @@ struct CtxBase {
     virtual int moment_rate(int rec0, int nrec, double* host) = 0;
     virtual int post(double* out4) = 0;
     virtual size_t elem() const = 0;
+    virtual int save_state(std::FILE* fp) = 0;
+    virtual int load_state(std::FILE* fp) = 0;
 };
 
 template <class T>
@@ -491,6 +493,61 @@ struct Ctx : CtxBase {
         return reset_state(false);
     }
 
+    // Checkpoint: the whole device state of the context is its one allocation (wave field,
+    // medium, PML split components, fault planes, step counter, history and station rings),
+    // written as it lies, after the host-side state a run depends on.
+    struct SavedHost {
+        unsigned long long block_bytes;
+        int steps_done, rec_written, medium_ok, fault_ok, layered;
+        FvwScalars fs;
+        unsigned long long npsi;
+    };
+    static constexpr size_t CKPT_CHUNK = 64ull << 20;
+    int save_state(std::FILE* fp) override {
+        if (!allocs.empty()) return FD3D_ERR_STATE;  // state outside the block: not restorable
+        CK(cudaStreamSynchronize(st));
+        SavedHost h{};
+        h.block_bytes = block_bytes; h.steps_done = steps_done; h.rec_written = rec_written;
+        h.medium_ok = medium_ok; h.fault_ok = fault_ok; h.layered = f.lay != nullptr; h.fs = fs;
+        h.npsi = psiZ0.size();
+        if (std::fwrite(&h, sizeof h, 1, fp) != 1) return FD3D_ERR_IO;
+        if (h.npsi && (std::fwrite(psiZ0.data(), sizeof(double), h.npsi, fp) != h.npsi ||
+                       std::fwrite(psiX0.data(), sizeof(double), h.npsi, fp) != h.npsi))
+            return FD3D_ERR_IO;
+        std::vector<char> buf(std::min(CKPT_CHUNK, block_bytes));
+        for (size_t off = 0; off < block_bytes; off += buf.size()) {
+            const size_t n = std::min(buf.size(), block_bytes - off);
+            CK(cudaMemcpy(buf.data(), block + off, n, cudaMemcpyDeviceToHost));
+            if (std::fwrite(buf.data(), 1, n, fp) != n) return FD3D_ERR_IO;
+        }
+        return FD3D_OK;
+    }
+    int load_state(std::FILE* fp) override {
+        SavedHost h{};
+        if (std::fread(&h, sizeof h, 1, fp) != 1) return FD3D_ERR_IO;
+        if (h.block_bytes != block_bytes || !allocs.empty()) return FD3D_ERR_ARG;  // another layout
+        std::vector<double> pz(h.npsi), px(h.npsi);
+        if (h.npsi && (std::fread(pz.data(), sizeof(double), h.npsi, fp) != h.npsi ||
+                       std::fread(px.data(), sizeof(double), h.npsi, fp) != h.npsi))
+            return FD3D_ERR_IO;
+        CK(cudaStreamSynchronize(st));
+        std::vector<char> buf(std::min(CKPT_CHUNK, block_bytes));
+        for (size_t off = 0; off < block_bytes; off += buf.size()) {
+            const size_t n = std::min(buf.size(), block_bytes - off);
+            if (std::fread(buf.data(), 1, n, fp) != n) return FD3D_ERR_IO;
+            CK(cudaMemcpy(block + off, buf.data(), n, cudaMemcpyHostToDevice));
+        }
+        steps_done = h.steps_done; rec_written = h.rec_written;
+        medium_ok = h.medium_ok != 0; fault_ok = h.fault_ok != 0;
+        f.lay = h.layered ? dlay : nullptr;
+        fs = h.fs;
+        psiZ0 = std::move(pz); psiX0 = std::move(px);
+        for (cudaGraphExec_t& gx : gexec)
+            if (gx) { cudaGraphExecDestroy(gx); gx = nullptr; }
+        nmark = 0;
+        return FD3D_OK;
+    }
+
     // zeroing of fd3d_theo.f90:59-88 and of the PML aux (fd3d_deriv.f90:1342-1410)
     int reset_state(bool keep_psi) {
         (void)keep_psi;
@@ -761,6 +818,44 @@ int fd3d_ctx_destroy(fd3d_ctx* ctx) {
     delete ctx->impl;
     delete ctx;
     return FD3D_OK;
+}
+
+// file layout: magic, sizeof(fd3d_params), the parameters, then the context's state
+static const char CKPT_MAGIC[8] = {'F', 'D', '3', 'D', 'C', 'K', 'P', '1'};
+
+int fd3d_checkpoint(fd3d_ctx* ctx, const char* path) {
+    if (!ctx || !path) return FD3D_ERR_ARG;
+    CtxBase* c = ctx->impl;
+    std::FILE* fp = std::fopen(path, "wb");
+    if (!fp) return FD3D_ERR_IO;
+    const unsigned psz = sizeof(fd3d_params);
+    int rc = (std::fwrite(CKPT_MAGIC, 1, 8, fp) == 8 && std::fwrite(&psz, sizeof psz, 1, fp) == 1 &&
+              std::fwrite(&c->p, sizeof(fd3d_params), 1, fp) == 1)
+                 ? c->save_state(fp) : FD3D_ERR_IO;
+    if (std::fclose(fp) != 0 && rc == FD3D_OK) rc = FD3D_ERR_IO;
+    return rc;
+}
+
+int fd3d_restore(const char* path, fd3d_ctx** out) {
+    if (!path || !out) return FD3D_ERR_ARG;
+    *out = nullptr;
+    std::FILE* fp = std::fopen(path, "rb");
+    if (!fp) return FD3D_ERR_IO;
+    char magic[8];
+    unsigned psz = 0;
+    fd3d_params p{};
+    int rc = FD3D_OK;
+    if (std::fread(magic, 1, 8, fp) != 8 || std::memcmp(magic, CKPT_MAGIC, 8) != 0 ||
+        std::fread(&psz, sizeof psz, 1, fp) != 1 || psz != sizeof(fd3d_params) ||
+        std::fread(&p, sizeof p, 1, fp) != 1)
+        rc = FD3D_ERR_IO;
+    if (rc == FD3D_OK) rc = fd3d_ctx_create(&p, out);
+    if (rc == FD3D_OK) {
+        rc = (*out)->impl->load_state(fp);
+        if (rc != FD3D_OK) { fd3d_ctx_destroy(*out); *out = nullptr; }
+    }
+    std::fclose(fp);
+    return rc;
 }
 
 int fd3d_upload_medium(fd3d_ctx* ctx, const void* l, const void* m, const void* d, int rk) {

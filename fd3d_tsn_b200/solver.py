@@ -84,6 +84,25 @@ class Solver:
         _ck(lib().fd3d_upload_fault_model(self.h, nli, nwi, *(a.ctypes.data_as(dp) for a in arrs), float(dip),
                                           int(dipslip)), "fd3d_upload_fault_model")
 
+    # ------------------------------------------------------------ checkpoint / resume
+    def checkpoint(self, path: str):
+        """Write the whole state of the run to one file (waits for the enqueued steps)."""
+        _ck(lib().fd3d_checkpoint(self.h, path.encode()), "fd3d_checkpoint")
+
+    @classmethod
+    def restore(cls, path: str, model: dict) -> "Solver":
+        """A solver resuming the run saved in path; model is the model that run was made
+        from (its sizes and law; the medium and fault come from the file)."""
+        self = cls.__new__(cls)
+        self.model = model
+        self.p = abi.make_params(model)
+        self.h = C.c_void_p()
+        _ck(lib().fd3d_restore(path.encode(), C.byref(self.h)), "fd3d_restore")
+        self.nxT = model["nxt"] - 2 * model["nabc"]
+        self.nzT = model["nzt"] - model["nfs"] - model["nabc"]
+        self.nf = 5 if model.get("law", "sw") == "fvw" else 4
+        return self
+
     # ------------------------------------------------------------ time loop
     def reset(self):
         _ck(lib().fd3d_reset(self.h), "fd3d_reset")

@@ -178,6 +178,15 @@ int fd3d_upload_fault(fd3d_ctx* ctx, const fd3d_fault* f);
 int fd3d_upload_fault_model(fd3d_ctx* ctx, int nli, int nwi, const double* T0I, const double* TsI,
                             const double* DcI, double dip, int dipslip);
 int fd3d_reset(fd3d_ctx* ctx);                      /* zero wave field, PML and fault state (fd3d_theo.f90:59-88) */
+/* Checkpoint and resume (the reference has no restart files; its state lives in module
+ * arrays for one run).  fd3d_checkpoint waits for the enqueued steps and writes the
+ * context's whole state -- parameters, wave field, medium, PML split components, fault
+ * planes, step counter and the history/station rings -- to one file (about the context's
+ * device memory in size).  fd3d_restore creates a context on the current device from such
+ * a file; fd3d_run on it continues the run bit for bit.  FD3D_ERR_IO on a file that is not
+ * a checkpoint of this library's layout. */
+int fd3d_checkpoint(fd3d_ctx* ctx, const char* path);
+int fd3d_restore(const char* path, fd3d_ctx** out);
 int fd3d_run(fd3d_ctx* ctx, int nsteps);            /* enqueue nsteps time steps; asynchronous */
 int fd3d_sync(fd3d_ctx* ctx);                       /* wait; returns first device error        */
 /* No counterpart in the reference.  Same time steps as fd3d_run, for hosts that cannot
