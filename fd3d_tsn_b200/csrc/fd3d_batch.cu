@@ -34,6 +34,7 @@
 #include "fd3d_kernels.cuh"
 #include "fd3d_opt.cuh"
 #include "fd3d_setup.h"
+#include "fd3d_trace.h"
 
 using namespace fd3d;
 
@@ -1014,6 +1015,7 @@ int fd3d_batch_reset(fd3d_batch* b, int slot) {
 }
 
 int fd3d_batch_run(fd3d_batch* b, int nsteps) {
+    fd3d::TraceRange trace_("fd3d_batch_run");
     if (!b || nsteps < 0) return FD3D_ERR_ARG;
     std::lock_guard<std::mutex> lk(b->mu);
     if (b->dirty || b->built_kchunk != b->tun.kchunk) {
@@ -1192,6 +1194,7 @@ int fd3d_batch_get_tuning(fd3d_batch* b, int* kchunk, int* ctas_per_sm, int* max
 // records the choice under `key` in the JSON-lines cache file (if given).  A cache
 // hit skips the timing.
 int fd3d_batch_autotune(fd3d_batch* b, int steps, const char* cache_path, const char* key) {
+    fd3d::TraceRange trace_("fd3d_batch_autotune");
     if (!b || steps < 1) return FD3D_ERR_ARG;
     for (const Model& M : b->models)
         if (M.live && M.steps != 0) return FD3D_ERR_STATE;

@@ -18,6 +18,7 @@
 #include "fd3d_post.cuh"
 #include "fd3d_setup.h"
 #include "fd3d_host.h"
+#include "fd3d_trace.h"
 
 using namespace fd3d;
 
@@ -824,6 +825,7 @@ int fd3d_ctx_destroy(fd3d_ctx* ctx) {
 static const char CKPT_MAGIC[8] = {'F', 'D', '3', 'D', 'C', 'K', 'P', '1'};
 
 int fd3d_checkpoint(fd3d_ctx* ctx, const char* path) {
+    fd3d::TraceRange trace_("fd3d_checkpoint");
     if (!ctx || !path) return FD3D_ERR_ARG;
     CtxBase* c = ctx->impl;
     std::FILE* fp = std::fopen(path, "wb");
@@ -837,6 +839,7 @@ int fd3d_checkpoint(fd3d_ctx* ctx, const char* path) {
 }
 
 int fd3d_restore(const char* path, fd3d_ctx** out) {
+    fd3d::TraceRange trace_("fd3d_restore");
     if (!path || !out) return FD3D_ERR_ARG;
     *out = nullptr;
     std::FILE* fp = std::fopen(path, "rb");
@@ -859,16 +862,19 @@ int fd3d_restore(const char* path, fd3d_ctx** out) {
 }
 
 int fd3d_upload_medium(fd3d_ctx* ctx, const void* l, const void* m, const void* d, int rk) {
+    fd3d::TraceRange trace_("fd3d_upload_medium");
     if (!ctx) return FD3D_ERR_ARG;
     return ctx->impl->upload_medium(l, m, d, rk);
 }
 
 int fd3d_upload_medium_layers(fd3d_ctx* ctx, const double* l, const double* m, const double* d) {
+    fd3d::TraceRange trace_("fd3d_upload_medium_layers");
     if (!ctx) return FD3D_ERR_ARG;
     return ctx->impl->upload_medium_layers(l, m, d);
 }
 
 int fd3d_upload_fault(fd3d_ctx* ctx, const fd3d_fault* f) {
+    fd3d::TraceRange trace_("fd3d_upload_fault");
     if (!ctx) return FD3D_ERR_ARG;
     return ctx->impl->upload_fault(f);
 }
@@ -894,6 +900,7 @@ static int get_graph(CtxBase* c, int g, cudaGraphExec_t* out) {
 }
 
 int fd3d_run(fd3d_ctx* ctx, int nsteps) {
+    fd3d::TraceRange trace_("fd3d_run");
     if (!ctx || nsteps < 0) return FD3D_ERR_ARG;
     CtxBase* c = ctx->impl;
     if (!c->medium_ok || !c->fault_ok) return FD3D_ERR_STATE;
@@ -972,6 +979,7 @@ int fd3d_history_records(fd3d_ctx* ctx, int* nrec) {
 }
 
 int fd3d_fetch_history(fd3d_ctx* ctx, int field, int rec0, int nrec, void* host, int rk) {
+    fd3d::TraceRange trace_("fd3d_fetch_history");
     if (!ctx || !host || nrec < 0 || rec0 < 0 || (rk != 4 && rk != 8)) return FD3D_ERR_ARG;
     CtxBase* c = ctx->impl;
     if (field < 0 || field >= c->nf) return FD3D_ERR_ARG;
@@ -1044,6 +1052,7 @@ int fd3d_fetch_plane(fd3d_ctx* ctx, int plane, double* host) {
 
 int fd3d_upload_fault_model(fd3d_ctx* ctx, int nli, int nwi, const double* T0I, const double* TsI, const double* DcI,
                             double dip, int dipslip) {
+    fd3d::TraceRange trace_("fd3d_upload_fault_model");
     if (!ctx) return FD3D_ERR_ARG;
     return ctx->impl->upload_fault_model(nli, nwi, T0I, TsI, DcI, dip, dipslip);
 }
@@ -1080,6 +1089,7 @@ int fd3d_fetch_final(fd3d_ctx* ctx, double* slipX, double* slipZ, double* ruptim
 }
 
 int fd3d_write_results(fd3d_ctx* ctx, const char* dir, int rk) {
+    fd3d::TraceRange trace_("fd3d_write_results");
     if (!ctx || !dir || (rk != 4 && rk != 8)) return FD3D_ERR_ARG;
     return fd3d::write_results(ctx, ctx->impl->p, ctx->impl->nf, ctx->impl->rec_written, dir, rk);
 }
