@@ -28,7 +28,8 @@
  *  - real_kind selects the host element type of a buffer: 4 (float) or 8 (double),
  *    as the reference's `real` is 4 bytes by default and 8 bytes with -r8.
  *  - One context is driven by one host thread at a time.  Device memory is owned by
- *    the context.  Work is enqueued on the context's own CUDA stream.
+ *    the context.  Work is enqueued on the context's own CUDA streams (a main stream,
+ *    and a side stream that each step forks from it and joins back into it).
  */
 #ifndef FD3D_GPU_H
 #define FD3D_GPU_H
