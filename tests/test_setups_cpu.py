@@ -142,3 +142,25 @@ def test_reference_inversion_example_reads():
     m = configs.inversion_example(os.path.join(REF_EXAMPLES, "Amatrice2016"), dipslip=True)
     fm = m["fault_model"]
     assert fm["T0I"].shape == (13, 8) and np.isfinite(fm["DcI"]).all() and fm["DcI"].min() > 0
+
+
+def test_fspace_variant_keeps_the_model_below_the_top():
+    m = configs.tiny_sw(nsteps=10)
+    f = configs.fspace_variant(m)
+    nab, ks = m["nabc"], m["nzt"] - m["nfs"]
+    assert f["fspace"] and f["nfs"] == nab and f["nzt"] == m["nzt"] + nab - m["nfs"]
+    assert f["nzt"] - f["nfs"] == ks                          # the former free-surface row
+    for a, b in zip(m["medium"], f["medium"]):
+        np.testing.assert_array_equal(b[:m["nzt"]], a)
+    for k, v in m["fault"].items():
+        if isinstance(v, np.ndarray):
+            np.testing.assert_array_equal(f["fault"][k][:, :m["nzt"]], v)
+            assert f["fault"][k].flags.f_contiguous
+
+
+def test_reference_example_in_the_fspace_build(tmp_path):
+    d = synthetic_deck(tmp_path, "TPV5")
+    a = configs.reference_example(d, "TPV5")
+    b = configs.reference_example(d, "TPV5", fspace=True)
+    assert b["nfs"] == b["nabc"] and b["nzt"] - b["nfs"] == a["nzt"] - a["nfs"]
+    np.testing.assert_array_equal(b["medium"][1][:a["nzt"] - a["nfs"]], a["medium"][1][:a["nzt"] - a["nfs"]])
