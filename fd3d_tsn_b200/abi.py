@@ -124,6 +124,7 @@ def load_library(path: str | None = None) -> C.CDLL:
     i, vp, dp, fp = C.c_int, C.c_void_p, _DP, C.POINTER(C.c_float)
     sig = {
         "fd3d_version": (C.c_char_p, []),
+        "fd3d_struct_sizes": (i, [C.POINTER(C.c_size_t), C.POINTER(C.c_size_t)]),
         "fd3d_status_string": (C.c_char_p, [i]),
         "fd3d_device_count": (i, [C.POINTER(i)]),
         "fd3d_set_device": (i, [i]),

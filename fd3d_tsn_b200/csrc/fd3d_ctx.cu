@@ -743,6 +743,13 @@ extern "C" {
 
 const char* fd3d_version(void) { return "fd3d-b200 0.1 (sm_100a)"; }
 
+int fd3d_struct_sizes(size_t* params_bytes, size_t* fault_bytes) {
+    if (!params_bytes || !fault_bytes) return FD3D_ERR_ARG;
+    *params_bytes = sizeof(fd3d_params);
+    *fault_bytes = sizeof(fd3d_fault);
+    return FD3D_OK;
+}
+
 const char* fd3d_status_string(int s) {
     switch (s) {
         case FD3D_OK: return "ok";

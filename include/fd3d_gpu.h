@@ -157,6 +157,9 @@ typedef struct fd3d_ctx fd3d_ctx;
 
 /* library info */
 const char* fd3d_version(void);
+/* sizeof(fd3d_params) and sizeof(fd3d_fault) as this library was built, for hosts that
+ * declare the structs themselves (a Fortran bind(C) type, ctypes) to check their layout. */
+int fd3d_struct_sizes(size_t* params_bytes, size_t* fault_bytes);
 const char* fd3d_status_string(int status);
 int fd3d_device_count(int* count);
 /* device used by contexts created afterwards on the calling host thread */

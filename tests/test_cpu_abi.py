@@ -100,3 +100,12 @@ def test_reference_decks_parse(deck):
     np.testing.assert_allclose(lam[3, 2, :], L, rtol=1e-12)
     np.testing.assert_allclose(mu[3, 2, :], M, rtol=1e-12)
     np.testing.assert_allclose(dd[3, 2, :], D, rtol=1e-12)
+
+
+def test_struct_layouts_match_the_library():
+    """The ctypes mirrors of fd3d_params and fd3d_fault have the library's sizes."""
+    lib = abi.load_library()
+    pb, fb = C.c_size_t(), C.c_size_t()
+    assert lib.fd3d_struct_sizes(C.byref(pb), C.byref(fb)) == 0
+    assert pb.value == C.sizeof(abi.Params)
+    assert fb.value == C.sizeof(abi.Fault)
