@@ -109,3 +109,29 @@ def test_struct_layouts_match_the_library():
     assert lib.fd3d_struct_sizes(C.byref(pb), C.byref(fb)) == 0
     assert pb.value == C.sizeof(abi.Params)
     assert fb.value == C.sizeof(abi.Fault)
+
+
+def test_fortran_module_matches_the_library():
+    """include/fd3d_gpu.f90 (not compiled here: no Fortran compiler in the image) binds only
+    exported functions, and its derived types list the C structs' fields in their order."""
+    import re
+    src = open(os.path.join(ROOT, "include", "fd3d_gpu.f90")).read()
+    out = subprocess.run(["nm", "-D", "--defined-only", abi.LIB_PATH], capture_output=True, text=True,
+                         check=True).stdout
+    exported = {line.split()[-1] for line in out.splitlines() if line.strip()}
+    bound = re.findall(r"function\s+(fd3d_\w+)\s*\(", src)
+    assert len(bound) >= 15
+    assert not [f for f in bound if f not in exported]
+
+    def fields(type_name):
+        body = re.search(r"type, bind\(C\) :: " + type_name + r"\n(.*?)end type", src, re.S).group(1)
+        names = []
+        for line in body.splitlines():
+            if "::" not in line:
+                continue
+            decl = line.split("::")[1]
+            names += [re.sub(r"\(.*\)", "", n).strip().lower() for n in decl.split(",")]
+        return names
+
+    assert fields("fd3d_params") == [n.lower() for n, _ in abi.Params._fields_]
+    assert fields("fd3d_fault") == [n.lower() for n, _ in abi.Fault._fields_]
