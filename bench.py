@@ -10,8 +10,13 @@ history planes) over the whole grid.
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
 
 Prints one JSON line.  value = padded cells x steps x N / max-over-ranks device time.
-Under torchrun (N>1) every rank runs its own independent model (replicas; the path has
-no exchange step), so scaling is weak.
+The same line carries, as "batch" and "serve", the batched workload (256 models of
+uneven size, 8 s simulated, against the same models solved one at a time) and the
+serving workload (a mixed-size request stream through the continuous-batching loop:
+capacity solves/s, p50 / p99 latency at 70% of that capacity, against one-at-a-time
+solves), both measured after the timed region.  With N > 1 every rank runs its own
+independent replicas (the path has no exchange step), so scaling is weak; --gpus N
+started without torchrun starts N ranks under torch.distributed.run itself.
 """
 from __future__ import annotations
 
@@ -22,7 +27,6 @@ import statistics
 import subprocess
 import sys
 import tempfile
-import threading
 import time
 
 import numpy as np
@@ -269,7 +273,9 @@ def run_b200(args, world, rank, local, pg):
                 w = line.split()
                 if len(w) == 3 and not w[0].startswith("#") and w[0] == args.workload and w[1] == dom:
                     traffic = int(w[2])
+    info = s.info()
     roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "interior_variant": info["interior_variant"], "layered_medium": info["layered_medium"],
                 "frac": achieved / peak, "peak_source": peak_kind, "traffic": traffic,
                 "algorithmic_bytes_per_launch": dom_bytes, "avg_launch_ms": dom_ms,
                 "step_frac": step_gbs / peak, "step_gbs": step_gbs,
@@ -284,6 +290,10 @@ def run_b200(args, world, rank, local, pg):
         e2e_v = max_over_ranks(pg, local, e2e.pop("_seconds"))
         e2e["value"] = whole_job_rate(cells * args.steps, world, e2e_v) / 1e9
 
+    # the batched and serving workloads, after the timed region of the production model
+    batch = batch_section(args, world, rank, local, pg) if args.batch and args.workload == "sw_large" else None
+    serving = serve_section(args, world, rank, local, pg) if args.serve and args.workload == "sw_large" else None
+
     cpu = None
     if rank == 0 and world == 1 and args.cpu_baseline > 0:
         cpu = cpu_baseline(m, args.cpu_baseline)
@@ -295,6 +305,10 @@ def run_b200(args, world, rank, local, pg):
                 "cpu_baseline": cpu, "e2e": e2e, "clocks": ck,
                 "gpu_launches": gpu_launches(m, args.steps),
                 "hbm_roofline_frac_step": step_gbs / peak}
+        if batch is not None:
+            line["batch"] = batch
+        if serving is not None:
+            line["serve"] = serving
         print(json.dumps(line), flush=True)
 
 
@@ -380,10 +394,40 @@ def _same_finals(a, b):
     return all(np.array_equal(a[k], b[k]) for k in ("slipX", "slipZ", "ruptime", "rise", "sliptime"))
 
 
-def run_batch_bench(args, world, rank, local, pg):
-    """256 slip-weakening models of uneven size (fault 8-24 x 6-14 km, h=200 m, 8 s) in
-    one persistent launch per chunk of steps, against the same models solved one at a
-    time through the single-model path."""
+def pml_cells(m):
+    """Cells of the PML strips' u/w loop ranges (init_pml, src/fd3d_deriv.f90:1319-1410):
+    x-low and x-high (nabc-1 wide, j up to nyt, interior k), y-low (nabc-1 rows), z-low
+    (nabc-1 planes) and, under FSPACE, the top strip."""
+    nxt, nyt, nzt, nab, nfs = m["nxt"], m["nyt"], m["nzt"], m["nabc"], m["nfs"]
+    nk = nzt - nfs - nab
+    n = 2 * (nab - 1) * (nyt - nab) * nk + (nxt - 2) * (nab - 1) * nk + (nxt - 2) * (nyt - 1) * (nab - 1)
+    if m.get("fspace"):
+        n += (nxt - 2) * (nyt - 1) * (nab - 1)
+    return n
+
+
+def interior_cells(m):
+    nab = m["nabc"]
+    return (m["nxt"] - 2 * nab) * (m["nyt"] - 2 - nab) * (m["nzt"] - nab - m["nfs"])
+
+
+# algorithmic bytes of one step of a layered-medium model: 108 B per interior cell (velocity
+# 48 + stress 60) and 264 B per PML cell (108 + 156: fields plus the split components)
+B_INTERIOR_LAYERED = B_ALG_VEL_LAYERED + B_ALG_STR_LAYERED
+B_PML_LAYERED = 108 + 156
+
+
+def step_bytes(m):
+    return interior_cells(m) * B_INTERIOR_LAYERED + pml_cells(m) * B_PML_LAYERED
+
+
+def batch_section(args, world, rank, local, pg):
+    """The batched workload: args.models slip-weakening models of uneven size (fault 8-24 x
+    6-14 km, h = 200 m, 8 s simulated) in one batch, the schedule and tile shape tuned on
+    the live batch first, against the same models solved one at a time through the
+    single-model path (create, upload, run, read back, destroy).  Solves/s and cell
+    updates/s are wall clock over the whole run; the HBM fraction is the batch's
+    algorithmic bytes (PML split components counted) over its GPU time."""
     from fd3d_tsn_b200 import configs
     from fd3d_tsn_b200.batch import Batch, bytes_needed
     from fd3d_tsn_b200.solver import lib
@@ -393,6 +437,7 @@ def run_batch_bench(args, world, rank, local, pg):
     for q, m in enumerate(models):
         m["request"] = q
     cells = sum(m["nxt"] * m["nyt"] * m["nzt"] * m["ntfd"] for m in models)
+    alg_bytes = sum(step_bytes(m) * m["ntfd"] for m in models)
     arena = int(sum(bytes_needed(m) for m in models) * 1.05) + (64 << 20)
     t_setup = time.perf_counter()
     b = Batch(arena, len(models) + 8)
@@ -415,33 +460,39 @@ def run_batch_bench(args, world, rank, local, pg):
     b.close()
     wall_max = max_over_ranks(pg, local, wall)
     ref, t_plain = plain(models)
+    t_plain_max = max_over_ranks(pg, local, t_plain)
     identical = all(_same_finals(finals[q], ref[q]) for q in ref)
-    if rank == 0:
-        line = {"metric": "batched solves/s", "value": whole_job_rate(len(models), world, wall_max), "unit": "solves/s",
-                "n_gpus": world, "higher_is_better": True, "scaling": "weak", "dtype": "f32", "data": "synthetic",
-                "config": {"workload": "batch", "models": len(models), "h_m": 200.0, "sim_s": 8.0,
-                           "cells_x_steps": cells},
-                "gcell_updates_per_s": cells / wall / 1e9, "gpu_s": gpu, "wall_s": wall, "setup_s": t_setup,
-                "tuning": tune,
-                "plain": {"solves_per_s": len(models) / t_plain, "wall_s": t_plain,
-                          "gcell_updates_per_s": cells / t_plain / 1e9},
-                "speedup_vs_plain": (len(models) / wall) / (len(models) / t_plain),
-                "results_identical_to_plain": identical}
-        print(json.dumps(line), flush=True)
+    peak, peak_kind = measured_peak()
+    rate = whole_job_rate(len(models), world, wall_max)
+    plain_rate = whole_job_rate(len(models), world, t_plain_max)
+    return {"metric": "batched solves/s", "value": rate, "unit": "solves/s",
+            "config": {"workload": "batch", "models": len(models), "h_m": 200.0, "sim_s": 8.0,
+                       "cells_x_steps": cells, "fault_km": [[8, 24], [6, 14]]},
+            "gcell_updates_per_s": cells * world / wall_max / 1e9, "wall_s": wall_max, "gpu_s": gpu,
+            "setup_s": t_setup,
+            "hbm": {"algorithmic_bytes": alg_bytes, "gbs_on_gpu_time": alg_bytes / gpu / 1e9,
+                    "frac": alg_bytes / gpu / 1e9 / peak, "peak": peak, "peak_source": peak_kind,
+                    "bytes_per_cell": "108 B per interior cell, 264 B per PML cell (split components counted)"},
+            "tuning": tune,
+            "plain": {"solves_per_s": plain_rate, "wall_s": t_plain_max,
+                      "gcell_updates_per_s": cells * world / t_plain_max / 1e9},
+            "speedup_vs_plain": rate / plain_rate,
+            "results_identical_to_plain": identical}
 
 
-def run_serve_bench(args, world, rank, local, pg):
-    """Poisson stream of mixed-size requests (95% batch-size models, 5% large h=100 m
-    models) through the continuous-batching loop.  The schedule and tile shape are
-    tuned once on a sample of the request mix before serving starts (a server warms up
-    before it takes traffic).  Two runs of the same stream: at the offered --rate (p50 /
-    p99 latency under that load) and with every request arriving at once (capacity,
-    the reported solves/s), against one-at-a-time plain solves of a sample."""
+def serve_section(args, world, rank, local, pg):
+    """Continuous batching of a Poisson stream of mixed-size requests (95% batch-size
+    models, 5% large h = 100 m models, args.sim_time simulated seconds each).  The
+    schedule and tile shape are tuned once on a sample of the mix before traffic (a
+    server warms up before it takes requests).  Two runs of the same stream: every
+    request arriving at once (capacity: the reported solves/s) and Poisson arrivals at
+    args.load of that capacity (p50 / p99 latency under load), against one-at-a-time
+    plain solves of a sample of the stream."""
     from fd3d_tsn_b200 import configs
     from fd3d_tsn_b200.serve import plain, pretune, serve
     from fd3d_tsn_b200.solver import lib
     lib().fd3d_set_device(local)
-    stream = configs.serving_stream(args.requests, seed=4242 + rank, rate=args.rate, sim_time=args.sim_time)
+    stream = configs.serving_stream(args.requests, seed=4242 + rank, rate=1.0, sim_time=args.sim_time)
     sample = set(range(0, len(stream), max(1, len(stream) // args.plain_sample)))
     budget = int(args.hbm_gb * (1 << 30))
     t_tune = time.perf_counter()
@@ -449,36 +500,75 @@ def run_serve_bench(args, world, rank, local, pg):
                      cache_path=os.path.join(tempfile.gettempdir(), "fd3d_batch_tune.jsonl"),
                      key=f"serve-{args.sim_time}-{args.requests}-{rank}")
     t_tune = time.perf_counter() - t_tune
-    results, stats = serve(stream, budget, chunk=32, tuning=tuning, keep_final=lambda r: r in sample)
     burst = [(0.0, m) for _, m in stream]
+    barrier(pg, local)
     _, cap = serve(burst, budget, chunk=32, tuning=tuning, keep_final=lambda r: False)
+    cap_max = max_over_ranks(pg, local, cap["makespan_s"])
+    capacity = whole_job_rate(cap["requests"], world, cap_max)
+    # the same requests arriving as a Poisson stream at args.load of the measured capacity
+    rate = args.load * cap["requests"] / cap_max
+    gaps = np.random.default_rng(4243 + rank).exponential(1.0 / rate, size=len(stream))
+    timed = [(float(t), m) for t, (_, m) in zip(np.cumsum(gaps), stream)]
+    results, stats = serve(timed, budget, chunk=32, tuning=tuning, keep_final=lambda r: r in sample)
     byreq = {r.request: r for r in results}
     ref, t_plain = plain([m for q, (_, m) in enumerate(stream) if q in sample], keep_final=lambda r: True)
     identical = all(_same_finals(byreq[q].final, ref[q]) for q in ref)
-    plain_rate = len(ref) / t_plain
-    cap_max = max_over_ranks(pg, local, cap["makespan_s"])
+    plain_rate = len(ref) / max_over_ranks(pg, local, t_plain) * world
+    nlarge = sum(1 for _, m in stream if m["dh"] == 100.0)
+    return {"metric": "serving solves/s", "value": capacity, "unit": "solves/s",
+            "config": {"workload": "serve", "requests": len(stream), "large_requests": nlarge,
+                       "large_fraction": 0.05, "sim_s": args.sim_time, "hbm_budget_gb": args.hbm_gb,
+                       "offered_rate_per_s": rate, "offered_load_of_capacity": args.load},
+            "p50_latency_s": stats["p50_latency_s"], "p99_latency_s": stats["p99_latency_s"],
+            "offered_load": stats, "capacity": cap, "tuning": tuning, "tuning_s": t_tune,
+            "plain": {"solves_per_s": plain_rate, "sample": len(ref), "wall_s": t_plain},
+            "speedup_vs_plain": capacity / plain_rate,
+            "results_identical_to_plain": identical}
+
+
+def _line(sec, world):
+    out = dict(sec)
+    out.update(n_gpus=world, higher_is_better=True, scaling="weak", dtype="f32", data="synthetic")
+    return out
+
+
+def run_batch_bench(args, world, rank, local, pg):
+    sec = batch_section(args, world, rank, local, pg)
     if rank == 0:
-        line = {"metric": "serving solves/s", "value": whole_job_rate(cap["requests"], world, cap_max),
-                "unit": "solves/s", "n_gpus": world, "higher_is_better": True, "scaling": "weak", "dtype": "f32",
-                "data": "synthetic",
-                "config": {"workload": "serve", "requests": len(stream), "arrival_rate_per_s": args.rate,
-                           "large_fraction": 0.05, "sim_s": args.sim_time, "hbm_budget_gb": args.hbm_gb},
-                "p50_latency_s": stats["p50_latency_s"], "p99_latency_s": stats["p99_latency_s"],
-                "offered_load": stats, "capacity": cap, "tuning": tuning, "tuning_s": t_tune,
-                "plain": {"solves_per_s": plain_rate, "sample": len(ref), "wall_s": t_plain},
-                "speedup_vs_plain": cap["solves_per_s"] / plain_rate,
-                "results_identical_to_plain": identical}
-        print(json.dumps(line), flush=True)
+        print(json.dumps(_line(sec, world)), flush=True)
+
+
+def run_serve_bench(args, world, rank, local, pg):
+    sec = serve_section(args, world, rank, local, pg)
+    if rank == 0:
+        print(json.dumps(_line(sec, world)), flush=True)
+
+
+def _free_port():
+    import socket
+    with socket.socket() as so:
+        so.bind(("127.0.0.1", 0))
+        return so.getsockname()[1]
+
+
+def relaunch(ngpus):
+    """bench.py --gpus N started as a plain process: run it again as N ranks under
+    torch.distributed.run (one process per GPU, rendezvous on 127.0.0.1)."""
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", str(ngpus),
+           "--master-addr", "127.0.0.1", "--master-port", str(_free_port()), os.path.abspath(__file__),
+           *sys.argv[1:]]
+    return subprocess.call(cmd)
 
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--models", type=int, default=256, help="batch workload: number of models")
-    ap.add_argument("--requests", type=int, default=2000, help="serve workload: number of requests")
-    ap.add_argument("--rate", type=float, default=60.0, help="serve workload: Poisson arrival rate (1/s)")
-    ap.add_argument("--sim-time", type=float, default=2.0, help="serve workload: simulated seconds per request")
-    ap.add_argument("--plain-sample", type=int, default=64, help="serve workload: plain solves timed")
-    ap.add_argument("--hbm-gb", type=float, default=120.0, help="serve workload: arena (HBM budget) in GB")
+    ap.add_argument("--models", type=int, default=256, help="batched workload: number of models")
+    ap.add_argument("--requests", type=int, default=500, help="serving workload: number of requests")
+    ap.add_argument("--load", type=float, default=0.7,
+                    help="serving workload: offered Poisson rate as a fraction of the measured capacity")
+    ap.add_argument("--sim-time", type=float, default=8.0, help="serving workload: simulated seconds per request")
+    ap.add_argument("--plain-sample", type=int, default=32, help="serving workload: plain solves timed")
+    ap.add_argument("--hbm-gb", type=float, default=120.0, help="serving workload: arena (HBM budget) in GB")
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=5)
@@ -487,9 +577,19 @@ def main():
     ap.add_argument("--cpu-baseline", type=float, default=15.0, help="seconds of oracle time (0 = skip)")
     ap.add_argument("--ref-seconds", type=float, default=60.0, help="reference arm: CPU seconds to time")
     ap.add_argument("--no-e2e", dest="e2e", action="store_false")
+    ap.add_argument("--no-batch", dest="batch", action="store_false",
+                    help="leave the batched workload out of the default line")
+    ap.add_argument("--no-serve", dest="serve", action="store_false",
+                    help="leave the serving workload out of the default line")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
+    ws = os.environ.get("WORLD_SIZE")
+    if ws is None and args.gpus > 1:
+        sys.exit(relaunch(args.gpus))
+    if ws is not None and int(ws) != args.gpus:
+        print(f"bench.py: --gpus {args.gpus} but WORLD_SIZE={ws}", file=sys.stderr)
+        sys.exit(2)
     world, rank, local, pg = dist_setup(args.gpus)
     try:
         if args.impl == "reference":

@@ -147,6 +147,7 @@ def load_library(path: str | None = None) -> C.CDLL:
         "fd3d_last_run_ms": (i, [vp, fp]),
         "fd3d_set_profiling": (i, [vp, i]),
         "fd3d_kernel_times": (i, [vp, fp, C.POINTER(i)]),
+        "fd3d_ctx_info": (i, [vp, C.POINTER(i), C.POINTER(i)]),
         "fd3d_read_deck": (i, [C.c_char_p, C.POINTER(Params), C.POINTER(dp), C.POINTER(dp), C.POINTER(dp)]),
         "fd3d_read_deck_ex": (i, [C.c_char_p, i, C.POINTER(Params), C.POINTER(dp), C.POINTER(dp), C.POINTER(dp)]),
         "fd3d_free": (None, [vp]),

@@ -178,6 +178,7 @@ struct CtxBase {
     virtual size_t elem() const = 0;
     virtual int save_state(std::FILE* fp) = 0;
     virtual int load_state(std::FILE* fp) = 0;
+    virtual bool layered() const = 0;
 };
 
 template <class T>
@@ -195,6 +196,7 @@ struct Ctx : CtxBase {
     T* fieldpool = nullptr;
     std::vector<double> psiX0, psiZ0;  // initial FVW state, restored by reset
     size_t elem() const override { return sizeof(T); }
+    bool layered() const override { return f.lay != nullptr; }
 
     // Device memory of the context: one allocation (zeroed once) carved into 256-byte
     // aligned arrays; a request beyond it gets its own allocation.
@@ -300,7 +302,11 @@ struct Ctx : CtxBase {
         CK(cudaMemcpyAsync(dprof, prof.data(), prof.size() * sizeof(Damp<T>), cudaMemcpyHostToDevice, st));
         X.prof = dprof;
         tma_ok = make_interior_maps<T>(g, f, vmaps, smaps) && prepare_tma_kernels<T>();
-        if (!tma_ok && icfg.variant == IV_TMA) icfg.variant = IV_PIPE;
+        if (!tma_ok && icfg.variant == IV_TMA) {
+            std::fprintf(stderr, "fd3d: tensor maps of the interior sweeps could not be encoded for this grid; "
+                                 "the interior sweeps fall back to plain loads (fd3d_ctx_info reports it)\n");
+            icfg.variant = IV_PIPE;
+        }
         if (dalloc(&it_dev, 1)) return FD3D_ERR_NOMEM;
         if (dalloc(&status, 1)) return FD3D_ERR_NOMEM;
         T* r = nullptr;
@@ -975,6 +981,14 @@ int fd3d_kernel_times(fd3d_ctx* ctx, float* ms, int* launches) {
         ms[k] = c->ktimes[k];
         if (launches) launches[k] = c->klaunch[k];
     }
+    return FD3D_OK;
+}
+
+int fd3d_ctx_info(fd3d_ctx* ctx, int* interior_variant, int* layered_medium) {
+    if (!ctx) return FD3D_ERR_ARG;
+    CtxBase* c = ctx->impl;
+    if (interior_variant) *interior_variant = c->icfg.variant;
+    if (layered_medium) *layered_medium = c->layered() ? 1 : 0;
     return FD3D_OK;
 }
 

@@ -132,6 +132,15 @@ class Solver:
         _ck(lib().fd3d_kernel_times(self.h, ms, n), "fd3d_kernel_times")
         return {abi.KERNEL_NAMES[k]: (ms[k], n[k]) for k in range(abi.NKERNELS)}
 
+    INTERIOR_VARIANTS = {0: "point", 1: "tiled", 2: "pipe", 3: "tma"}
+
+    def info(self) -> dict:
+        """Which interior sweep runs ("tma" unless the tensor maps could not be encoded or
+        FD3D_INTERIOR chose another) and whether the medium is read as a 1-D profile."""
+        v, lay = C.c_int(), C.c_int()
+        _ck(lib().fd3d_ctx_info(self.h, C.byref(v), C.byref(lay)), "fd3d_ctx_info")
+        return dict(interior_variant=self.INTERIOR_VARIANTS.get(v.value, str(v.value)), layered_medium=bool(lay.value))
+
     # ------------------------------------------------------------ outputs
     def history_records(self) -> int:
         n = C.c_int()

@@ -16,6 +16,8 @@ module fd3d_gpu
   integer(c_int), parameter :: FD3D_ERR_BUSY = -10, FD3D_ERR_TIMEOUT = -11
   integer(c_int), parameter :: FD3D_LAW_SW = 0, FD3D_LAW_FVW = 1
   integer(c_int), parameter :: FD3D_PREC_F32 = 0, FD3D_PREC_F64 = 1
+  integer(c_int), parameter :: FD3D_INTERIOR_POINT = 0, FD3D_INTERIOR_TILED = 1
+  integer(c_int), parameter :: FD3D_INTERIOR_PIPE = 2, FD3D_INTERIOR_TMA = 3
 
   type, bind(C) :: fd3d_params
     integer(c_int) :: nxt, nyt, nzt, nabc, nfs, ntfd
@@ -80,6 +82,11 @@ module fd3d_gpu
     integer(c_int) function fd3d_sync(ctx) bind(C)
       import
       type(c_ptr), value :: ctx
+    end function
+    integer(c_int) function fd3d_ctx_info(ctx, interior_variant, layered_medium) bind(C)
+      import
+      type(c_ptr), value :: ctx
+      integer(c_int) :: interior_variant, layered_medium
     end function
     integer(c_int) function fd3d_fetch_history(ctx, field, rec0, nrec, host, real_kind) bind(C)
       import

@@ -232,6 +232,17 @@ int fd3d_last_run_ms(fd3d_ctx* ctx, float* ms);
 /* per-kernel timing over the last run when profiling is switched on */
 int fd3d_set_profiling(fd3d_ctx* ctx, int on);
 int fd3d_kernel_times(fd3d_ctx* ctx, float* ms /* FD3D_NKERNELS */, int* launches);
+/* How the context runs its time step (no counterpart in the reference).  interior_variant:
+ * FD3D_INTERIOR_TMA, the interior sweeps fed by 3-D tensor-memory-accelerator tiles (the
+ * default), or a slower plain-load variant, taken when the tensor maps cannot be encoded for
+ * this grid (a message on stderr says so at creation) or when the FD3D_INTERIOR environment
+ * variable selects it.  layered_medium: 1 when the uploaded medium varies with depth only and
+ * the sweeps read one value per plane.  Either pointer may be NULL. */
+#define FD3D_INTERIOR_POINT 0
+#define FD3D_INTERIOR_TILED 1
+#define FD3D_INTERIOR_PIPE  2
+#define FD3D_INTERIOR_TMA   3
+int fd3d_ctx_info(fd3d_ctx* ctx, int* interior_variant, int* layered_medium);
 #define FD3D_NKERNELS 8
 /* kernel ids in fd3d_kernel_times: 0 vel_interior, 1 vel_fault, 2 vel_pml, 3 vel_fs,
    4 str_interior, 5 str_fault, 6 str_pml, 7 fault_bc (traction+friction+output) */

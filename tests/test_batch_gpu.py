@@ -4,7 +4,8 @@ Every model in a batch must produce the same bits as the same model solved alone
 with fd3d_run (the per-item device bodies are the single-model kernels' bodies), no
 matter which other models share the launch, when it joined, which schedule runs the
 batch (one persistent cooperative kernel, or graphs of per-region kernels) or which
-tile shape the autotuner picked.
+tile shape the autotuner picked.  Models of the batched workload's own size are also
+checked against the oracle directly, in both schedules.
 """
 import numpy as np
 import pytest
@@ -12,8 +13,14 @@ import pytest
 from fd3d_tsn_b200 import configs
 from fd3d_tsn_b200.batch import Batch, bytes_needed
 from fd3d_tsn_b200.solver import Solver
+from oracle.oracle import MIXED, Oracle
 
 pytestmark = pytest.mark.gpu
+
+
+def rel_l2(a, b):
+    nb = np.linalg.norm(b)
+    return np.linalg.norm(np.asarray(a) - np.asarray(b)) / (nb if nb > 0 else 1.0)
 
 
 def small_models(n, seed0=100, steps=30):
@@ -123,3 +130,53 @@ def test_autotune_keeps_results(tmp_path):
     b2 = Batch(1 << 30, 4)
     b2.add(models[0])
     assert b2.autotune(steps=5, cache_path=str(tmp_path / "tune.jsonl"), key="test3") == {**t, "max_ctas_per_sm": t["max_ctas_per_sm"]}
+
+
+def batch_size_fvw(steps):
+    """A rate-and-state model of the batched workload's size (h = 200 m, 140 x 30 x 70
+    simulated cells, a 16 x 8 km fault, nucleation ramp on)."""
+    m = configs.fvw_model(140, 30, 70, 200.0, 1.0, 88, fault_m=(16e3, 8e3), dt=0.008, ntfd=steps,
+                          history_stride=1, border_m=2000.0, R=2000.0, TT=0.1)
+    m["history_capacity"] = steps
+    return m
+
+
+@SCHEDULES
+def test_batch_models_against_oracle(schedule):
+    """Models of the batched workload's distribution (fault 8-24 x 6-14 km, h = 200 m,
+    grids of 0.35-0.9 M cells) plus a rate-and-state model of the same size, in one
+    batch, each against the oracle: slip weakening bit for bit (histories, final planes,
+    tractions, slip path), rate-and-state within 1e-5 relative
+    L2 on all five history fields and the state planes."""
+    steps = 40
+    models = configs.batch_set(4, seed=515, ntfd=steps)
+    for m in models:
+        m["history_capacity"] = steps
+    fvw = batch_size_fvw(steps)
+    b = Batch(4 << 30, 8)
+    b.set_schedule(schedule)
+    slots = [b.add(m) for m in models]
+    fslot = b.add(fvw)
+    b.run(steps)
+    b.sync()
+    for m, slot in zip(models, slots):
+        assert b.steps_done(slot) == steps
+        o = Oracle(m, MIXED)
+        oh, _ = o.step(steps)
+        assert np.abs(oh[:, 0]).max() > 0.1, "the nucleation patch must slip"
+        for f in range(4):
+            np.testing.assert_array_equal(b.history(slot, f, 0, steps), oh[:, f], err_msg=f"field {f}")
+        fo, fb = o.final(), b.final(slot)
+        for k in fo:
+            np.testing.assert_array_equal(fb[k], fo[k], err_msg=k)
+        for name in ("tx", "tz", "distZ"):
+            np.testing.assert_array_equal(b.plane(slot, name), o.plane(name), err_msg=name)
+        o.close()
+    o = Oracle(fvw, MIXED)
+    oh, _ = o.step(steps)
+    assert np.abs(oh[:, 0]).max() > 1e-3, "the nucleation must start slip"
+    for f in range(5):
+        assert rel_l2(b.history(fslot, f, 0, steps), oh[:, f]) <= 1e-5, f
+    for name in ("psiX", "psiZ", "slipX", "slipZ"):
+        assert rel_l2(b.plane(fslot, name), o.plane(name)) <= 1e-5, name
+    b.close()

@@ -12,7 +12,8 @@ import pytest
 from fd3d_tsn_b200 import abi, configs, solver
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-REF_EXAMPLES = "/root/reference/examples"
+# the reference's examples/ directory (input decks), when a copy is at hand
+REF_EXAMPLES = os.environ.get("FD3D_REFERENCE_EXAMPLES", "")
 
 
 def test_library_exports_every_header_symbol():
@@ -86,7 +87,8 @@ def test_deck_cfl_stop(tmp_path):
     assert e.value.code == -2
 
 
-@pytest.mark.skipif(not os.path.isdir(REF_EXAMPLES), reason="reference examples not present")
+@pytest.mark.skipif(not (REF_EXAMPLES and os.path.isdir(REF_EXAMPLES)),
+                    reason="FD3D_REFERENCE_EXAMPLES does not name the reference's examples directory")
 @pytest.mark.parametrize("deck", ["TPV5", "TPV104", "TPV9", "Amatrice2016"])
 def test_reference_decks_parse(deck):
     d = os.path.join(REF_EXAMPLES, deck)

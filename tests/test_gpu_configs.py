@@ -4,9 +4,16 @@
   the whole run against the oracle, bit for bit in FP32, and the FP32 build against the
   FP64 oracle at the stated accuracy (relative L2 <= 1e-3 on the slip-rate and traction
   histories, final slip <= 1e-4, rupture time within 2 dt).
-* The production model (1000 x 400 x 500 cells, 214 M padded): properties that hold at
-  any size -- a run repeated after fd3d_reset is the same bits, and the FP64 build of
-  the same kernels agrees with the FP32 build at the stated accuracy.
+* The production model (1000 x 400 x 500 cells, 214 M padded): the first 24 steps bit
+  for bit against the oracle (histories, stations, wave fields, fault planes), and
+  properties that hold at any size -- a run repeated after fd3d_reset is the same bits,
+  and the FP64 build of the same kernels agrees with the FP32 build at the stated
+  accuracy.
+* The rate-and-state model (600 x 300 x 400 cells, 79 M padded, histories every 5
+  steps): 50 steps against the oracle within 1e-5 relative L2 (CUDA's and libm's
+  exp/log/sinh/asinh differ in the last bits).
+* A rate-and-state model that ruptures (48 x 14 x 32 cells, 250 steps): the FP32 build
+  against the FP64 oracle at the stated accuracy, rupture time included.
 """
 import numpy as np
 import pytest
@@ -71,6 +78,80 @@ def test_small_model_fp32_against_fp64_oracle():
     ruptured = fo["ruptime"] < 1e4
     assert np.all((fg["ruptime"] < 1e4) == ruptured)
     assert np.abs(fg["ruptime"][ruptured] - fo["ruptime"][ruptured]).max() <= 2 * m["dt"]
+
+
+def test_production_model_bitwise_against_oracle():
+    """214 M padded cells, 5 layers, 800 x 400 frictional nodes: the FP32 build against
+    the oracle's FP32-field / FP64-accumulator variant over 24 steps, compared one
+    array at a time to bound the host memory (each 3-D field is 1.7 GB in FP64)."""
+    steps = 24
+    m = configs.sw_large(ntfd=steps)
+    m["history_capacity"] = steps
+    o = Oracle(m, MIXED)
+    oh, os_ = o.step(steps)
+    s = Solver(m)
+    s.run(steps)
+    s.sync()
+    assert np.abs(oh[:, 0]).max() > 0.1, "the nucleation patch must slip"
+    for f in range(4):
+        np.testing.assert_array_equal(s.history(f), oh[:, f], err_msg=f"history field {f}")
+    np.testing.assert_array_equal(s.stations(), os_)
+    del oh
+    for name in ("u", "w", "xz", "yy"):
+        np.testing.assert_array_equal(s.field(name), o.field(name), err_msg=name)
+    for name in ("tx", "tz", "distX", "distZ", "slipX", "slipZ", "ruptime", "rise", "sliptime"):
+        np.testing.assert_array_equal(s.plane(name), o.plane(name), err_msg=name)
+    s.close()
+    o.close()
+
+
+def test_fvw_medium_against_oracle():
+    """600 x 300 x 400 cells, rate-and-state friction, FP64 state and Newton solve at the
+    fault, nucleation ramp on, histories every 5 steps: 50 steps against the oracle."""
+    steps = 50
+    m = configs.fvw_medium(ntfd=steps)
+    assert m["history_stride"] == 5
+    m["history_capacity"] = steps // 5
+    o = Oracle(m, MIXED)
+    oh, os_ = o.step(steps)
+    s = Solver(m)
+    s.run(steps)
+    s.sync()
+    nrec = steps // 5
+    assert s.history_records() == nrec
+    ohr = oh[4::5]   # the oracle returns every step; the records are steps 5, 10, ...
+    for f in range(5):
+        assert rel_l2(s.history(f), ohr[:, f]) <= 1e-5, (f, rel_l2(s.history(f), ohr[:, f]))
+    assert rel_l2(s.stations(), os_[4::5]) <= 1e-5
+    for name in ("psiX", "psiZ", "slipX", "slipZ", "T0X"):   # T0X carries the nucleation ramp
+        assert rel_l2(s.plane(name), o.plane(name)) <= 1e-5, name
+    s.close()
+    o.close()
+
+
+def test_fvw_fp32_against_fp64_oracle():
+    """Rate-and-state friction, FP32 wave field with the FP64 per-node state and slip-rate
+    solve, against the all-FP64 oracle at the stated accuracy: relative L2 <= 1e-3 on the
+    slip-rate, traction and state histories, final slip <= 1e-4, and rupture time within
+    2 dt on the same set of ruptured nodes."""
+    steps = 250
+    m = configs.tiny_fvw(nsteps=steps, nxT=48, nzT=32)
+    m["history_capacity"] = steps
+    o = Oracle(m, F64)
+    oh, _ = o.step(steps)
+    s = Solver(m)
+    s.run(steps)
+    s.sync()
+    for f in range(5):
+        assert rel_l2(s.history(f), oh[:, f]) <= 1e-3, (f, rel_l2(s.history(f), oh[:, f]))
+    fo, fg = o.final(), s.final()
+    assert rel_l2(fg["slipX"], fo["slipX"]) <= 1e-4
+    assert rel_l2(fg["slipZ"], fo["slipZ"]) <= 1e-4
+    ruptured = fo["ruptime"] < 1e4
+    assert ruptured.sum() > 100, "the model must rupture beyond its nucleation"
+    assert np.all((fg["ruptime"] < 1e4) == ruptured)
+    assert np.abs(fg["ruptime"][ruptured] - fo["ruptime"][ruptured]).max() <= 2 * m["dt"]
+    s.close()
 
 
 def test_production_model_repeatable_and_fp64_consistent():

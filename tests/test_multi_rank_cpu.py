@@ -3,7 +3,8 @@
 The path shards only as replicas: the process group carries the barrier around the
 timed region and the max-over-ranks reduction of the timings, nothing else.  These
 tests run that plumbing with the gloo backend and check the whole-job aggregate, and
-run the reference arm under torchrun, where rank 0 alone works and prints.
+run the reference arm under torchrun, where rank 0 alone works and prints, and as a plain
+process with --gpus 2, which starts the two ranks itself.
 """
 import json
 import os
@@ -72,3 +73,23 @@ def test_reference_arm_under_torchrun_prints_once():
     assert line["cpu_baseline"]["kind"] == "port" and line["cpu_baseline"]["cores"] >= 1
     assert line["e2e"]["h2d_bytes_per_step"] == 0 and line["e2e"]["d2h_bytes_per_step"] == 0
     assert line["value"] > 0
+
+
+def test_gpus_flag_starts_the_ranks_itself():
+    """bench.py --gpus 2 run as a plain process (no WORLD_SIZE) relaunches itself as two
+    ranks under torch.distributed.run, and rank 0 alone prints the line."""
+    env = {k: v for k, v in os.environ.items() if k not in ("WORLD_SIZE", "RANK", "LOCAL_RANK")}
+    env.update(FD3D_BENCH_BACKEND="gloo", FD3D_ORACLE_THREADS="2")
+    cmd = [sys.executable, "bench.py", "--impl", "reference", "--gpus", "2", "--workload", "sw_small",
+           "--steps", "2", "--warmup", "3", "--ref-seconds", "1"]
+    r = subprocess.run(cmd, cwd=ROOT, env=env, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = [json.loads(l) for l in r.stdout.splitlines() if l.startswith("{")]
+    assert len(lines) == 1 and lines[0]["impl"] == "reference"
+
+
+def test_gpus_flag_must_match_the_rank_count():
+    env = dict(os.environ, WORLD_SIZE="2", RANK="0", LOCAL_RANK="0", FD3D_BENCH_BACKEND="gloo")
+    r = subprocess.run([sys.executable, "bench.py", "--impl", "reference", "--gpus", "3"], cwd=ROOT, env=env,
+                       capture_output=True, text=True, timeout=120)
+    assert r.returncode == 2 and "WORLD_SIZE=2" in r.stderr

@@ -1,12 +1,14 @@
 """The continuous-batching request loop: requests of mixed size arrive while others
 are on the GPU, are admitted as arena space frees up (their set-up overlapping the
-running chunk), and each result is the same bits as the request solved alone."""
+running chunk), and each result is the same bits as the request solved alone and as the
+oracle's solve of it."""
 import numpy as np
 import pytest
 
 from fd3d_tsn_b200 import configs
 from fd3d_tsn_b200.batch import bytes_needed
 from fd3d_tsn_b200.serve import plain, pretune, serve
+from oracle.oracle import MIXED, Oracle
 
 pytestmark = [pytest.mark.gpu, pytest.mark.timeout(300)]
 
@@ -62,3 +64,27 @@ def test_oversized_request_is_rejected_not_queued_forever():
     results, stats = serve(s, budget, chunk=8)
     assert stats["rejected"] == 1 and stats["requests"] == 2
     assert {r.request for r in results} == {small[0]["request"], small[1]["request"]}
+
+
+def test_served_results_against_oracle():
+    """Requests of the batched workload's size (h = 200 m, 0.35-0.9 M cells) through the
+    request loop, two of them checked against the oracle directly, bit for bit."""
+    steps = 30
+    models = configs.batch_set(6, seed=616, ntfd=steps)
+    s = []
+    for q, m in enumerate(models):
+        m["request"] = q
+        m["history_capacity"] = 8
+        s.append((0.002 * q, m))
+    budget = 3 * max(bytes_needed(m) for m in models)
+    results, stats = serve(s, budget, chunk=8)
+    assert stats["requests"] == len(models) and stats["rejected"] == 0
+    byreq = {r.request: r for r in results}
+    for q in (0, 5):
+        o = Oracle(models[q], MIXED)
+        o.step(steps)
+        fo = o.final()
+        assert np.abs(fo["slipX"]).max() > 0, "the request must slip"
+        for k in fo:
+            np.testing.assert_array_equal(byreq[q].final[k], fo[k], err_msg=f"request {q} {k}")
+        o.close()

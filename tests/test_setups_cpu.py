@@ -12,7 +12,8 @@ import pytest
 from fd3d_tsn_b200 import configs
 from oracle.oracle import F64, Oracle
 
-REF_EXAMPLES = "/root/reference/examples"
+# the reference's examples/ directory (input decks), when a copy is at hand
+REF_EXAMPLES = os.environ.get("FD3D_REFERENCE_EXAMPLES", "")
 
 
 def write_sw_scec(path, no0, hx0, hz0, hdelta, T0, T0n, sn, mus, muso, mud, d0h):
@@ -100,7 +101,8 @@ def test_fvw_setups_nucleate(tmp_path, variant):
     assert o.plane("T0X").max() > 40e6
 
 
-@pytest.mark.skipif(not os.path.isdir(REF_EXAMPLES), reason="reference examples not present")
+@pytest.mark.skipif(not (REF_EXAMPLES and os.path.isdir(REF_EXAMPLES)),
+                    reason="FD3D_REFERENCE_EXAMPLES does not name the reference's examples directory")
 @pytest.mark.parametrize("deck,setup", [("TPV5", "TPV5"), ("TPV9", "TPV9"), ("TPV104", "TPV104")])
 def test_reference_example_decks_build(deck, setup):
     m = configs.reference_example(os.path.join(REF_EXAMPLES, deck), setup)
@@ -137,7 +139,8 @@ def test_inversion_deck_reads_control_points(tmp_path):
     assert np.abs(o.plane("T0Z")).max() > 0 and np.all(o.plane("T0X") == 0)
 
 
-@pytest.mark.skipif(not os.path.isdir(REF_EXAMPLES), reason="reference examples not present")
+@pytest.mark.skipif(not (REF_EXAMPLES and os.path.isdir(REF_EXAMPLES)),
+                    reason="FD3D_REFERENCE_EXAMPLES does not name the reference's examples directory")
 def test_reference_inversion_example_reads():
     m = configs.inversion_example(os.path.join(REF_EXAMPLES, "Amatrice2016"), dipslip=True)
     fm = m["fault_model"]
