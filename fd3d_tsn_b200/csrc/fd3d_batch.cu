@@ -247,7 +247,7 @@ __global__ void __launch_bounds__(256) k_bint(const ModelDev* __restrict__ model
 }
 
 template <bool STRESS>
-__global__ void __launch_bounds__(PML_TILE, 4) k_bpml(const ModelDev* __restrict__ models,
+__global__ void __launch_bounds__(PML_TILE, STRESS ? 3 : 4) k_bpml(const ModelDev* __restrict__ models,
                                                       const Work* __restrict__ work, int b0,
                                                       const int* __restrict__ limit, const int* run_step,
                                                       int* gstatus) {
@@ -483,7 +483,7 @@ void build_model_items(Model& M, int m, int kch) {
     const int fx = (std::max(nxT, p.nxt) + 31) / 32, fz = (nzT + 7) / 8;
     for (int y = 0; y < fz; ++y)
         for (int x = 0; x < fx; ++x) per[0].push_back(Work{tm | W_VEL_FAULT, x, y, 0});
-    const int npml = (int)((M.dev.D.cum[PML_MAXS] + 255) / 256);
+    const int npml = (int)((M.dev.D.cum[PML_MAXS] + PML_TILE - 1) / PML_TILE);
     for (int x = 0; x < npml; ++x) {
         per[0].push_back(Work{tm | W_VEL_PML, x, 0, 0});
         per[2].push_back(Work{tm | W_STR_PML, x, 0, 0});
@@ -917,6 +917,7 @@ int fd3d_batch_add(fd3d_batch* b, const fd3d_params* pin, const double* lam_k, c
     d.law = M.p.law;
     std::vector<Damp<float>> prof;
     make_pml<float>(M.p, d.D, prof);
+    if (!pml_modes_hold(d.D, prof)) return FD3D_ERR_ARG;
     M.bytes = model_bytes(M.p, d.g, d.D, (int)prof.size(), M.nf, M.cap);
     if (!b->arena.alloc(M.bytes, &M.off)) return FD3D_ERR_NOMEM;
     Bump bp{b->arena_base + M.off};

@@ -156,7 +156,7 @@ struct CtxBase {
     int overlap = 1;
     float last_ms = 0.f;
     bool profiling = false;
-    int pml_minb_vel = 1, pml_minb_str = 4;  // register caps of the PML sweeps (CTAs per SM)
+    int pml_minb_vel = 1, pml_minb_str = 3;  // register caps of the PML sweeps (CTAs per SM; 3 keeps the stress sweep unspilled)
     std::vector<cudaEvent_t> kev;   // 2 per kernel id
     float ktimes[FD3D_NKERNELS] = {0};
     int klaunch[FD3D_NKERNELS] = {0};
@@ -253,6 +253,7 @@ struct Ctx : CtxBase {
         nf = (law == FD3D_LAW_FVW) ? 5 : 4;
         std::vector<Damp<T>> prof;
         make_pml<T>(p, D, prof);
+        if (!pml_modes_hold(D, prof)) return FD3D_ERR_ARG;
         const int stride = std::max(1, p.history_stride);
         p.history_stride = stride;
         const long long plane = (long long)(p.nxt - 2 * p.nabc) * (p.nzt - p.nfs - p.nabc);

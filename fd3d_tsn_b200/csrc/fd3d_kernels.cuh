@@ -154,18 +154,20 @@ __device__ __forceinline__ void vel_fault_body(Grid g, Fields<T> f, Fault<T> q, 
 constexpr int PML_MAXS = 5;  // strips 1-4, and 5 (the top) under FSPACE
 struct PmlDesc {
     Strip s[PML_MAXS];
-    long long cum[PML_MAXS + 1];  // cumulative cell counts of the u/w loop ranges (an absent strip adds 0)
+    long long cum[PML_MAXS + 1];  // first compact index of each strip (a multiple of PML_TILE); cum[PML_MAXS] = end
+    long long cnt[PML_MAXS];      // cells of each strip's u/w loop range (0 for an absent strip)
     int ns;                       // strips present: 4, or 5 under FSPACE
 };
 
 // PML auxiliary components (the 24 split fields that init_pml allocates per strip,
 // fd3d_deriv.f90:1330-1406, 1413-1437) are indexed by the compact cell index t of the
-// u/w loop ranges of the strips (strip s holds t in [cum[s], cum[s+1])) and stored in blocks
-// of 32 cells: inside a block the 32 values of one component are contiguous and the
+// u/w loop ranges of the strips (strip s holds t in [cum[s], cum[s] + cnt[s]); each strip
+// starts on a PML_TILE boundary, so every tile lies in one strip) and stored in blocks of
+// 32 cells: inside a block the 32 values of one component are contiguous and the
 // components of a group follow each other.  The velocity group (u,v,w splits, 9
 // components) and the stress group (xx,yy,zz,xy,xz,yz splits, 15) are separate spans,
 // so the auxiliaries of PML_TILE consecutive cells are one contiguous range per group:
-// one bulk copy brings a tile's range into shared memory and one writes it back.
+// one bulk copy brings a tile's range into shared memory.
 constexpr int AUX_NV = 9, AUX_NS = 15;
 constexpr int PML_TILE = 256;
 inline long long pml_aux_cells(const PmlDesc& D) { return (D.cum[PML_MAXS] + PML_TILE - 1) / PML_TILE * PML_TILE; }
@@ -179,12 +181,27 @@ struct alignas(4 * sizeof(T)) Damp {
     T m, p, r, o;  // 1 - omega, 1 + omega, RN(1/(1 + omega)), omega
 };
 
-// p_new = (p*(1-omega) + inc) / (1+omega) of one split component.  Where omega is 0 the
-// general form gives p + inc exactly (a*1 = a, x/1 = x), so that form is selected there
-// (a warp-vote branch instead measured no faster, and slower in the batch kernel).
-template <class T>
-__device__ __forceinline__ T pml_split(T p, T inc, const Damp<T>& o) {
-    return (o.o == (T)0) ? p + inc : div_pre(p * o.m + inc, o.p, o.r);
+// Damping of one split direction over a strip, from where init_pml leaves the profiles
+// zero (fd3d_deriv.f90:1436-1490): the x strips are damped in x only, the y strip in y
+// and, in its corners, in x; the z strips in z and, in their corners and edges, in x and
+// y.  SPLIT_NEVER: omega = 0 over the whole strip, the update is p + inc.  SPLIT_ALWAYS:
+// the general form (p*(1-omega) + inc)/(1+omega), which is also exact where omega = 0
+// (a*1 = a, x/1 = x).  SPLIT_MAYBE: the general form where any lane of the warp is
+// damped, p + inc where none is (a warp-uniform branch, so no lane forms a quotient it
+// discards).  The host checks the SPLIT_NEVER directions against the profiles
+// (pml_modes_hold).
+enum { SPLIT_NEVER = 0, SPLIT_MAYBE = 1, SPLIT_ALWAYS = 2 };
+// strip class: 0 the x strips (1, 2), 1 the y strip (3), 2 the z strips (4, and 5 under FSPACE)
+__host__ __device__ constexpr int pml_class(int s) { return s <= 1 ? 0 : (s == 2 ? 1 : 2); }
+// mode of direction DIR (0 x, 1 y, 2 z) in strip class C
+__host__ __device__ constexpr int split_mode(int C, int DIR) {
+    return DIR == C ? SPLIT_ALWAYS : (DIR < C ? SPLIT_MAYBE : SPLIT_NEVER);
+}
+
+template <class T, int MODE>
+__device__ __forceinline__ T pml_split(T p, T inc, const Damp<T>& o, bool warp_damped) {
+    if (MODE == SPLIT_NEVER || (MODE == SPLIT_MAYBE && !warp_damped)) return p + inc;
+    return div_pre(p * o.m + inc, o.p, o.r);
 }
 
 template <class T>
@@ -204,13 +221,18 @@ inline void pml_aux_bind(PmlAux<T>& X, T* pool, const PmlDesc& D) {
 // shared-memory slot of component c of the cell that thread l of a tile owns
 __device__ __forceinline__ int aux_sm(int l, int ncomp, int c) { return (l >> 5) * 32 * ncomp + 32 * c + (l & 31); }
 
-// locate strip and (i,j,k) of compact cell index t (u/w loop range of every strip)
-__device__ __forceinline__ bool pml_locate(const PmlDesc& D, long long t, int& s, int& i, int& j, int& k) {
-    if (t >= D.cum[PML_MAXS]) return false;
-    s = (t >= D.cum[1]) + (t >= D.cum[2]) + (t >= D.cum[3]) + (t >= D.cum[4]);
+// strip of the tile that starts at compact index t0
+__device__ __forceinline__ int pml_tile_strip(const PmlDesc& D, long long t0) {
+    return (t0 >= D.cum[1]) + (t0 >= D.cum[2]) + (t0 >= D.cum[3]) + (t0 >= D.cum[4]);
+}
+
+// (i,j,k) of compact cell index t of strip s; false past the strip's last cell
+__device__ __forceinline__ bool pml_cell(const PmlDesc& D, int s, long long t, int& i, int& j, int& k) {
+    const long long r0 = t - D.cum[s];
+    if (r0 >= D.cnt[s]) return false;
     const Strip& S = D.s[s];
     // strip-local index fits 32 bits (a strip is ni*nj*nk cells)
-    unsigned r = (unsigned)(t - D.cum[s]);
+    const unsigned r = (unsigned)r0;
     const unsigned ni = (unsigned)S.ni, nj = (unsigned)(S.jend_uw - S.nyb + 1);
     unsigned q1, k2, ri, rj;
     if (S.fastdiv) {
@@ -239,7 +261,8 @@ __device__ __forceinline__ void pml_tile_begin(T* sm, const T* src, int ncomp, u
     }
 }
 // Wait (bounded) for the tile's load; false on every thread if any thread gave up
-// (ST_TIMEOUT recorded after one more bounded wait for the copy in flight).
+// (ST_TIMEOUT recorded after one more bounded wait for the copy in flight).  Every
+// thread of the CTA leaves it converged.
 __device__ __forceinline__ bool pml_tile_wait(uint32_t bar, uint32_t parity, int* status) {
     const bool ok = mbar_wait(bar, parity);
     if (__syncthreads_or(!ok)) {
@@ -249,19 +272,18 @@ __device__ __forceinline__ bool pml_tile_wait(uint32_t bar, uint32_t parity, int
     }
     return true;
 }
-// pml_uvw: split-field PML velocity in the strips (fd3d_deriv.f90:1927-2293), one
-// tile of PML_TILE consecutive cells per CTA of PML_TILE threads.  Returns false if the
-// staging copy timed out.
-template <class T>
-__device__ __forceinline__ bool vel_pml_tile(const Grid& g, const Fields<T>& f, const PmlDesc& D, const PmlAux<T>& X,
-                                             const StepConst<T>& c, int tile, T* sm, uint32_t bar, uint32_t parity,
-                                             int* status) {
+
+// pml_uvw in one tile of strip class C (fd3d_deriv.f90:1927-2293): one cell per thread.
+template <class T, int C>
+__device__ __forceinline__ bool vel_pml_tile_c(const Grid& g, const Fields<T>& f, const PmlDesc& D,
+                                               const PmlAux<T>& X, const StepConst<T>& c, int s, long long t0, T* sm,
+                                               uint32_t bar, uint32_t parity, int* status) {
+    constexpr int MX = split_mode(C, 0), MY = split_mode(C, 1), MZ = split_mode(C, 2);
     const int l = threadIdx.y * blockDim.x + threadIdx.x;
-    const long long t0 = (long long)tile * PML_TILE;
     T* gaux = X.vel + t0 * AUX_NV;
     pml_tile_begin(sm, gaux, AUX_NV, bar);
-    int s = 0, i = 0, j = 0, k = 0;
-    const bool act = pml_locate(D, t0 + l, s, i, j, k);
+    int i = 0, j = 0, k = 0;
+    const bool act = pml_cell(D, s, t0 + l, i, j, k);
     T d = 1, rl = 0, xx0 = 0, xx1 = 0, xy0 = 0, xy1 = 0, xz0 = 0, xz1 = 0, xz2 = 0, yz0 = 0, yz1 = 0, zz0 = 0, zz1 = 0;
     T xy2 = 0, yy0 = 0, yy1 = 0, yz2 = 0, vold = 0;
     Damp<T> ox{}, oxS{}, oy{}, oz{};
@@ -270,9 +292,9 @@ __device__ __forceinline__ bool vel_pml_tile(const Grid& g, const Fields<T>& f, 
     const long long sy = g.px, sz = g.plane;
     if (act) {  // field loads overlap the staging copy
         const Strip& S = D.s[s];
-        const int i2 = i - S.nxb, j2 = j - S.nyb, k2 = k - S.nzb;
-        ox = X.prof[S.ox_off + i2]; oxS = X.prof[S.oxS_off + i2];
-        oy = X.prof[S.oy_off + j2]; oz = X.prof[S.oz_off + k2];
+        if (MX != SPLIT_NEVER) { ox = X.prof[S.ox_off + i - S.nxb]; oxS = X.prof[S.oxS_off + i - S.nxb]; }
+        if (MY != SPLIT_NEVER) oy = X.prof[S.oy_off + j - S.nyb];
+        if (MZ != SPLIT_NEVER) oz = X.prof[S.oz_off + k - S.nzb];
         p = g.at(i, j, k);
         dov = (j <= S.nye);
         if (f.lay) rl = f.lay[4 * g.nzt + k - 1];  // dt/d of the plane (1-D medium)
@@ -285,38 +307,51 @@ __device__ __forceinline__ bool vel_pml_tile(const Grid& g, const Fields<T>& f, 
         }
     }
     if (!pml_tile_wait(bar, parity, status)) return false;
+    // warp-uniform: does any cell of this warp lie where the direction is damped?
+    const bool wx = MX == SPLIT_MAYBE && __any_sync(0xffffffffu, ox.o != (T)0 || oxS.o != (T)0);
+    const bool wy = MY == SPLIT_MAYBE && __any_sync(0xffffffffu, oy.o != (T)0);
     if (act) {
         const T dt = c.dt, dh = c.dh, rdh = c.rdh;
         const T r = f.lay ? rl : dt / d;
-        // p = (p*(1 - omega) + (dt/d)*diff/dh) / (1 + omega), every division rounded as IEEE
-        // Where omega is 0 (most split directions of a strip) a*(1-0) = a and x/(1+0) = x
-        // exactly, so the branch skips a multiply and a division without changing a bit.
+        // p = (p*(1 - omega) + (dt/d)*diff/dh) / (1 + omega), every division rounded as IEEE.
         // The result goes straight back to the component's global slot (one coalesced
         // 128-byte row per warp and component), so no bulk store has to drain.
-        auto upd = [&](int comp, const Damp<T>& o, T diff) {
-            const int q = aux_sm(l, AUX_NV, comp);
-            const T inc = div_pre(r * diff, dh, rdh);
-            const T a = pml_split(sm[q], inc, o);
-            gaux[q] = a;
-            return a;
-        };
-        const T u0 = upd(AX_U0, ox, xx0 - xx1);
-        const T u1 = upd(AX_U1, oy, xy0 - xy1);
-        const T u2 = upd(AX_U2, oz, xz0 - xz1);
-        const T w0 = upd(AX_W0, oxS, xz2 - xz0);
-        const T w1 = upd(AX_W1, oy, yz0 - yz1);
-        const T w2 = upd(AX_W2, oz, zz1 - zz0);
+        auto inc = [&](T diff) { return div_pre(r * diff, dh, rdh); };
+        auto put = [&](int comp, T a) { gaux[aux_sm(l, AUX_NV, comp)] = a; return a; };
+        auto aux = [&](int comp) { return sm[aux_sm(l, AUX_NV, comp)]; };
+        const T u0 = put(AX_U0, pml_split<T, MX>(aux(AX_U0), inc(xx0 - xx1), ox, wx));
+        const T u1 = put(AX_U1, pml_split<T, MY>(aux(AX_U1), inc(xy0 - xy1), oy, wy));
+        const T u2 = put(AX_U2, pml_split<T, MZ>(aux(AX_U2), inc(xz0 - xz1), oz, false));
+        const T w0 = put(AX_W0, pml_split<T, MX>(aux(AX_W0), inc(xz2 - xz0), oxS, wx));
+        const T w1 = put(AX_W1, pml_split<T, MY>(aux(AX_W1), inc(yz0 - yz1), oy, wy));
+        const T w2 = put(AX_W2, pml_split<T, MZ>(aux(AX_W2), inc(zz1 - zz0), oz, false));
         f.u[p] = u0 + u1 + u2;
         f.w[p] = w0 + w1 + w2;
         if (dov) {
-            const T v0 = upd(AX_V0, oxS, xy2 - xy0);
-            const T v1 = upd(AX_V1, oy, yy0 - yy1);
-            const T v2 = upd(AX_V2, oz, yz0 - yz2);
+            const T v0 = put(AX_V0, pml_split<T, MX>(aux(AX_V0), inc(xy2 - xy0), oxS, wx));
+            const T v1 = put(AX_V1, pml_split<T, MY>(aux(AX_V1), inc(yy0 - yy1), oy, wy));
+            const T v2 = put(AX_V2, pml_split<T, MZ>(aux(AX_V2), inc(yz0 - yz2), oz, false));
             if (j == g.nyt - 1) f.v[p + sy] = vold;  // bnd2d mirror of the value before this update
             f.v[p] = v0 + v1 + v2;
         }
     }
     return true;
+}
+
+// pml_uvw: split-field PML velocity in the strips (fd3d_deriv.f90:1927-2293), one
+// tile of PML_TILE consecutive cells per CTA of PML_TILE threads.  Returns false if the
+// staging copy timed out.
+template <class T>
+__device__ __forceinline__ bool vel_pml_tile(const Grid& g, const Fields<T>& f, const PmlDesc& D, const PmlAux<T>& X,
+                                             const StepConst<T>& c, int tile, T* sm, uint32_t bar, uint32_t parity,
+                                             int* status) {
+    const long long t0 = (long long)tile * PML_TILE;
+    const int s = pml_tile_strip(D, t0);
+    switch (pml_class(s)) {
+        case 0: return vel_pml_tile_c<T, 0>(g, f, D, X, c, s, t0, sm, bar, parity, status);
+        case 1: return vel_pml_tile_c<T, 1>(g, f, D, X, c, s, t0, sm, bar, parity, status);
+        default: return vel_pml_tile_c<T, 2>(g, f, D, X, c, s, t0, sm, bar, parity, status);
+    }
 }
 
 // fuvw at the ghost row k=ks+1 (fd3d_deriv.f90:1018-1062).  w needs u and v of the
@@ -442,27 +477,34 @@ __device__ __forceinline__ void str_fault_body(Grid g, Fields<T> f, Fault<T> q, 
     }
 }
 
-// pml_xyz in the strips (fd3d_deriv.f90:2304-3143), one tile per CTA as vel_pml_tile
-template <class T>
-__device__ __forceinline__ bool str_pml_tile(const Grid& g, const Fields<T>& f, const PmlDesc& D, const PmlAux<T>& X,
-                                             const StepConst<T>& c, int tile, T* sm, uint32_t bar, uint32_t parity,
-                                             int* status) {
+// pml_xyz in one tile of strip class C (fd3d_deriv.f90:2304-3143), as vel_pml_tile_c
+template <class T, int C>
+__device__ __forceinline__ bool str_pml_tile_c(const Grid& g, const Fields<T>& f, const PmlDesc& D,
+                                               const PmlAux<T>& X, const StepConst<T>& c, int s, long long t0, T* sm,
+                                               uint32_t bar, uint32_t parity, int* status) {
+    constexpr int MX = split_mode(C, 0), MY = split_mode(C, 1), MZ = split_mode(C, 2);
     const int l = threadIdx.y * blockDim.x + threadIdx.x;
-    const long long t0 = (long long)tile * PML_TILE;
     T* gaux = X.str + t0 * AUX_NS;
     pml_tile_begin(sm, gaux, AUX_NS, bar);
-    int s = 0, i = 0, j = 0, k = 0;
-    const bool act = pml_locate(D, t0 + l, s, i, j, k);
+    int i = 0, j = 0, k = 0;
+    const bool act = pml_cell(D, s, t0 + l, i, j, k);
     long long p = 0;
     bool dxy = false, top = false;
     const long long sy = g.px, sz = g.plane;
     T xl = 0, xm = 0, mz = 0, up = 0, ux = 0, uz = 0, vp = 0, vy = 0, wp = 0, wz = 0, wx = 0;
     T my = 0, md = 0, uy = 0, vx = 0, vz = 0, wy = 0, xyo = 0, yzo = 0;
+    // xy and yz take omegayS in strips 3-5 and xz, yz omegazS in strips 4-5; in the other
+    // strips those directions are undamped (SPLIT_NEVER), so oyS / ozS serve every class
+    Damp<T> ox{}, oxS{}, oy{}, oyS{}, oz{}, ozS{};
     if (act) {  // field loads overlap the staging copy
         const Strip& S = D.s[s];
+        const int i2 = i - S.nxb, j2 = j - S.nyb, k2 = k - S.nzb;
+        if (MX != SPLIT_NEVER) { ox = X.prof[S.ox_off + i2]; oxS = X.prof[S.oxS_off + i2]; }
+        if (MY != SPLIT_NEVER) { oy = X.prof[S.oy_off + j2]; oyS = X.prof[S.oyS_off + j2]; }
+        if (MZ != SPLIT_NEVER) { oz = X.prof[S.oz_off + k2]; ozS = X.prof[S.ozS_off + k2]; }
         p = g.at(i, j, k);
         dxy = (j <= S.nye);
-        top = !g.fspace && (s <= 2) && (k == S.nze);  // xz/yz aux zeroed at the top row, strips 1-3 (not FSPACE)
+        top = !g.fspace && (C <= 1) && (k == S.nze);  // xz/yz aux zeroed at the top row, strips 1-3 (not FSPACE)
         if (f.lay) {  // 1-D medium: mu(i,j+1,k) = mu(i,j,k), mu(i+1,j+1,k+1) = mu(i,j,k+1)
             xl = f.lay[k - 1]; xm = f.lay[g.nzt + k - 1]; mz = f.lay[g.nzt + k];
         } else {
@@ -479,59 +521,63 @@ __device__ __forceinline__ bool str_pml_tile(const Grid& g, const Fields<T>& f, 
         }
     }
     if (!pml_tile_wait(bar, parity, status)) return false;
+    const bool dx = MX == SPLIT_MAYBE && __any_sync(0xffffffffu, ox.o != (T)0 || oxS.o != (T)0);
+    const bool dy = MY == SPLIT_MAYBE && __any_sync(0xffffffffu, oy.o != (T)0 || oyS.o != (T)0);
     if (act) {
-        const Strip& S = D.s[s];
-        const int i2 = i - S.nxb, j2 = j - S.nyb, k2 = k - S.nzb;
-        const Damp<T> ox = X.prof[S.ox_off + i2], oxS = X.prof[S.oxS_off + i2];
-        const Damp<T> oy = X.prof[S.oy_off + j2], oz = X.prof[S.oz_off + k2];
-        // xy, yz use omegayS in strips 3-5; xz, yz use omegazS in strips 4, 5
-        const Damp<T> oyxy = X.prof[(s >= 2 ? S.oyS_off : S.oy_off) + j2];
-        const Damp<T> ozxz = X.prof[(s >= 3 ? S.ozS_off : S.oz_off) + k2];
         const T dt = c.dt, dh = c.dh, rdh = c.rdh;
         const T a = xl + (T)2 * xm, b = xl;
         const T diff1 = ux - up, diff2 = vp - vy, diff3 = wp - wz;
         // p = (p*(1 - omega) + dt*modulus*diff/dh) / (1 + omega), every division rounded as IEEE
-        // omega = 0: exact shortcut as in vel_pml_tile
-        auto upd = [&](int comp, const Damp<T>& o, T mod, T diff) {
-            const int q = aux_sm(l, AUX_NS, comp - AUX_NV);
-            const T inc = div_pre(dt * mod * diff, dh, rdh);
-            const T pa = pml_split(sm[q], inc, o);
-            gaux[q] = pa;
-            return pa;
-        };
-        const T x0 = upd(AX_XX0, oxS, a, diff1);
-        const T x1 = upd(AX_XX1, oy, b, diff2);
-        const T x2 = upd(AX_XX2, oz, b, diff3);
+        auto inc = [&](T mod, T diff) { return div_pre(dt * mod * diff, dh, rdh); };
+        auto aux = [&](int comp) { return sm[aux_sm(l, AUX_NS, comp - AUX_NV)]; };
+        auto put = [&](int comp, T v) { gaux[aux_sm(l, AUX_NS, comp - AUX_NV)] = v; return v; };
+        const T x0 = put(AX_XX0, pml_split<T, MX>(aux(AX_XX0), inc(a, diff1), oxS, dx));
+        const T x1 = put(AX_XX1, pml_split<T, MY>(aux(AX_XX1), inc(b, diff2), oy, dy));
+        const T x2 = put(AX_XX2, pml_split<T, MZ>(aux(AX_XX2), inc(b, diff3), oz, false));
         f.xx[p] = x0 + x1 + x2;
-        const T y0 = upd(AX_YY0, oxS, b, diff1);
-        const T y1 = upd(AX_YY1, oy, a, diff2);
-        const T y2 = upd(AX_YY2, oz, b, diff3);
+        const T y0 = put(AX_YY0, pml_split<T, MX>(aux(AX_YY0), inc(b, diff1), oxS, dx));
+        const T y1 = put(AX_YY1, pml_split<T, MY>(aux(AX_YY1), inc(a, diff2), oy, dy));
+        const T y2 = put(AX_YY2, pml_split<T, MZ>(aux(AX_YY2), inc(b, diff3), oz, false));
         f.yy[p] = y0 + y1 + y2;
-        const T z0 = upd(AX_ZZ0, oxS, b, diff1);
-        const T z1 = upd(AX_ZZ1, oy, b, diff2);
-        const T z2 = upd(AX_ZZ2, oz, a, diff3);
+        const T z0 = put(AX_ZZ0, pml_split<T, MX>(aux(AX_ZZ0), inc(b, diff1), oxS, dx));
+        const T z1 = put(AX_ZZ1, pml_split<T, MY>(aux(AX_ZZ1), inc(b, diff2), oy, dy));
+        const T z2 = put(AX_ZZ2, pml_split<T, MZ>(aux(AX_ZZ2), inc(a, diff3), oz, false));
         f.zz[p] = z0 + z1 + z2;
         {   // xz (j up to jend_uw)
             const T xmu = (xm + mz) / (T)2;
-            const T q0 = upd(AX_XZ0, ozxz, xmu, uz - up);
-            const T q1 = upd(AX_XZ1, ox, xmu, wp - wx);
+            const T q0 = put(AX_XZ0, pml_split<T, MZ>(aux(AX_XZ0), inc(xmu, uz - up), ozS, false));
+            const T q1 = put(AX_XZ1, pml_split<T, MX>(aux(AX_XZ1), inc(xmu, wp - wx), ox, dx));
             f.xz[p] = q0 + q1;
-            if (top) { gaux[aux_sm(l, AUX_NS, AX_XZ0 - AUX_NV)] = (T)0; gaux[aux_sm(l, AUX_NS, AX_XZ1 - AUX_NV)] = (T)0; }
+            if (top) { put(AX_XZ0, (T)0); put(AX_XZ1, (T)0); }
         }
         if (dxy) {
             T xmu = (xm + my) / (T)2;
-            const T e0 = upd(AX_XY0, oyxy, xmu, uy - up);
-            const T e1 = upd(AX_XY1, ox, xmu, vp - vx);
+            const T e0 = put(AX_XY0, pml_split<T, MY>(aux(AX_XY0), inc(xmu, uy - up), oyS, dy));
+            const T e1 = put(AX_XY1, pml_split<T, MX>(aux(AX_XY1), inc(xmu, vp - vx), ox, dx));
             xmu = (xm + md) / (T)2;
-            const T h0 = upd(AX_YZ0, ozxz, xmu, vz - vp);
-            const T h1 = upd(AX_YZ1, oyxy, xmu, wy - wp);
+            const T h0 = put(AX_YZ0, pml_split<T, MZ>(aux(AX_YZ0), inc(xmu, vz - vp), ozS, false));
+            const T h1 = put(AX_YZ1, pml_split<T, MY>(aux(AX_YZ1), inc(xmu, wy - wp), oyS, dy));
             if (j == g.nyt - 1) { f.xy[p + sy] = xyo; f.yz[p + sy] = yzo; }  // strbnd mirror
             f.xy[p] = e0 + e1;
             f.yz[p] = h0 + h1;
-            if (top) { gaux[aux_sm(l, AUX_NS, AX_YZ0 - AUX_NV)] = (T)0; gaux[aux_sm(l, AUX_NS, AX_YZ1 - AUX_NV)] = (T)0; }
+            if (top) { put(AX_YZ0, (T)0); put(AX_YZ1, (T)0); }
         }
     }
     return true;
+}
+
+// pml_xyz in the strips (fd3d_deriv.f90:2304-3143), one tile per CTA as vel_pml_tile
+template <class T>
+__device__ __forceinline__ bool str_pml_tile(const Grid& g, const Fields<T>& f, const PmlDesc& D, const PmlAux<T>& X,
+                                             const StepConst<T>& c, int tile, T* sm, uint32_t bar, uint32_t parity,
+                                             int* status) {
+    const long long t0 = (long long)tile * PML_TILE;
+    const int s = pml_tile_strip(D, t0);
+    switch (pml_class(s)) {
+        case 0: return str_pml_tile_c<T, 0>(g, f, D, X, c, s, t0, sm, bar, parity, status);
+        case 1: return str_pml_tile_c<T, 1>(g, f, D, X, c, s, t0, sm, bar, parity, status);
+        default: return str_pml_tile_c<T, 2>(g, f, D, X, c, s, t0, sm, bar, parity, status);
+    }
 }
 
 // fres (fd3d_deriv.f90:1067-1104)

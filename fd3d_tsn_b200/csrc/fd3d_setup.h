@@ -57,6 +57,7 @@ void make_pml(const fd3d_params& p, PmlDesc& D, std::vector<Damp<T>>& prof) {
         if (s >= D.ns) {  // absent strip: empty range
             D.s[s] = D.s[s - 1];
             D.s[s].ncells = 0;
+            D.cnt[s] = 0;
             D.cum[s + 1] = D.cum[s];
             continue;
         }
@@ -67,10 +68,12 @@ void make_pml(const fd3d_params& p, PmlDesc& D, std::vector<Damp<T>>& prof) {
         S.ncells = (long long)S.ni * S.nj1 * S.nk;
         S.base = base;
         base += S.ncells;
-        D.cum[s + 1] = D.cum[s] + (long long)S.ni * (S.jend_uw - S.nyb + 1) * S.nk;
+        // every strip starts on a tile boundary, so a tile's cells share a strip
+        D.cnt[s] = (long long)S.ni * (S.jend_uw - S.nyb + 1) * S.nk;
+        D.cum[s + 1] = D.cum[s] + (D.cnt[s] + PML_TILE - 1) / PML_TILE * PML_TILE;
         S.rni = 1.0f / (float)S.ni;
         S.rnj = 1.0f / (float)(S.jend_uw - S.nyb + 1);
-        S.fastdiv = (D.cum[s + 1] - D.cum[s]) < (1LL << 24);
+        S.fastdiv = D.cnt[s] < (1LL << 24);
         ox[s].assign(S.ni, (T)0); oxS[s].assign(S.ni, (T)0);
         oy[s].assign(S.nj1, (T)0); oyS[s].assign(S.nj1, (T)0);
         oz[s].assign(S.nk, (T)0); ozS[s].assign(S.nk, (T)0);
@@ -120,6 +123,26 @@ void make_pml(const fd3d_params& p, PmlDesc& D, std::vector<Damp<T>>& prof) {
         S.oy_off = put(oy[s]); S.oyS_off = put(oyS[s]);
         S.oz_off = put(oz[s]); S.ozS_off = put(ozS[s]);
     }
+}
+
+// The PML sweeps update a split direction as p + inc where its strip class says the
+// direction is never damped (split_mode, fd3d_kernels.cuh); that is exact only if every
+// omega of that direction's profiles is zero over the strip.  Checked once per set-up.
+template <class T>
+bool pml_modes_hold(const PmlDesc& D, const std::vector<Damp<T>>& prof) {
+    for (int s = 0; s < D.ns; ++s) {
+        const Strip& S = D.s[s];
+        const int C = pml_class(s);
+        const int offs[3][2] = {{S.ox_off, S.oxS_off}, {S.oy_off, S.oyS_off}, {S.oz_off, S.ozS_off}};
+        const int len[3] = {S.ni, S.nj1, S.nk};
+        for (int dir = 0; dir < 3; ++dir) {
+            if (split_mode(C, dir) != SPLIT_NEVER) continue;
+            for (int v = 0; v < 2; ++v)
+                for (int q = 0; q < len[dir]; ++q)
+                    if (prof[(size_t)offs[dir][v] + q].o != (T)0) return false;
+        }
+    }
+    return true;
 }
 
 template <class T>
