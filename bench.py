@@ -313,7 +313,9 @@ def run_b200(args, world, rank, local, pg):
 
 
 def gpu_launches(m, steps):
-    per_step = 11 + (1 if m.get("law") == "fvw" and m["fault"].get("nucleation") else 0)
+    # vel interior, fault band, PML, free surface; stress interior, fault band, PML; fres +
+    # fault boundary condition (one fused launch); the nucleation ramp of rate-and-state runs
+    per_step = 8 - (1 if m.get("fspace") else 0) + (1 if m.get("law") == "fvw" and m["fault"].get("nucleation") else 0)
     return per_step * steps
 
 

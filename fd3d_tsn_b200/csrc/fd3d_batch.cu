@@ -5,12 +5,13 @@
 // items.  Two schedules run it: the persistent one is one cooperative kernel per run
 // whose CTAs walk the items phase by phase and meet at a bounded grid-wide barrier
 // between phases; the graph one replays CUDA graphs of per-region kernels over all
-// models (see k_bint).  A time step has seven phases:
+// models (see k_bint).  A time step has five phases:
 //   0 velocity: interior tiles, fault band + fault plane, PML chunks
 //   1 free-surface velocity ghosts
 //   2 stress: interior tiles, fault band + fault plane, PML chunks
-//   3 free-surface stress ghosts
-//   4 trial traction   5 friction   6 output planes (+ nucleation ramp)
+//   3 fault boundary condition: free-surface stress ghosts and the fused trial traction,
+//     friction and output tiles (fault_bc_body)
+//   4 nucleation ramp (rate-and-state models that have one; an empty phase is skipped)
 // Every item runs the same __device__ body as the single-model launch of that region
 // (fd3d_kernels.cuh / fd3d_opt.cuh), so a model's results do not depend on which other
 // models share the launch.  The schedule, the z-extent of the interior tiles and (for
@@ -51,10 +52,9 @@ using namespace fd3d;
 namespace {
 
 enum WorkType : int {
-    W_VEL_INT = 0, W_VEL_FAULT, W_VEL_PML, W_VEL_FS, W_STR_INT, W_STR_FAULT, W_STR_PML, W_STR_FS,
-    W_TRAC, W_FRIC, W_OUT, W_NUC
+    W_VEL_INT = 0, W_VEL_FAULT, W_VEL_PML, W_VEL_FS, W_STR_INT, W_STR_FAULT, W_STR_PML, W_STR_FS, W_FBC, W_NUC
 };
-constexpr int NPHASE = 7;
+constexpr int NPHASE = 5;
 
 struct Work {
     int tm;          // type | model << 8
@@ -146,6 +146,7 @@ k_batch(const ModelDev* __restrict__ models, const ModelMaps* __restrict__ maps,
     for (int s = 0; s < nsteps; ++s) {
         for (int ph = 0; ph < NPHASE; ++ph) {
             const int b0 = pbeg[ph], b1 = pbeg[ph + 1];
+            if (b0 == b1) continue;  // an empty phase needs no barrier (uniform over the grid)
             for (int w = b0 + blockIdx.x; w < b1; w += nb) {
                 const Work it = work[w];
                 const int m = it.tm >> 8, type = it.tm & 255;
@@ -177,9 +178,10 @@ k_batch(const ModelDev* __restrict__ models, const ModelMaps* __restrict__ maps,
                         ++pt;
                         break;
                     case W_STR_FS: str_fs_body<float>(M.g, M.f, it.bx, it.by, 0); break;
-                    case W_TRAC: traction_body<float>(M.g, M.f, M.q, M.c, it.bx, it.by, 0); break;
-                    case W_FRIC: friction_body<float>(M.g, M.f, M.q, M.c, M.law, M.fs, M.it_dev, it.bx, it.by, 0); break;
-                    case W_OUT: output_body<float>(M.g, M.f, M.q, M.law, M.it_dev, M.h, M.status, it.bx, it.by, 0); break;
+                    case W_FBC:
+                        fault_bc_body<float>(M.g, M.f, M.q, M.c, M.law, M.fs, M.it_dev, M.h, M.status, it.bx, it.by,
+                                             ring);
+                        break;
                     case W_NUC: nucleation_body<float>(M.g, M.q, M.c, M.fs, M.it_dev, it.bx, it.by, 0); break;
                     default: break;
                 }
@@ -218,7 +220,7 @@ __global__ void k_check_grid_barrier(BatchSync* sync, int* status) {
 // order, and k_step_end advances the run's step counter (items of a model whose
 // step limit is reached return at once).  Each kernel gets its own register and
 // shared-memory budget, so each region runs at its own occupancy.
-constexpr int NTYPES = 12;
+constexpr int NTYPES = 10;
 
 __device__ __forceinline__ bool item_live(const Work& it, const int* limit, const int* run_step, int& m) {
     m = it.tm >> 8;
@@ -264,6 +266,7 @@ __global__ void __launch_bounds__(PML_TILE, STRESS ? 3 : 4) k_bpml(const ModelDe
 
 __global__ void __launch_bounds__(256) k_bplane(const ModelDev* __restrict__ models, const Work* __restrict__ work,
                                                 int b0, const int* __restrict__ limit, const int* run_step) {
+    __shared__ float sm[FBC_SMEM];
     const Work it = work[b0 + blockIdx.x];
     int m;
     if (!item_live(it, limit, run_step, m)) return;
@@ -275,9 +278,9 @@ __global__ void __launch_bounds__(256) k_bplane(const ModelDev* __restrict__ mod
         case W_VEL_FS: vel_fs_body<float>(M.g, M.f, it.bx, it.by, 0); break;
         case W_STR_FAULT: str_fault_body<float>(M.g, M.f, M.q, M.c, it.bx, it.by, 0); break;
         case W_STR_FS: str_fs_body<float>(M.g, M.f, it.bx, it.by, 0); break;
-        case W_TRAC: traction_body<float>(M.g, M.f, M.q, M.c, it.bx, it.by, 0); break;
-        case W_FRIC: friction_body<float>(M.g, M.f, M.q, M.c, M.law, M.fs, M.it_dev, it.bx, it.by, 0); break;
-        case W_OUT: output_body<float>(M.g, M.f, M.q, M.law, M.it_dev, M.h, M.status, it.bx, it.by, 0); break;
+        case W_FBC:
+            fault_bc_body<float>(M.g, M.f, M.q, M.c, M.law, M.fs, M.it_dev, M.h, M.status, it.bx, it.by, sm);
+            break;
         case W_NUC: nucleation_body<float>(M.g, M.q, M.c, M.fs, M.it_dev, it.bx, it.by, 0); break;
         default: break;
     }
@@ -375,7 +378,9 @@ struct Bump {  // carve aligned sub-arrays out of one model block
     }
 };
 
-constexpr int NF_PLANES = 37, ND_PLANES = 11;
+// fault planes of a model: NF_PLANES single and NF2_PLANES two-plane float arrays, ND_PLANES
+// single and ND2_PLANES two-plane double arrays (the two-plane state of Fault)
+constexpr int NF_PLANES = 33, NF2_PLANES = 2, ND_PLANES = 10, ND2_PLANES = 1;
 
 size_t model_bytes(const fd3d_params& p, const Grid& g, const PmlDesc& D, int prof_n, int nf, int cap) {
     const size_t n2 = (size_t)p.nxt * p.nzt;
@@ -384,7 +389,9 @@ size_t model_bytes(const fd3d_params& p, const Grid& g, const PmlDesc& D, int pr
     auto add = [&](size_t bytes) { b = ((b + 255) & ~(size_t)255) + bytes; };
     add((size_t)g.n3 * 12 * 4);
     for (int k = 0; k < NF_PLANES; ++k) add(n2 * 4);
+    for (int k = 0; k < NF2_PLANES; ++k) add(2 * n2 * 4);
     for (int k = 0; k < ND_PLANES; ++k) add(n2 * 8);
+    for (int k = 0; k < ND2_PLANES; ++k) add(2 * n2 * 8);
     add(pml_aux_elems(D) * 4);
     add((size_t)prof_n * sizeof(Damp<float>));
     add((size_t)cap * nf * plane * 4);
@@ -496,16 +503,16 @@ void build_model_items(Model& M, int m, int kch) {
         }
     const int px = (nxT + 31) / 32;
     for (int y = 0; y < fz; ++y)
-        for (int x = 0; x < px; ++x) {
-            per[2].push_back(Work{tm | W_STR_FAULT, x, y, 0});
-            per[4].push_back(Work{tm | W_TRAC, x, y, 0});
-            per[5].push_back(Work{tm | W_FRIC, x, y, 0});
-            per[6].push_back(Work{tm | W_OUT, x, y, 0});
-        }
+        for (int x = 0; x < px; ++x) per[2].push_back(Work{tm | W_STR_FAULT, x, y, 0});
+    {   // fused fault BC tiles (fault_bc_body)
+        int nfres, tx, nt;
+        fault_bc_grid(g, nfres, tx, nt);
+        for (int t = 0; t < nt; ++t) per[3].push_back(Work{tm | W_FBC, t % tx, t / tx, 0});
+    }
     if (M.p.law == FD3D_LAW_FVW && M.dev.fs.nucleation) {
         const int ni = (p.nxt - p.nabc) - (p.nabc - 1) + 1, nk = g.ks() - (p.nabc - 1) + 1;
         for (int y = 0; y < (nk + 7) / 8; ++y)
-            for (int x = 0; x < (ni + 31) / 32; ++x) per[6].push_back(Work{tm | W_NUC, x, y, 0});
+            for (int x = 0; x < (ni + 31) / 32; ++x) per[4].push_back(Work{tm | W_NUC, x, y, 0});
     }
     M.items_kchunk = kch;
 }
@@ -637,11 +644,9 @@ int enqueue_graph_step(fd3d_batch* b) {
         BCK(cudaEventRecord(b->evf[2], b->side[1]));
         BCK(cudaStreamWaitEvent(b->st, b->evf[1], 0));
         BCK(cudaStreamWaitEvent(b->st, b->evf[2], 0));
-        plane(b->st, tfs, tfs + 1);
+        plane(b->st, tfs, half ? W_FBC + 1 : tfs + 1);  // after the stresses: fres and the fault BC tiles
     }
-    plane(b->st, W_TRAC, W_TRAC + 1);
-    plane(b->st, W_FRIC, W_FRIC + 1);
-    plane(b->st, W_OUT, W_NUC + 1);  // output and nucleation ramp share a phase
+    plane(b->st, W_NUC, W_NUC + 1);
     k_step_end<<<1, 1, 0, b->st>>>(b->d_run_step);
     BCK(cudaGetLastError());
     return FD3D_OK;
@@ -747,11 +752,14 @@ int reset_model(fd3d_batch* b, Model& M, cudaStream_t st) {
     const size_t n2 = (size_t)M.p.nxt * M.p.nzt;
     ModelDev& d = M.dev;
     BCK(cudaMemsetAsync(d.f.u, 0, (size_t)d.g.n3 * 9 * sizeof(float), st));
-    float* zt[] = {d.q.tx, d.q.tz, d.q.txt, d.q.tzt, d.q.RFx, d.q.RFz, d.q.avdx, d.q.avdz, d.q.v1t, d.q.au1, d.q.av1,
+    float* zt[] = {d.q.tx, d.q.tz, d.q.RFx, d.q.RFz, d.q.v1t, d.q.au1, d.q.av1,
                    d.q.aw1, d.q.uZ, d.q.wX, d.q.schangeX, d.q.schangeZ};
     for (float* a : zt) BCK(cudaMemsetAsync(a, 0, n2 * sizeof(float), st));
-    double* zd[] = {d.q.distX, d.q.distZ, d.q.slipX, d.q.slipZ, d.q.rise};
+    BCK(cudaMemsetAsync(d.q.avdx, 0, 2 * n2 * sizeof(float), st));
+    BCK(cudaMemsetAsync(d.q.avdz, 0, 2 * n2 * sizeof(float), st));
+    double* zd[] = {d.q.distZ, d.q.slipX, d.q.slipZ, d.q.rise};
     for (double* a : zd) BCK(cudaMemsetAsync(a, 0, n2 * sizeof(double), st));
+    BCK(cudaMemsetAsync(d.q.distX, 0, 2 * n2 * sizeof(double), st));
     BCK(cudaMemsetAsync(d.X.vel, 0, pml_aux_elems(d.D) * sizeof(float), st));
     k_model_reset<<<(unsigned)((n2 + 255) / 256), 256, 0, st>>>(d, (int)n2);
     BCK(cudaGetLastError());
@@ -930,15 +938,20 @@ int fd3d_batch_add(fd3d_batch* b, const fd3d_params* pin, const double* lam_k, c
     float* mu = fp + 10 * (size_t)d.g.n3;
     float* dd = fp + 11 * (size_t)d.g.n3;
     d.f.lam = lam; d.f.mu = mu; d.f.d = dd;  // d.f.lay: the layer table, set below
-    float** fq[NF_PLANES] = {&d.q.tx, &d.q.tz, &d.q.txt, &d.q.tzt, &d.q.RFx, &d.q.RFz, &d.q.avdx, &d.q.avdz, &d.q.v1t,
+    float** fq[NF_PLANES] = {&d.q.tx, &d.q.tz, &d.q.RFx, &d.q.RFz, &d.q.v1t,
                              &d.q.au1, &d.q.av1, &d.q.aw1, &d.q.uZ, &d.q.wX, &d.q.tabsX, &d.q.tabsZ, &d.q.T0X,
                              &d.q.T0Z, &d.q.T0Xb, &d.q.Dc, &d.q.peakX, &d.q.dynX, &d.q.DcX, &d.q.peakZ, &d.q.dynZ,
                              &d.q.DcZ, &d.q.coh, &d.q.aX, &d.q.bX, &d.q.vwX, &d.q.fwX, &d.q.aZ, &d.q.bZ, &d.q.vwZ,
                              &d.q.fwZ, &d.q.schangeX, &d.q.schangeZ};
     for (float** a : fq) *a = bp.take<float>(n2);
-    double** dq[ND_PLANES] = {&d.q.psiX, &d.q.psiZ, &d.q.distX, &d.q.distZ, &d.q.slipX, &d.q.slipZ, &d.q.ruptime,
+    float** fq2[NF2_PLANES] = {&d.q.avdx, &d.q.avdz};
+    for (float** a : fq2) *a = bp.take<float>(2 * n2);
+    d.q.txt = d.q.tzt = nullptr;  // the fused fault BC keeps the trial tractions in shared memory
+    double** dq[ND_PLANES] = {&d.q.psiX, &d.q.psiZ, &d.q.distZ, &d.q.slipX, &d.q.slipZ, &d.q.ruptime,
                               &d.q.rise, &d.q.sliptime, &d.psiX0, &d.psiZ0};
     for (double** a : dq) *a = bp.take<double>(n2);
+    d.q.distX = bp.take<double>(2 * n2);
+    d.q.n2 = (int)n2;
     float* aux = bp.take<float>(pml_aux_elems(d.D));
     pml_aux_bind(d.X, aux, d.D);
     Damp<float>* dprof = bp.take<Damp<float>>(prof.size());
@@ -1107,7 +1120,8 @@ int fd3d_batch_fetch_plane(fd3d_batch* b, int slot, int plane, double* host) {
         case FD3D_PLANE_TX: ts = d.q.tx; break;             case FD3D_PLANE_TZ: ts = d.q.tz; break;
         case FD3D_PLANE_SLIPX: ds = d.q.slipX; break;       case FD3D_PLANE_SLIPZ: ds = d.q.slipZ; break;
         case FD3D_PLANE_RUPTIME: ds = d.q.ruptime; break;   case FD3D_PLANE_RISE: ds = d.q.rise; break;
-        case FD3D_PLANE_SLIPTIME: ds = d.q.sliptime; break; case FD3D_PLANE_DISTX: ds = d.q.distX; break;
+        case FD3D_PLANE_SLIPTIME: ds = d.q.sliptime; break;
+        case FD3D_PLANE_DISTX: ds = pp_wr(d.q.distX, M.steps, (int)n2); break;  // the plane of the last step
         case FD3D_PLANE_DISTZ: ds = d.q.distZ; break;       case FD3D_PLANE_PSIX: ds = d.q.psiX; break;
         case FD3D_PLANE_PSIZ: ds = d.q.psiZ; break;         case FD3D_PLANE_T0X: ts = d.q.T0X; break;
         case FD3D_PLANE_T0Z: ts = d.q.T0Z; break;           case FD3D_PLANE_SCHANGEX: ts = d.q.schangeX; break;

@@ -68,11 +68,17 @@ constexpr int LAY_N = 5;  // profile entries per plane
 
 // Fault-plane state.  F = field type, double = accumulators (slip, slip path,
 // rupture time, rise, slip time, psi).
+//
+// avdx, avdz (the damping memory of the trial traction) and distX (the slip path of the
+// X nodes) hold two planes each: step it reads plane (it+1)&1 and writes plane it&1, so
+// the fault boundary condition, which recomputes the trial and post-friction tractions of
+// a tile's neighbouring nodes, never reads a value another CTA is updating.  After n steps
+// the current plane is n&1 (pp_rd / pp_wr below).
 template <class T>
 struct Fault {
     // traction_com
     T *tx, *tz;           // traction after friction (read by next step's fault velocity)
-    T *txt, *tzt;         // trial traction (before friction)
+    T *txt, *tzt;         // trial traction (scratch of the separate-launch fault BC only)
     T *RFx, *RFz, *avdx, *avdz, *v1t, *au1, *av1, *aw1;
     // friction_com
     T *uZ, *wX, *tabsX, *tabsZ, *T0X, *T0Z, *T0Xb, *Dc;
@@ -82,7 +88,14 @@ struct Fault {
     // source_com
     double *distX, *distZ, *slipX, *slipZ, *ruptime, *rise, *sliptime;
     T *schangeX, *schangeZ;  // last step's shear traction / strength planes
+    int n2;                  // nxt*nzt, the size of one plane
 };
+
+// plane of a two-plane state array that step `it` reads / writes
+template <class U>
+__host__ __device__ __forceinline__ U* pp_rd(U* base, int it, int n2) { return base + (size_t)((it + 1) & 1) * n2; }
+template <class U>
+__host__ __device__ __forceinline__ U* pp_wr(U* base, int it, int n2) { return base + (size_t)(it & 1) * n2; }
 
 struct FvwScalars {
     double Sn, v0, f0, fw, uini, wini;

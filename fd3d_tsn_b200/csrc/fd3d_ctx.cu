@@ -113,9 +113,23 @@ __global__ void k_interp_fric(Grid g, Fault<T> q) {
     q.T0X[a] = (q.T0Xb[a] + q.T0Xb[b] + q.T0Xb[c] + q.T0Xb[d]) / (T)4;
 }
 
+// Makes `dev` the calling thread's current device for the scope of a call and puts the
+// previous one back on exit (a host thread may have another device current).
+struct DeviceGuard {
+    int prev = -1;
+    bool changed = false;
+    explicit DeviceGuard(int dev) {
+        if (cudaGetDevice(&prev) == cudaSuccess && prev != dev && cudaSetDevice(dev) == cudaSuccess) changed = true;
+    }
+    ~DeviceGuard() {
+        if (changed) cudaSetDevice(prev);
+    }
+};
+
 struct CtxBase {
     fd3d_params p;
     Grid g;
+    int device = 0;        // the device the context's memory and streams live on
     cudaStream_t st = nullptr;
     int law = 0;
     int nf = 4;            // history planes per record
@@ -154,6 +168,9 @@ struct CtxBase {
         return best < 0 ? cudaStreamSynchronize(st) : cudaEventSynchronize(mark_ev[best]);
     }
     int overlap = 1;
+    // the fault boundary condition as separate launches (fres, traction, friction, output)
+    // with the trial tractions in q.txt / q.tzt instead of the fused kernel
+    bool split_bc = false;
     float last_ms = 0.f;
     bool profiling = false;
     int pml_minb_vel = 1, pml_minb_str = 3;  // register caps of the PML sweeps (CTAs per SM; 3 keeps the stress sweep unspilled)
@@ -238,6 +255,7 @@ struct Ctx : CtxBase {
     }
 
     int alloc() override {
+        CK(cudaGetDevice(&device));
         CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
         if (const char* e = std::getenv("FD3D_OVERLAP")) overlap = std::atoi(e);
         CK(cudaStreamCreateWithFlags(&st2, cudaStreamNonBlocking));
@@ -267,7 +285,7 @@ struct Ctx : CtxBase {
         {   // size of everything below, in the order it is carved
             const size_t n2 = (size_t)p.nxt * p.nzt;
             block_bytes = carve((size_t)g.n3 * 12 * sizeof(T)) + 37 * carve(n2 * sizeof(T)) +
-                          9 * carve(n2 * sizeof(double)) + carve(pml_aux_elems(D) * sizeof(T)) +
+                          10 * carve(n2 * sizeof(double)) + carve(pml_aux_elems(D) * sizeof(T)) +
                           carve(prof.size() * sizeof(Damp<T>)) + 2 * carve(sizeof(int)) +
                           carve((size_t)cap * nf * plane * sizeof(T)) +
                           carve((size_t)cap * std::max(1, p.nstations) * 3 * sizeof(T)) +
@@ -288,13 +306,18 @@ struct Ctx : CtxBase {
         f.mu = b + 10 * (size_t)g.n3;
         f.d = b + 11 * (size_t)g.n3;
         const size_t n2 = (size_t)p.nxt * p.nzt;
-        T** tp[] = {&q.tx, &q.tz, &q.txt, &q.tzt, &q.RFx, &q.RFz, &q.avdx, &q.avdz, &q.v1t, &q.au1, &q.av1, &q.aw1,
+        T** tp[] = {&q.tx, &q.tz, &q.RFx, &q.RFz, &q.v1t, &q.au1, &q.av1, &q.aw1,
                     &q.uZ, &q.wX, &q.tabsX, &q.tabsZ, &q.T0X, &q.T0Z, &q.T0Xb, &q.Dc, &q.peakX, &q.dynX, &q.DcX, &q.peakZ,
                     &q.dynZ, &q.DcZ, &q.coh, &q.aX, &q.bX, &q.vwX, &q.fwX, &q.aZ, &q.bZ, &q.vwZ, &q.fwZ,
                     &q.schangeX, &q.schangeZ};
         for (T** a : tp) if (dalloc(a, n2)) return FD3D_ERR_NOMEM;
-        double** dp[] = {&q.psiX, &q.psiZ, &q.distX, &q.distZ, &q.slipX, &q.slipZ, &q.ruptime, &q.rise, &q.sliptime};
+        // two-plane state (Fault): damping memory and X-node slip path
+        if (dalloc(&q.avdx, 2 * n2) || dalloc(&q.avdz, 2 * n2)) return FD3D_ERR_NOMEM;
+        double** dp[] = {&q.psiX, &q.psiZ, &q.distZ, &q.slipX, &q.slipZ, &q.ruptime, &q.rise, &q.sliptime};
         for (double** a : dp) if (dalloc(a, n2)) return FD3D_ERR_NOMEM;
+        if (dalloc(&q.distX, 2 * n2)) return FD3D_ERR_NOMEM;
+        q.n2 = (int)n2;
+        q.txt = q.tzt = nullptr;  // trial tractions live in shared memory (fault_bc_body)
         T* pool = nullptr;
         if (dalloc(&pool, pml_aux_elems(D))) return FD3D_ERR_NOMEM;
         pml_aux_bind(X, pool, D);
@@ -561,11 +584,13 @@ struct Ctx : CtxBase {
         (void)keep_psi;
         CK(cudaMemsetAsync(fieldpool, 0, (size_t)g.n3 * 9 * sizeof(T), st));
         const size_t n2 = (size_t)p.nxt * p.nzt;
-        T* zt[] = {q.tx, q.tz, q.txt, q.tzt, q.RFx, q.RFz, q.avdx, q.avdz, q.v1t, q.au1, q.av1, q.aw1, q.uZ, q.wX,
-                   q.schangeX, q.schangeZ};
+        T* zt[] = {q.tx, q.tz, q.RFx, q.RFz, q.v1t, q.au1, q.av1, q.aw1, q.uZ, q.wX, q.schangeX, q.schangeZ};
         for (T* a : zt) CK(cudaMemsetAsync(a, 0, n2 * sizeof(T), st));
-        double* zd[] = {q.distX, q.distZ, q.slipX, q.slipZ, q.rise};
+        CK(cudaMemsetAsync(q.avdx, 0, 2 * n2 * sizeof(T), st));
+        CK(cudaMemsetAsync(q.avdz, 0, 2 * n2 * sizeof(T), st));
+        double* zd[] = {q.distZ, q.slipX, q.slipZ, q.rise};
         for (double* a : zd) CK(cudaMemsetAsync(a, 0, n2 * sizeof(double), st));
+        CK(cudaMemsetAsync(q.distX, 0, 2 * n2 * sizeof(double), st));
         std::vector<double> big(n2, 1.e4);
         CK(cudaMemcpyAsync(q.ruptime, big.data(), n2 * sizeof(double), cudaMemcpyHostToDevice, st));
         CK(cudaMemcpyAsync(q.sliptime, big.data(), n2 * sizeof(double), cudaMemcpyHostToDevice, st));
@@ -643,14 +668,20 @@ struct Ctx : CtxBase {
         if (ov) join(3);
         // fault boundary condition
         kbeg(7);
-        if (!p.fspace) k_str_fs<T><<<dim3((p.nxt + 31) / 32, (p.nyt + 7) / 8), b2, 0, st>>>(g, f);  // fres
-        k_traction<T><<<dim3((nxT + 31) / 32, (nzT + 7) / 8), b2, 0, st>>>(g, f, q, c);
-        k_friction<T><<<dim3((nxT + 31) / 32, (nzT + 7) / 8), b2, 0, st>>>(g, f, q, c, law, fs, it_dev);
         HistDesc h;
         h.ring = ring; h.cap = hist_cap; h.stride = p.history_stride; h.nf = nf; h.nst = p.nstations;
         for (int s = 0; s < p.nstations; ++s) { h.sta[3 * s] = p.staX[s]; h.sta[3 * s + 1] = p.staY[s]; h.sta[3 * s + 2] = p.staZ[s]; }
         h.seis = seis;
-        k_output<T><<<dim3((nxT + 31) / 32, (nzT + 7) / 8), b2, 0, st>>>(g, f, q, law, it_dev, h, status);
+        if (!split_bc) {   // fres and the fused trial traction, friction and output tiles in one launch
+            int nfres, tiles_x, tiles;
+            fault_bc_grid(g, nfres, tiles_x, tiles);
+            k_fault_bc<T><<<nfres + tiles, b2, 0, st>>>(g, f, q, c, law, fs, it_dev, h, status, nfres, tiles_x);
+        } else {           // the same as separate launches, trial tractions in q.txt / q.tzt
+            if (!p.fspace) k_str_fs<T><<<dim3((p.nxt + 31) / 32, (p.nyt + 7) / 8), b2, 0, st>>>(g, f);  // fres
+            k_traction<T><<<dim3((nxT + 31) / 32, (nzT + 7) / 8), b2, 0, st>>>(g, f, q, c, it_dev);
+            k_friction<T><<<dim3((nxT + 31) / 32, (nzT + 7) / 8), b2, 0, st>>>(g, f, q, c, law, fs, it_dev);
+            k_output<T><<<dim3((nxT + 31) / 32, (nzT + 7) / 8), b2, 0, st>>>(g, f, q, law, it_dev, h, status);
+        }
         if (law == FD3D_LAW_FVW && fs.nucleation) {
             const int ni = (p.nxt - p.nabc) - (p.nabc - 1) + 1, nk = g.ks() - (p.nabc - 1) + 1;
             k_nucleation<T><<<dim3((ni + 31) / 32, (nk + 7) / 8), b2, 0, st>>>(g, q, c, fs, it_dev);
@@ -693,7 +724,8 @@ struct Ctx : CtxBase {
             case FD3D_PLANE_SLIPX: ds = q.slipX; break;      case FD3D_PLANE_SLIPZ: ds = q.slipZ; break;
             case FD3D_PLANE_RUPTIME: ds = q.ruptime; break;  case FD3D_PLANE_RISE: ds = q.rise; break;
             case FD3D_PLANE_SLIPTIME: ds = q.sliptime; break;
-            case FD3D_PLANE_DISTX: ds = q.distX; break;      case FD3D_PLANE_DISTZ: ds = q.distZ; break;
+            case FD3D_PLANE_DISTX: ds = pp_wr(q.distX, steps_done, (int)n2); break;  // the last step's plane
+            case FD3D_PLANE_DISTZ: ds = q.distZ; break;
             case FD3D_PLANE_PSIX: ds = q.psiX; break;        case FD3D_PLANE_PSIZ: ds = q.psiZ; break;
             case FD3D_PLANE_T0X: ts = q.T0X; break;          case FD3D_PLANE_T0Z: ts = q.T0Z; break;
             case FD3D_PLANE_SCHANGEX: ts = q.schangeX; break; case FD3D_PLANE_SCHANGEZ: ts = q.schangeZ; break;
@@ -917,6 +949,7 @@ int fd3d_run(fd3d_ctx* ctx, int nsteps) {
     fd3d::TraceRange trace_("fd3d_run");
     if (!ctx || nsteps < 0) return FD3D_ERR_ARG;
     CtxBase* c = ctx->impl;
+    DeviceGuard dg(c->device);
     if (!c->medium_ok || !c->fault_ok) return FD3D_ERR_STATE;
     CK(cudaEventRecord(c->ev0, c->st));
     int left = nsteps;
@@ -1119,14 +1152,17 @@ int fd3d_write_results(fd3d_ctx* ctx, const char* dir, int rk) {
 }  // extern "C"
 
 // ---------------------------------------------------------------------------
-// fd3d_run_noalloc: the time step with the fault boundary condition's trial-traction
-// scratch taken from a fixed, file-scope device array instead of memory the library
-// allocates.  Meant for hosts that cannot let the library allocate device memory once
-// their run has started (their device memory is handed out by another runtime, such
-// as the OpenACC present table of a Fortran host, or was reserved up front against a
-// fixed budget).  fd3d_run may allocate on its first call (it instantiates a CUDA graph
-// of the step); this entry point launches the kernels one by one and calls no
-// cudaMalloc, cudaFree or other allocating routine.
+// fd3d_run_noalloc: the time step with the fault boundary condition as separate launches
+// (fres, trial traction, friction, output) whose trial-traction scratch is taken from a
+// fixed, file-scope device array instead of memory the library allocates.  Meant for
+// hosts that cannot let the library allocate device memory once their run has started
+// (their device memory is handed out by another runtime, such as the OpenACC present
+// table of a Fortran host, or was reserved up front against a fixed budget).  fd3d_run
+// may allocate on its first call (it instantiates a CUDA graph of the step); this entry
+// point launches the kernels one by one and calls no cudaMalloc, cudaFree or other
+// allocating routine.  The array's device address is looked up once per device and kept
+// for the life of the process, so a device reset (cudaDeviceReset) between calls is not
+// supported.
 //
 // Limit: nxt*nzt <= FD3D_NOALLOC_MAX_PLANE fault-plane nodes (the array holds two
 // planes of doubles, 16 MiB, on every GPU that loads the library, until exit).
@@ -1175,7 +1211,9 @@ int run_noalloc_t(Ctx<T>* c, int nsteps, void* scratch) {
     T* const tzt0 = c->q.tzt;
     c->q.txt = (T*)scratch;
     c->q.tzt = (T*)scratch + n2;
+    c->split_bc = true;
     for (int s = 0; s < nsteps; ++s) c->enqueue_step();
+    c->split_bc = false;
     c->q.txt = txt0;
     c->q.tzt = tzt0;
     CK(cudaGetLastError());
@@ -1187,6 +1225,7 @@ int run_noalloc_t(Ctx<T>* c, int nsteps, void* scratch) {
 }  // namespace
 
 extern "C" int fd3d_run_noalloc(fd3d_ctx* ctx, int nsteps) {
+    fd3d::TraceRange trace_("fd3d_run_noalloc");
     if (!ctx || nsteps < 0) return FD3D_ERR_ARG;
     CtxBase* c = ctx->impl;
     if (!c->medium_ok || !c->fault_ok) return FD3D_ERR_STATE;
@@ -1196,10 +1235,9 @@ extern "C" int fd3d_run_noalloc(fd3d_ctx* ctx, int nsteps) {
                      FD3D_NOALLOC_MAX_PLANE);
         return FD3D_ERR_ARG;
     }
-    cudaPointerAttributes attr;
-    CK(cudaPointerGetAttributes(&attr, c->it_dev));  // the device the context lives on
+    DeviceGuard dg(c->device);  // the memset and the launches go to the context's device
     void* scratch = nullptr;
-    int rc = noalloc_scratch(attr.device, &scratch);
+    int rc = noalloc_scratch(c->device, &scratch);
     if (rc) return rc;
     if (auto* cf = dynamic_cast<Ctx<float>*>(c)) return run_noalloc_t(cf, nsteps, scratch);
     if (auto* cd = dynamic_cast<Ctx<double>*>(c)) return run_noalloc_t(cd, nsteps, scratch);

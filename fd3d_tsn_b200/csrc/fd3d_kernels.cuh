@@ -2,7 +2,8 @@
 // field type T: float for the production build, double for the FP64 build).
 //
 // The step is eight launches, each a set of reference regions whose write sets are
-// disjoint and which read nothing another thread of the same launch writes:
+// disjoint and which read nothing another thread of the same launch writes (the fused
+// fault boundary condition forms what its fres CTAs write from what they read):
 //   1 vel_interior  uxx1/vyy1/wzz1 (fd3d_deriv.f90:50-193)
 //   2 vel_fault     uxx0a/vyy0a/wzz0a at j=nyt-1 + v mirror (fd3d_deriv.f90:198-508),
 //                   tasu1/tasw1 at j=nyt (fd3d_deriv.f90:1109-1234)
@@ -12,9 +13,13 @@
 //   6 str_fault     sxx/sxy0/sxz0/syz0 at j=nyt-1 + xy/yz mirror, sxz1, tasii
 //                   (fd3d_deriv.f90:677-1012,1239-1314)
 //   7 str_pml       pml_xyz (fd3d_deriv.f90:2304-2992)
-//   8 str_fs        fres (fd3d_deriv.f90:1067-1104)
-// followed by the fault boundary condition (fd3d_theo.f90:233-542) in three plane
-// launches: traction, friction (|T| + friction law + slip), output planes.
+//   8 fault_bc      fres (fd3d_deriv.f90:1067-1104) and the fault boundary condition
+//                   (fd3d_theo.f90:225-467): trial traction, |T| at the staggered nodes,
+//                   friction law with slip and rupture time, output planes, fused per
+//                   tile (fault_bc_body)
+// and, for rate-and-state runs with a nucleation ramp, the ramp (fd3d_theo.f90:487-542).
+// The fault boundary condition also exists as separate launches (str_fs, traction,
+// friction, output), which fd3d_run_noalloc uses.
 //
 // Operation order inside every expression follows the reference so that, with
 // contraction of multiply-add switched off (--fmad=false), the FP32 and FP64
@@ -601,7 +606,8 @@ __device__ __forceinline__ void str_fs_body(Grid g, Fields<T> f, int bx_, int by
 // trial traction, damping, RF (fd3d_theo.f90:233-308).  Under FSPACE the top row k = ks
 // takes the interior formula and no ghost row is written (fd3d_theo.f90:260-283).
 template <class T>
-__device__ __forceinline__ void traction_body(Grid g, Fields<T> f, Fault<T> q, StepConst<T> c, int bx_, int by_, int bz_) {
+__device__ __forceinline__ void traction_body(Grid g, Fields<T> f, Fault<T> q, StepConst<T> c, const int* it_dev,
+                                              int bx_, int by_, int bz_) {
     const int i = g.nabc + 1 + bx_ * blockDim.x + threadIdx.x;
     const int k = g.nabc + 1 + by_ * blockDim.y + threadIdx.y;
     const int ks = g.ks();
@@ -611,6 +617,9 @@ __device__ __forceinline__ void traction_body(Grid g, Fields<T> f, Fault<T> q, S
     const int n2 = g.at2(i, k);
     const T c1 = c.c1, c2 = c.c2, dht = c.dht, ds = c.damp_s;
     const T* xx = f.xx; const T* xz = f.xz; const T* zz = f.zz;
+    const int it = *it_dev;
+    const T* avdz_rd = pp_rd(q.avdz, it, q.n2); T* avdz_wr = pp_wr(q.avdz, it, q.n2);
+    const T* avdx_rd = pp_rd(q.avdx, it, q.n2); T* avdx_wr = pp_wr(q.avdx, it, q.n2);
     const bool inner = (k < ks) || g.fspace;
     T pdz;
     if (inner)
@@ -619,22 +628,22 @@ __device__ __forceinline__ void traction_body(Grid g, Fields<T> f, Fault<T> q, S
     else
         pdz = ((xz[p + 1 - sz] - xz[p - sz]) / ((T)2 * (T)4) + (zz[p + sz] - zz[p]) / ((T)2 * (T)2) -
                f.yz[p - sy - sz] / (T)4);
-    T av = ds * (pdz - q.avdz[n2]);
+    T av = ds * (pdz - avdz_rd[n2]);
     T rf = pdz + av;
     q.RFz[n2] = rf;
     T tzv;
     if (inner) tzv = -rf - (T)0.5 * f.d[p] * dht * f.w[p];
     else        tzv = -rf - (T)0.5 * f.d[p] * dht * f.w[p] / (T)2;
     q.tzt[n2] = tzv;
-    q.avdz[n2] = pdz;
+    avdz_wr[n2] = pdz;
     const T pdx = (c1 * (xx[p] - xx[p - 1]) + c2 * (xx[p + 1] - xx[p - 2])) / (T)2 +
                   (c1 * (xz[p] - xz[p - sz]) + c2 * (xz[p + sz] - xz[p - 2 * sz])) / (T)2 - f.xy[p - sy];
-    av = ds * (pdx - q.avdx[n2]);
+    av = ds * (pdx - avdx_rd[n2]);
     rf = pdx + av;
     q.RFx[n2] = rf;
     const T txv = -rf - (T)0.5 * f.d[p] * dht * f.u[p];
     q.txt[n2] = txv;
-    q.avdx[n2] = pdx;
+    avdx_wr[n2] = pdx;
     // ghost row nzt-1 (fd3d_theo.f90:304-307); with nfs=2: nzt-1 = ks+1, nzt-2 = ks, nzt-3 = ks-1
     if (!g.fspace && k == ks) q.txt[g.at2(i, ks + 1)] = +txv;
     if (!g.fspace && k == ks - 1) q.tzt[g.at2(i, ks + 1)] = -tzv;
@@ -647,7 +656,10 @@ __device__ __forceinline__ void friction_body(Grid g, Fields<T> f, Fault<T> q, S
     const int i = g.nabc + 1 + bx_ * blockDim.x + threadIdx.x;
     const int k = g.nabc + 1 + by_ * blockDim.y + threadIdx.y;
     if (i > g.nxt - g.nabc || k > g.ks()) return;
-    const double time = (double)(*it_dev) * c.dtA;
+    const int it = *it_dev;
+    const double time = (double)it * c.dtA;
+    const double* distX_rd = pp_rd(q.distX, it, q.n2);
+    double* distX_wr = pp_wr(q.distX, it, q.n2);
     const double dtA = c.dtA, rup = 1.e-3;
     const long long sy = g.px, sz = g.plane;
     (void)sy;
@@ -724,16 +736,18 @@ __device__ __forceinline__ void friction_body(Grid g, Fields<T> f, Fault<T> q, S
             const double psi = (q.psiX[n2] - psiss) * exp(-sr * dtA / (double)q.Dc[n2]) + psiss;
             q.psiX[n2] = psi;
             const double fric = s.Sn * a * asinh(sr * exp(psi / a) / (2.0 * s.v0));
-            q.distX[n2] = q.distX[n2] - 2.0 * (double)u1out * dtA;
+            distX_wr[n2] = distX_rd[n2] - 2.0 * (double)u1out * dtA;
             q.schangeX[n2] = (T)fric;
         } else {
-            const double dx = q.distX[n2], dcx = (double)q.DcX[n2];
+            const double dx = distX_rd[n2], dcx = (double)q.DcX[n2];
             double fric;
             if (dx <= (double)q.Dc[n2]) fric = (double)q.peakX[n2] * (1.0 - dx / dcx) + (double)q.dynX[n2] * dx / dcx + (double)q.coh[n2];
             else                        fric = (double)q.dynX[n2] + (double)q.coh[n2];
             if ((double)tabsX >= fric) {
-                q.distX[n2] = dx - 2.0 * (double)u1out * dtA;
+                distX_wr[n2] = dx - 2.0 * (double)u1out * dtA;
                 txn = (T)(((double)txn + (double)T0X[n2]) * fric / (double)tabsX - (double)T0X[n2]);
+            } else {
+                distX_wr[n2] = dx;  // carried into this step's plane
             }
         }
         q.tx[n2] = txn;
@@ -804,6 +818,312 @@ __device__ __forceinline__ void output_body(Grid g, Fields<T> f, Fault<T> q, int
         r[3 * plane] = scz;
         if (h.nf > 4) r[4 * plane] = (T)q.psiZ[n2];
     }
+}
+
+// ---------------------------------------------------------------- fused fault BC
+// The fault boundary condition of one step in one launch (fd3d_theo.f90:225-467): fres, the
+// trial traction, |T| at the staggered nodes, the friction law with slip and rupture time,
+// and the output planes.  A CTA owns a FBC_TX x FBC_TZ tile of fault nodes and computes the
+// trial tractions of the tile and a one-node ring around it, and the post-friction
+// tractions of the X nodes of the tile plus one column and one row beyond, into shared
+// memory; the ring values it only reads, so the state it needs from neighbouring nodes is
+// the state before this step (the two-plane avdx, avdz and distX of Fault) and nothing
+// another CTA writes in the same launch.  fres runs in separate CTAs of the same launch:
+// the three stresses it writes that the trial traction reads (zz at ks+1, xz at ks and
+// ks+1, fd3d_deriv.f90:1087-1102) are formed from the values fres reads, with the same
+// operation (a negation, or the zero it stores).
+constexpr int FBC_TX = 32, FBC_TZ = 8;                   // owned nodes of a tile (CTA of 32 x 8 threads)
+constexpr int FBC_HX = FBC_TX + 2, FBC_HZ = FBC_TZ + 2;  // trial tractions: the tile and a one-node ring
+constexpr int FBC_PX = FBC_TX + 1, FBC_PZ = FBC_TZ + 1;  // post-friction X-node tractions: tile + 1 in +i, +k
+constexpr int FBC_SMEM = 2 * FBC_HX * FBC_HZ + FBC_PX * FBC_PZ;  // elements of T
+
+template <class T>
+struct TrialTraction { T pdz, pdx, rfz, rfx, tzv, txv; };
+
+// trial traction at fault node (i,k) (fd3d_theo.f90:233-308), in the operation order of
+// traction_body; VIRT: fres has not run yet, its stores are formed here
+template <class T, bool VIRT>
+__device__ __forceinline__ TrialTraction<T> trial_traction(const Grid& g, const Fields<T>& f, const StepConst<T>& c,
+                                                           const T* avdz_rd, const T* avdx_rd, int i, int k) {
+    const int ks = g.ks();
+    const bool virt = VIRT && !g.fspace;
+    const long long sy = g.px;
+    auto XZ = [&](int ii, int kk) -> T {
+        if (virt && kk == ks) return (T)0;                                 // xz(i,nyt,nzt-nfs) = 0
+        if (virt && kk == ks + 1) return -f.xz[g.at(ii, g.nyt, ks - 1)];   // xz(ks+1) = -xz(ks-1)
+        return f.xz[g.at(ii, g.nyt, kk)];
+    };
+    auto ZZ = [&](int kk) -> T {
+        if (virt && kk == ks + 1) return -f.zz[g.at(i, g.nyt, ks)];        // zz(ks+1) = -zz(ks)
+        return f.zz[g.at(i, g.nyt, kk)];
+    };
+    const long long p = g.at(i, g.nyt, k);
+    const int n2 = g.at2(i, k);
+    const T c1 = c.c1, c2 = c.c2, dht = c.dht, ds = c.damp_s;
+    const T* xx = f.xx;
+    const bool inner = (k < ks) || g.fspace;
+    TrialTraction<T> t;
+    if (inner)
+        t.pdz = (c1 * (XZ(i + 1, k) - XZ(i, k)) + c2 * (XZ(i + 2, k) - XZ(i - 1, k))) / (T)2 +
+                (c1 * (ZZ(k + 1) - ZZ(k)) + c2 * (ZZ(k + 2) - ZZ(k - 1))) / (T)2 - f.yz[p - sy];
+    else
+        t.pdz = ((XZ(i + 1, k - 1) - XZ(i, k - 1)) / ((T)2 * (T)4) + (ZZ(k + 1) - ZZ(k)) / ((T)2 * (T)2) -
+                 f.yz[p - sy - g.plane] / (T)4);
+    T av = ds * (t.pdz - avdz_rd[n2]);
+    t.rfz = t.pdz + av;
+    if (inner) t.tzv = -t.rfz - (T)0.5 * f.d[p] * dht * f.w[p];
+    else       t.tzv = -t.rfz - (T)0.5 * f.d[p] * dht * f.w[p] / (T)2;
+    t.pdx = (c1 * (xx[p] - xx[p - 1]) + c2 * (xx[p + 1] - xx[p - 2])) / (T)2 +
+            (c1 * (XZ(i, k) - XZ(i, k - 1)) + c2 * (XZ(i, k + 1) - XZ(i, k - 2))) / (T)2 - f.xy[p - sy];
+    av = ds * (t.pdx - avdx_rd[n2]);
+    t.rfx = t.pdx + av;
+    t.txv = -t.rfx - (T)0.5 * f.d[p] * dht * f.u[p];
+    return t;
+}
+
+// Friction at the X node (i,k) (fd3d_theo.f90:375-410) from trial tractions in shared
+// memory: returns the traction after friction; OWN: also the node's state (tabsX, wX,
+// slip path, psi, strength).
+template <class T, bool OWN>
+__device__ __forceinline__ T friction_x(const Grid& g, const Fields<T>& f, const Fault<T>& q, const StepConst<T>& c,
+                                        int law, const FvwScalars& s, const double* distX_rd, double* distX_wr,
+                                        T txt0, T tint, int i, int k) {
+    const int n2 = g.at2(i, k);
+    const double dtA = c.dtA;
+    const long long sz = g.plane;
+    const T sxv = txt0 + q.T0X[n2];
+    const T tabsX = sqrt(sxv * sxv + tint * tint);
+    const long long p = g.at(i, g.nyt, k);
+    const T U = f.u[p], W = f.w[p];
+    const T wX = (W + f.w[p - 1] + f.w[p - sz] + f.w[p - 1 - sz]) / (T)4;
+    const T u1out = -sqrt(wX * wX + U * U);
+    T txn = txt0;
+    if (OWN) { q.tabsX[n2] = tabsX; q.wX[n2] = wX; }
+    if (law == 1) {
+        if (OWN) {
+            const double a = (double)q.aX[n2];
+            const double s1 = 2.0 * (fabs((double)wX) + fabs(s.wini)), s2 = 2.0 * (fabs((double)U) + fabs(s.uini));
+            const double sr = sqrt(s1 * s1 + s2 * s2);
+            const double flv = s.f0 - ((double)q.bX[n2] - a) * log(sr / s.v0);
+            const double fw = (double)q.fwX[n2];
+            const double fss = fw + (flv - fw) / pow(1.0 + pow(sr / (double)q.vwX[n2], 8.0), 1.0 / 8.0);
+            const double psiss = a * (log(sinh(fss / a)) + log(2.0 * s.v0 / sr));
+            const double psi = (q.psiX[n2] - psiss) * exp(-sr * dtA / (double)q.Dc[n2]) + psiss;
+            q.psiX[n2] = psi;
+            const double fric = s.Sn * a * asinh(sr * exp(psi / a) / (2.0 * s.v0));
+            distX_wr[n2] = distX_rd[n2] - 2.0 * (double)u1out * dtA;
+            q.schangeX[n2] = (T)fric;
+        }
+    } else {
+        const double dx = distX_rd[n2], dcx = (double)q.DcX[n2];
+        double fric;
+        if (dx <= (double)q.Dc[n2]) fric = (double)q.peakX[n2] * (1.0 - dx / dcx) + (double)q.dynX[n2] * dx / dcx + (double)q.coh[n2];
+        else                        fric = (double)q.dynX[n2] + (double)q.coh[n2];
+        double dnew = dx;
+        if ((double)tabsX >= fric) {
+            dnew = dx - 2.0 * (double)u1out * dtA;
+            txn = (T)(((double)txn + (double)q.T0X[n2]) * fric / (double)tabsX - (double)q.T0X[n2]);
+        }
+        if (OWN) distX_wr[n2] = dnew;
+    }
+    if (OWN) q.tx[n2] = txn;
+    return txn;
+}
+
+// Friction at the Z node (i,k) (fd3d_theo.f90:326-373): state, slip, rupture time; returns tz.
+template <class T>
+__device__ __forceinline__ T friction_z(const Grid& g, const Fields<T>& f, const Fault<T>& q, const StepConst<T>& c,
+                                        int law, const FvwScalars& s, double time, T tzt0, T tint, int i, int k) {
+    const int n2 = g.at2(i, k);
+    const double dtA = c.dtA, rup = 1.e-3;
+    const long long sz = g.plane;
+    const T* T0Z = q.T0Z;
+    const T szv = tzt0 + T0Z[n2];
+    const T tabsZ = sqrt(tint * tint + szv * szv);
+    q.tabsZ[n2] = tabsZ;
+    const long long p = g.at(i, g.nyt, k);
+    const T U = f.u[p], W = f.w[p];
+    const T uZ = (U + f.u[p + 1] + f.u[p + sz] + f.u[p + 1 + sz]) / (T)4;
+    q.uZ[n2] = uZ;
+    const T u1out = -sqrt(W * W + uZ * uZ);
+    T tzn = tzt0;
+    if (law == 1) {
+        const double a = (double)q.aZ[n2];
+        const double s1 = 2.0 * (fabs((double)W) + fabs(s.wini)), s2 = 2.0 * (fabs((double)uZ) + fabs(s.uini));
+        const double sr = sqrt(s1 * s1 + s2 * s2);
+        const double flv = s.f0 - ((double)q.bZ[n2] - a) * log(sr / s.v0);
+        const double fw = (double)q.fwZ[n2];
+        const double fss = fw + (flv - fw) / pow(1.0 + pow(sr / (double)q.vwZ[n2], 8.0), 1.0 / 8.0);
+        const double psiss = a * (log(sinh(fss / a)) + log(2.0 * s.v0 / sr));
+        const double psi = (q.psiZ[n2] - psiss) * exp(-sr * dtA / (double)q.Dc[n2]) + psiss;
+        q.psiZ[n2] = psi;
+        const double fric = s.Sn * a * asinh(sr * exp(psi / a) / (2.0 * s.v0));
+        q.distZ[n2] = q.distZ[n2] - 2.0 * (double)u1out * dtA;
+        q.schangeZ[n2] = (T)fric;
+        if (fabs(2.0 * (double)u1out) > rup) {
+            if (q.ruptime[n2] != 1.e4) q.rise[n2] = time;
+            if (q.ruptime[n2] == 1.e4) q.ruptime[n2] = time;
+        }
+    } else {
+        const double dz = q.distZ[n2], dcz = (double)q.DcZ[n2];
+        double fric;
+        if (dz <= dcz) fric = (double)q.peakZ[n2] * (1.0 - dz / dcz) + (double)q.dynZ[n2] * dz / dcz + (double)q.coh[n2];
+        else           fric = (double)q.dynZ[n2] + (double)q.coh[n2];
+        if ((double)tabsZ >= fric) {
+            q.distZ[n2] = dz - 2.0 * (double)u1out * dtA;
+            tzn = (T)(((double)tzn + (double)T0Z[n2]) * fric / (double)tabsZ - (double)T0Z[n2]);
+            if (-2.0 * (double)u1out > rup) {
+                if (q.ruptime[n2] != 1.e4) q.rise[n2] = time;
+                if (q.ruptime[n2] == 1.e4) q.ruptime[n2] = time;
+            }
+        }
+    }
+    q.tz[n2] = tzn;
+    q.slipZ[n2] = q.slipZ[n2] - 2.0 * (double)W * dtA;
+    q.slipX[n2] = q.slipX[n2] - 2.0 * (double)uZ * dtA;
+    if (q.sliptime[n2] == 1.e4 && q.distZ[n2] > (double)q.Dc[n2]) q.sliptime[n2] = time;
+    return tzn;
+}
+
+// One tile of the fused fault boundary condition (without fres).  A CTA of 32 x 8 threads;
+// sm holds FBC_SMEM elements.
+template <class T>
+__device__ __forceinline__ void fault_bc_body(const Grid& g, const Fields<T>& f, const Fault<T>& q,
+                                              const StepConst<T>& c, int law, const FvwScalars& s, const int* it_dev,
+                                              const HistDesc& h, int* status, int bx_, int by_, T* sm) {
+    const int tid = threadIdx.y * 32 + threadIdx.x;
+    const int i0 = g.nabc + 1 + bx_ * FBC_TX, k0 = g.nabc + 1 + by_ * FBC_TZ;
+    const int ie = g.nxt - g.nabc, ks = g.ks();
+    const int it = *it_dev;
+    const T* avdz_rd = pp_rd(q.avdz, it, q.n2); T* avdz_wr = pp_wr(q.avdz, it, q.n2);
+    const T* avdx_rd = pp_rd(q.avdx, it, q.n2); T* avdx_wr = pp_wr(q.avdx, it, q.n2);
+    const double* distX_rd = pp_rd(q.distX, it, q.n2); double* distX_wr = pp_wr(q.distX, it, q.n2);
+    T* s_txt = sm;                        // [FBC_HZ][FBC_HX], node (i,k) at (i-i0+1) + (k-k0+1)*FBC_HX
+    T* s_tzt = sm + FBC_HX * FBC_HZ;
+    T* s_tx = sm + 2 * FBC_HX * FBC_HZ;   // [FBC_PZ][FBC_PX], node (i,k) at (i-i0) + (k-k0)*FBC_PX
+    __syncthreads();                      // the shared memory may hold the previous item's values
+
+    // 1. trial tractions of the tile and its ring; the owner stores a node's state
+    for (int n = tid; n < FBC_HX * FBC_HZ; n += 256) {
+        const int ri = n % FBC_HX, rk = n / FBC_HX;
+        const int i = i0 - 1 + ri, k = k0 - 1 + rk;
+        T tx_ = 0, tz_ = 0;   // outside the traction loops the reference's tx, tz stay 0
+        if (i >= g.nabc + 1 && i <= ie) {
+            if (k >= g.nabc + 1 && k <= ks) {
+                const TrialTraction<T> t = trial_traction<T, true>(g, f, c, avdz_rd, avdx_rd, i, k);
+                tx_ = t.txv;
+                tz_ = t.tzv;
+                if (ri >= 1 && ri <= FBC_TX && rk >= 1 && rk <= FBC_TZ) {
+                    const int n2 = g.at2(i, k);
+                    q.RFz[n2] = t.rfz;
+                    q.RFx[n2] = t.rfx;
+                    avdz_wr[n2] = t.pdz;
+                    avdx_wr[n2] = t.pdx;
+                }
+            } else if (!g.fspace && k == ks + 1) {  // ghost row: tx(nzt-1) = tx(nzt-2), tz(nzt-1) = -tz(nzt-3)
+                tx_ = +trial_traction<T, true>(g, f, c, avdz_rd, avdx_rd, i, ks).txv;
+                tz_ = -trial_traction<T, true>(g, f, c, avdz_rd, avdx_rd, i, ks - 1).tzv;
+            }
+        }
+        s_txt[n] = tx_;
+        s_tzt[n] = tz_;
+    }
+    __syncthreads();
+    auto TXT = [&](int i, int k) { return s_txt[(i - i0 + 1) + (k - k0 + 1) * FBC_HX]; };
+    auto TZT = [&](int i, int k) { return s_tzt[(i - i0 + 1) + (k - k0 + 1) * FBC_HX]; };
+    auto TINT_X = [&](int i, int k) {  // 4-point average of tz + T0Z around X node (i,k)
+        const int n2 = g.at2(i, k), w1 = g.at2(i - 1, k), w2 = g.at2(i, k - 1), w3 = g.at2(i - 1, k - 1);
+        return (TZT(i, k) + q.T0Z[n2] + TZT(i - 1, k) + q.T0Z[w1] + TZT(i, k - 1) + q.T0Z[w2] + TZT(i - 1, k - 1) +
+                q.T0Z[w3]) / (T)4;
+    };
+
+    // 2. friction: the Z and X nodes of the tile (thread = node), then the X nodes of the
+    //    column and row beyond it (their tractions after friction, for the output)
+    const int ti = threadIdx.x, tk = threadIdx.y;
+    const int i = i0 + ti, k = k0 + tk;
+    const bool own = i <= ie && k <= ks;
+    T tzn = 0, txo = 0;   // beyond the interior plane the reference's tx stays 0
+    if (own) {
+        const double time = (double)it * c.dtA;
+        const int n2 = g.at2(i, k), e1 = g.at2(i + 1, k), e2 = g.at2(i, k + 1), e3 = g.at2(i + 1, k + 1);
+        const T tintz = (TXT(i, k) + q.T0X[n2] + TXT(i + 1, k) + q.T0X[e1] + TXT(i, k + 1) + q.T0X[e2] +
+                         TXT(i + 1, k + 1) + q.T0X[e3]) / (T)4;
+        tzn = friction_z<T>(g, f, q, c, law, s, time, TZT(i, k), tintz, i, k);
+        txo = friction_x<T, true>(g, f, q, c, law, s, distX_rd, distX_wr, TXT(i, k), TINT_X(i, k), i, k);
+        if (k == ks) {  // the reference's tx/tz arrays also carry the ghost row nzt-1
+            const int gh = g.at2(i, k + 1);
+            q.tx[gh] = TXT(i, k + 1);
+            q.tz[gh] = TZT(i, k + 1);
+        }
+    }
+    s_tx[ti + tk * FBC_PX] = txo;
+    if (tid < FBC_PX + FBC_TZ) {  // column i0+FBC_TX (k0..k0+FBC_TZ), then row k0+FBC_TZ (i0..i0+FBC_TX-1)
+        const int hi = tid < FBC_PZ ? i0 + FBC_TX : i0 + (tid - FBC_PZ);
+        const int hk = tid < FBC_PZ ? k0 + tid : k0 + FBC_TZ;
+        T txh = 0;
+        if (hi <= ie && hk <= ks && law == 0)
+            txh = friction_x<T, false>(g, f, q, c, law, s, distX_rd, distX_wr, TXT(hi, hk), TINT_X(hi, hk), hi, hk);
+        else if (hi <= ie && hk <= ks)
+            txh = TXT(hi, hk);
+        s_tx[(hi - i0) + (hk - k0) * FBC_PX] = txh;
+    }
+    __syncthreads();
+
+    // 3. output planes, stations, history ring (fd3d_theo.f90:413-467) of the tile's nodes
+    if (bx_ == 0 && by_ == 0 && tid < h.nst && it % h.stride == 0) {
+        const long long slot = (long long)((it / h.stride - 1) % h.cap);
+        const long long p = g.at(h.sta[3 * tid], h.sta[3 * tid + 1], h.sta[3 * tid + 2]);
+        T* sp = (T*)h.seis + slot * (3 * h.nst) + 3 * tid;
+        sp[0] = f.u[p]; sp[1] = f.v[p]; sp[2] = f.w[p];
+    }
+    if (!own) return;
+    auto TX = [&](int ii, int kk) { return s_tx[(ii - i0) + (kk - k0) * FBC_PX]; };
+    const bool top = (k == ks);
+    const long long p = g.at(i, g.nyt, k), sz = g.plane;
+    const int n2 = g.at2(i, k), e1 = g.at2(i + 1, k), e2 = g.at2(i, k + 1), e3 = g.at2(i + 1, k + 1);
+    const T U = f.u[p], U2 = f.u[p + 1], W = f.w[p];
+    T srx, srz, scx, scz;
+    srz = (T)-2 * W;
+    if (!top) {
+        const T U3 = f.u[p + sz], U4 = f.u[p + 1 + sz];
+        srx = ((T)-2 * U - (T)2 * U2 - (T)2 * U3 - (T)2 * U4) / (T)4;
+        if (law == 0) {
+            scz = tzn + q.T0Z[n2];
+            scx = (TX(i, k) + q.T0X[n2] + TX(i + 1, k) + q.T0X[e1] + TX(i, k + 1) + q.T0X[e2] + TX(i + 1, k + 1) +
+                   q.T0X[e3]) / (T)4;
+        }
+    } else {
+        if (law == 1) {
+            srx = ((T)-2 * U - (T)2 * U2) / (T)4;
+        } else {
+            scz = tzn + q.T0Z[n2];
+            scx = (TX(i, k) + q.T0X[n2] + TX(i + 1, k) + q.T0X[e1]) / (T)2;
+            srx = ((T)-2 * U - (T)2 * U2) / (T)2;
+        }
+    }
+    if (law == 1) { scx = q.schangeX[n2]; scz = q.schangeZ[n2]; }
+    else { q.schangeX[n2] = scx; q.schangeZ[n2] = scz; }
+    if (!(isfinite((double)srx) && isfinite((double)srz) && isfinite((double)scx) && isfinite((double)scz)))
+        atomicOr(status, ST_NONFINITE);
+    if (it % h.stride == 0) {
+        const int nxT = g.nxt - 2 * g.nabc, nzT = ks - g.nabc;
+        const long long slot = (long long)((it / h.stride - 1) % h.cap);
+        const long long plane = (long long)nxT * nzT;
+        T* r = (T*)h.ring + slot * h.nf * plane + (long long)(k - g.nabc - 1) * nxT + (i - g.nabc - 1);
+        r[0] = srx;
+        r[plane] = srz;
+        r[2 * plane] = scx;
+        r[3 * plane] = scz;
+        if (h.nf > 4) r[4 * plane] = (T)q.psiZ[n2];
+    }
+}
+
+// grid of the fused fault BC: fres CTAs (32 x 8 (i,j) each), then the fault tiles
+inline void fault_bc_grid(const Grid& g, int& nfres, int& tiles_x, int& tiles) {
+    nfres = g.fspace ? 0 : ((g.nxt + 31) / 32) * ((g.nyt + 7) / 8);
+    const int nxT = g.nxt - 2 * g.nabc, nzT = g.ks() - g.nabc;
+    tiles_x = (nxT + FBC_TX - 1) / FBC_TX;
+    tiles = tiles_x * ((nzT + FBC_TZ - 1) / FBC_TZ);
 }
 
 // TPV103/104 smooth nucleation of T0X (fd3d_theo.f90:487-542)
@@ -890,8 +1210,8 @@ __global__ void k_str_fs(Grid g, Fields<T> f) {
 }
 
 template <class T>
-__global__ void k_traction(Grid g, Fields<T> f, Fault<T> q, StepConst<T> c) {
-    traction_body<T>(g, f, q, c, blockIdx.x, blockIdx.y, blockIdx.z);
+__global__ void k_traction(Grid g, Fields<T> f, Fault<T> q, StepConst<T> c, const int* it_dev) {
+    traction_body<T>(g, f, q, c, it_dev, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
 template <class T>
@@ -904,6 +1224,23 @@ template <class T>
 __global__ void k_output(Grid g, Fields<T> f, Fault<T> q, int law, const int* it_dev, const __grid_constant__ HistDesc h,
                          int* status) {
     output_body<T>(g, f, q, law, it_dev, h, status, blockIdx.x, blockIdx.y, blockIdx.z);
+}
+
+// The fused fault boundary condition of one step: nfres CTAs of fres, then the fault tiles
+// (tiles_x per row of tiles); CTA of 32 x 8 threads.
+template <class T>
+__global__ void __launch_bounds__(256) k_fault_bc(Grid g, Fields<T> f, Fault<T> q, StepConst<T> c, int law,
+                                                  FvwScalars s, const int* it_dev, const __grid_constant__ HistDesc h,
+                                                  int* status, int nfres, int tiles_x) {
+    __shared__ T sm[FBC_SMEM];
+    const int b = blockIdx.x;
+    if (b < nfres) {
+        const int sx = (g.nxt + 31) / 32;
+        str_fs_body<T>(g, f, b % sx, b / sx, 0);
+        return;
+    }
+    const int t = b - nfres;
+    fault_bc_body<T>(g, f, q, c, law, s, it_dev, h, status, t % tiles_x, t / tiles_x, sm);
 }
 
 template <class T>

@@ -197,12 +197,15 @@ int fd3d_sync(fd3d_ctx* ctx);                       /* wait; returns first devic
  * let the library allocate device memory once their run has started (device memory
  * owned by another runtime, e.g. a Fortran host's OpenACC data region, or reserved up
  * front against a fixed budget).  It calls no cudaMalloc/cudaFree and instantiates no
- * graph; the trial-traction scratch of the fault boundary condition lives in a fixed
- * device array of the library (2 planes of doubles for up to 2^20 = nxt*nzt fault-plane
- * nodes, 16 MiB held on every GPU that loads the library until exit).  Larger planes
- * are rejected with FD3D_ERR_ARG.  The first call on a device looks up that array's
- * device address, so make it before any stream capture.  All calls share the array:
- * calls whose work overlaps on one GPU (contexts on different streams) race on it. */
+ * graph: it launches the step kernels one by one, the fault boundary condition as four
+ * launches whose trial-traction scratch lives in a fixed device array of the library
+ * (2 planes of doubles for up to 2^20 = nxt*nzt fault-plane nodes, 16 MiB held on every
+ * GPU that loads the library until exit).  Larger planes are rejected with FD3D_ERR_ARG.
+ * The first call on a device looks up that array's device address, so make it before
+ * any stream capture; the address is kept for the life of the process, so a device
+ * reset between calls is not supported.  The call runs on the context's device whatever
+ * device the calling thread has current.  All calls share the array: calls whose work
+ * overlaps on one GPU (contexts on different streams) race on it. */
 int fd3d_run_noalloc(fd3d_ctx* ctx, int nsteps);
 int fd3d_steps_done(fd3d_ctx* ctx, int* it);
 /* Records rec0..rec0+nrec-1 of one history plane (x fastest per record).  Waits only for

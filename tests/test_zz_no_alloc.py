@@ -2,10 +2,11 @@
 
 fd3d_run_noalloc is for hosts that cannot let the library allocate device memory once
 their run has started, for instance a Fortran host whose device arrays belong to the
-OpenACC runtime, or a service that reserved its HBM up front.  It takes the fault
-boundary condition's scratch from a fixed device array of the library instead of
-memory the library allocates.  Its results must equal fd3d_run's bit for bit (the
-same kernels in the same order), over two calls in a row.
+OpenACC runtime, or a service that reserved its HBM up front.  It runs the fault
+boundary condition as separate launches whose scratch comes from a fixed device array
+of the library instead of memory the library allocates.  Its results must equal
+fd3d_run's (whose fused fault-boundary kernel keeps that scratch in shared memory) bit
+for bit, over two calls in a row.
 
 This file is named so that pytest collects it last.
 """
@@ -54,3 +55,30 @@ def test_noalloc_rejects_planes_over_the_limit():
     s = Solver(m)
     assert _noalloc(s, 1) == -1
     assert s.steps_done() == 0
+
+
+def test_noalloc_leaves_device_memory_unchanged():
+    """A call after set-up allocates no device memory: the device's free memory is the same
+    before and after it (measured around the second call, after the first has loaded the
+    kernels it launches), and fd3d_run afterwards still agrees with a context that only
+    ever ran fd3d_run."""
+    import torch
+    m = configs.tiny_sw(nsteps=60)
+    ref = Solver(m)
+    new = Solver(m)
+    assert _noalloc(new, 20) == 0
+    new.sync()
+    torch.cuda.mem_get_info(0)      # the first query sets up the caller's view of the device
+    free0, _ = torch.cuda.mem_get_info(0)
+    assert _noalloc(new, 20) == 0
+    new.sync()
+    free1, _ = torch.cuda.mem_get_info(0)
+    assert free1 == free0, (free0, free1)
+    new.run(20)
+    new.sync()
+    ref.run(60)
+    ref.sync()
+    for f in range(ref.nf):
+        np.testing.assert_array_equal(new.history(f), ref.history(f), err_msg=f"field {f}")
+    for name in ("tx", "tz", "slipX", "distX", "ruptime"):
+        np.testing.assert_array_equal(new.plane(name), ref.plane(name), err_msg=name)
