@@ -52,8 +52,7 @@ using namespace fd3d;
 namespace {
 
 enum WorkType : int {
-    W_VEL_INT = 0, W_VEL_FAULT, W_VEL_PML, W_VEL_FS, W_STR_INT, W_STR_FAULT, W_STR_PML, W_STR_FS, W_FBC, W_NUC,
-    W_VEL_PMLS, W_STR_PMLS  // slab marches of the y and z PML strips
+    W_VEL_INT = 0, W_VEL_FAULT, W_VEL_PML, W_VEL_FS, W_STR_INT, W_STR_FAULT, W_STR_PML, W_STR_FS, W_FBC, W_NUC
 };
 constexpr int NPHASE = 5;
 
@@ -139,16 +138,10 @@ k_batch(const ModelDev* __restrict__ models, const ModelMaps* __restrict__ maps,
     float* ring = reinterpret_cast<float*>(smem_raw + ((128u - (smem_addr(smem_raw) & 127u)) & 127u));
     __shared__ __align__(8) uint64_t bars[TMA_NS];
     __shared__ __align__(8) uint64_t pbar;  // PML tiles staged through the ring memory
-    __shared__ __align__(8) uint64_t sbar[2];  // PML slab planes staged through the ring memory
-    if (threadIdx.x == 0 && threadIdx.y == 0) {
-        mbar_init(smem_addr(&pbar), 1);
-        mbar_init(smem_addr(&sbar[0]), 1);
-        mbar_init(smem_addr(&sbar[1]), 1);
-    }
+    if (threadIdx.x == 0 && threadIdx.y == 0) mbar_init(smem_addr(&pbar), 1);
     tma_ring_init(bars);
     unsigned pc = 0;  // planes this CTA has put through its ring
     unsigned pt = 0;  // PML tiles this CTA has staged (mbarrier phase = pt & 1)
-    unsigned ps = 0;  // PML slab planes this CTA has staged (vel_pml_slab)
     const unsigned nb = gridDim.x;
     for (int s = 0; s < nsteps; ++s) {
         for (int ph = 0; ph < NPHASE; ++ph) {
@@ -172,12 +165,6 @@ k_batch(const ModelDev* __restrict__ models, const ModelMaps* __restrict__ maps,
                         ok = vel_pml_tile<float>(M.g, M.f, M.D, M.X, M.c, it.bx, ring, smem_addr(&pbar), pt & 1u,
                                                  gstatus);
                         ++pt;
-                        break;
-                    case W_VEL_PMLS:
-                        ok = vel_pml_slab_cta<float>(M.g, M.f, M.D, M.X, M.c, it.bx, ring, sbar, ps, gstatus);
-                        break;
-                    case W_STR_PMLS:
-                        ok = str_pml_slab_cta<float>(M.g, M.f, M.D, M.X, M.c, it.bx, ring, sbar, ps, gstatus);
                         break;
                     case W_VEL_FS: vel_fs_body<float>(M.g, M.f, it.bx, it.by, 0); break;
                     case W_STR_INT:
@@ -233,7 +220,7 @@ __global__ void k_check_grid_barrier(BatchSync* sync, int* status) {
 // order, and k_step_end advances the run's step counter (items of a model whose
 // step limit is reached return at once).  Each kernel gets its own register and
 // shared-memory budget, so each region runs at its own occupancy.
-constexpr int NTYPES = 12;
+constexpr int NTYPES = 10;
 
 __device__ __forceinline__ bool item_live(const Work& it, const int* limit, const int* run_step, int& m) {
     m = it.tm >> 8;
@@ -275,29 +262,6 @@ __global__ void __launch_bounds__(PML_TILE, STRESS ? 3 : 4) k_bpml(const ModelDe
     const ModelDev& M = models[m];
     if (STRESS) str_pml_tile<float>(M.g, M.f, M.D, M.X, M.c, it.bx, sm, smem_addr(&bar), 0u, gstatus);
     else vel_pml_tile<float>(M.g, M.f, M.D, M.X, M.c, it.bx, sm, smem_addr(&bar), 0u, gstatus);
-}
-
-// one PML slab per CTA (dynamic shared memory: pml_slab_smem<float>(STRESS))
-template <bool STRESS>
-__global__ void __launch_bounds__(256, 3) k_bpmls(const ModelDev* __restrict__ models, const Work* __restrict__ work,
-                                               int b0, const int* __restrict__ limit, const int* run_step,
-                                               int* gstatus) {
-    extern __shared__ __align__(128) unsigned char smem_raw[];
-    float* ring = reinterpret_cast<float*>(smem_raw + ((128u - (smem_addr(smem_raw) & 127u)) & 127u));
-    __shared__ __align__(8) uint64_t sbar[2];
-    const Work it = work[b0 + blockIdx.x];
-    int m;
-    if (!item_live(it, limit, run_step, m)) return;
-    if (threadIdx.x == 0 && threadIdx.y == 0) {
-        mbar_init(smem_addr(&sbar[0]), 1);
-        mbar_init(smem_addr(&sbar[1]), 1);
-        fence_mbar_init();
-    }
-    __syncthreads();
-    const ModelDev& M = models[m];
-    unsigned ps = 0;
-    if (STRESS) str_pml_slab_cta<float>(M.g, M.f, M.D, M.X, M.c, it.bx, ring, sbar, ps, gstatus);
-    else vel_pml_slab_cta<float>(M.g, M.f, M.D, M.X, M.c, it.bx, ring, sbar, ps, gstatus);
 }
 
 __global__ void __launch_bounds__(256) k_bplane(const ModelDev* __restrict__ models, const Work* __restrict__ work,
@@ -526,14 +490,10 @@ void build_model_items(Model& M, int m, int kch) {
     const int fx = (std::max(nxT, p.nxt) + 31) / 32, fz = (nzT + 7) / 8;
     for (int y = 0; y < fz; ++y)
         for (int x = 0; x < fx; ++x) per[0].push_back(Work{tm | W_VEL_FAULT, x, y, 0});
-    const int npml = (int)(M.dev.D.cum[2] / PML_TILE);  // tiles of the x strips
+    const int npml = (int)((M.dev.D.cum[PML_MAXS] + PML_TILE - 1) / PML_TILE);
     for (int x = 0; x < npml; ++x) {
         per[0].push_back(Work{tm | W_VEL_PML, x, 0, 0});
         per[2].push_back(Work{tm | W_STR_PML, x, 0, 0});
-    }
-    for (int x = 0; x < M.dev.D.scum[PML_MAXS]; ++x) {  // slabs of the y and z strips
-        per[0].push_back(Work{tm | W_VEL_PMLS, x, 0, 0});
-        per[2].push_back(Work{tm | W_STR_PMLS, x, 0, 0});
     }
     const int sx = (p.nxt + 31) / 32, sy = p.fspace ? 0 : (p.nyt + 7) / 8;  // no fuvw/fres under FSPACE
     for (int y = 0; y < sy; ++y)
@@ -672,15 +632,6 @@ int enqueue_graph_step(fd3d_batch* b) {
                     b->d_models, b->d_maps, b->d_work_t, b->tbeg[ti], b->d_limit, b->d_run_step, kc, b->d_status);
         }
         plane(b->side[0], tf, tf + 1);
-        const int tq = half ? W_STR_PMLS : W_VEL_PMLS;
-        if (n_of(tq) > 0) {  // PML slabs, then tiles, on the PML branch
-            if (half)
-                k_bpmls<true><<<n_of(tq), blk, pml_slab_smem<float>(true), b->side[1]>>>(
-                    b->d_models, b->d_work_t, b->tbeg[tq], b->d_limit, b->d_run_step, b->d_status);
-            else
-                k_bpmls<false><<<n_of(tq), blk, pml_slab_smem<float>(false), b->side[1]>>>(
-                    b->d_models, b->d_work_t, b->tbeg[tq], b->d_limit, b->d_run_step, b->d_status);
-        }
         if (n_of(tp) > 0) {
             if (half)
                 k_bpml<true><<<n_of(tp), blk, 0, b->side[1]>>>(b->d_models, b->d_work_t, b->tbeg[tp], b->d_limit,

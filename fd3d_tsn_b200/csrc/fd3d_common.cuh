@@ -43,10 +43,6 @@ struct Strip {
     int ox_off, oxS_off, oy_off, oyS_off, oz_off, ozS_off;  // offsets into the profile table
     float rni, rnj;                    // 1/ni, 1/(jend_uw-nyb+1) for the index split (udiv_small)
     int fastdiv;                       // the strip's u/w range has fewer than 2^24 cells
-    // slab marches (y and z strips, pml_slab in fd3d_kernels.cuh): rows rlo..rhi (k for the y
-    // strip, j for the z strips, u/w range), march mlo..mhi (j, resp. k), nib blocks of 32 i
-    // and nrb blocks of 8 rows
-    int rlo, rhi, mlo, mhi, nib, nrb;
 };
 
 // 24 split components per strip: u(3) v(3) w(3) xx(3) yy(3) zz(3) xy(2) xz(2) yz(2)

@@ -173,7 +173,7 @@ struct CtxBase {
     bool split_bc = false;
     float last_ms = 0.f;
     bool profiling = false;
-    int pml_minb_vel = 1, pml_minb_str = 4;  // register caps of the x-strip PML tiles (CTAs per SM; both fit unspilled)
+    int pml_minb_vel = 1, pml_minb_str = 3;  // register caps of the PML sweeps (CTAs per SM; 3 keeps the stress sweep unspilled)
     std::vector<cudaEvent_t> kev;   // 2 per kernel id
     float ktimes[FD3D_NKERNELS] = {0};
     int klaunch[FD3D_NKERNELS] = {0};
@@ -325,7 +325,6 @@ struct Ctx : CtxBase {
         if (dalloc(&dprof, prof.size())) return FD3D_ERR_NOMEM;
         CK(cudaMemcpyAsync(dprof, prof.data(), prof.size() * sizeof(Damp<T>), cudaMemcpyHostToDevice, st));
         X.prof = dprof;
-        if (!prepare_pml_slab_kernels<T>()) return FD3D_ERR_CUDA;
         tma_ok = make_interior_maps<T>(g, f, vmaps, smaps) && prepare_tma_kernels<T>();
         if (!tma_ok && icfg.variant == IV_TMA) {
             std::fprintf(stderr, "fd3d: tensor maps of the interior sweeps could not be encoded for this grid; "

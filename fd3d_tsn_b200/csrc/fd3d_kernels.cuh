@@ -161,18 +161,15 @@ struct PmlDesc {
     Strip s[PML_MAXS];
     long long cum[PML_MAXS + 1];  // first compact index of each strip (a multiple of PML_TILE); cum[PML_MAXS] = end
     long long cnt[PML_MAXS];      // cells of each strip's u/w loop range (0 for an absent strip)
-    int scum[PML_MAXS + 1];       // slab CTAs before each strip (the y and z strips march in slabs)
     int ns;                       // strips present: 4, or 5 under FSPACE
 };
 
 // PML auxiliary components (the 24 split fields that init_pml allocates per strip,
-// fd3d_deriv.f90:1330-1406, 1413-1437) are stored in tiles of PML_TILE cells, in blocks of
+// fd3d_deriv.f90:1330-1406, 1413-1437) are indexed by the compact cell index t of the
+// u/w loop ranges of the strips (strip s holds t in [cum[s], cum[s] + cnt[s]); each strip
+// starts on a PML_TILE boundary, so every tile lies in one strip) and stored in blocks of
 // 32 cells: inside a block the 32 values of one component are contiguous and the
-// components of a group follow each other.  Each strip starts on a tile boundary (strip s
-// holds the cells [cum[s], cum[s+1])).  The x strips (1, 2) order their cells by the
-// compact index of their u/w loop ranges (i fastest); the y and z strips order them by
-// slab: tile ((m - mlo)*nrb + rb)*nib + ib holds plane m of the 32 x 8 block (ib, rb) of
-// (i, row) cells, row ty of the block in the tile's block ty.  The velocity group (u,v,w splits, 9
+// components of a group follow each other.  The velocity group (u,v,w splits, 9
 // components) and the stress group (xx,yy,zz,xy,xz,yz splits, 15) are separate spans,
 // so the auxiliaries of PML_TILE consecutive cells are one contiguous range per group:
 // one bulk copy brings a tile's range into shared memory.
@@ -349,13 +346,17 @@ __device__ __forceinline__ bool vel_pml_tile_c(const Grid& g, const Fields<T>& f
 // pml_uvw: split-field PML velocity in the strips (fd3d_deriv.f90:1927-2293), one
 // tile of PML_TILE consecutive cells per CTA of PML_TILE threads.  Returns false if the
 // staging copy timed out.
-// Tiles cover the x strips (class 0); the y and z strips march in slabs (vel_pml_slab).
 template <class T>
 __device__ __forceinline__ bool vel_pml_tile(const Grid& g, const Fields<T>& f, const PmlDesc& D, const PmlAux<T>& X,
                                              const StepConst<T>& c, int tile, T* sm, uint32_t bar, uint32_t parity,
                                              int* status) {
     const long long t0 = (long long)tile * PML_TILE;
-    return vel_pml_tile_c<T, 0>(g, f, D, X, c, pml_tile_strip(D, t0), t0, sm, bar, parity, status);
+    const int s = pml_tile_strip(D, t0);
+    switch (pml_class(s)) {
+        case 0: return vel_pml_tile_c<T, 0>(g, f, D, X, c, s, t0, sm, bar, parity, status);
+        case 1: return vel_pml_tile_c<T, 1>(g, f, D, X, c, s, t0, sm, bar, parity, status);
+        default: return vel_pml_tile_c<T, 2>(g, f, D, X, c, s, t0, sm, bar, parity, status);
+    }
 }
 
 // fuvw at the ghost row k=ks+1 (fd3d_deriv.f90:1018-1062).  w needs u and v of the
@@ -576,325 +577,13 @@ __device__ __forceinline__ bool str_pml_tile(const Grid& g, const Fields<T>& f, 
                                              const StepConst<T>& c, int tile, T* sm, uint32_t bar, uint32_t parity,
                                              int* status) {
     const long long t0 = (long long)tile * PML_TILE;
-    return str_pml_tile_c<T, 0>(g, f, D, X, c, pml_tile_strip(D, t0), t0, sm, bar, parity, status);
+    const int s = pml_tile_strip(D, t0);
+    switch (pml_class(s)) {
+        case 0: return str_pml_tile_c<T, 0>(g, f, D, X, c, s, t0, sm, bar, parity, status);
+        case 1: return str_pml_tile_c<T, 1>(g, f, D, X, c, s, t0, sm, bar, parity, status);
+        default: return str_pml_tile_c<T, 2>(g, f, D, X, c, s, t0, sm, bar, parity, status);
+    }
 }
-
-// ---------------------------------------------------------------- PML slab marches
-// The y strip (class 1) and the z strips (class 2) are nabc-1 cells thick in y or z and
-// long in the other two directions.  A CTA of 32 x 8 threads owns 32 consecutive i and 8
-// consecutive rows (k for the y strip, j for the z strips) and marches the strip's
-// thickness (j, resp. k) plane by plane.  The field values a cell shares with its
-// neighbour along the march are carried in registers, the next plane's other field values
-// are loaded while the current plane is computed, and each plane's split components (one
-// 256-cell tile of the aux pool) are staged into a two-slot shared-memory ring by a bulk
-// copy, the plane after next issued as soon as a slot is free.  The arithmetic and its
-// order are those of vel_pml_tile_c / str_pml_tile_c, so the results are the same bits.
-
-// slot and mbarrier phase of the n-th plane a CTA stages through its two-slot ring
-__device__ __forceinline__ int slab_slot(unsigned n) { return (int)(n & 1u); }
-__device__ __forceinline__ uint32_t slab_parity(unsigned n) { return (n >> 1) & 1u; }
-
-// strip and slab index within the strip of slab CTA b (slab strips only)
-__device__ __forceinline__ int pml_slab_strip(const PmlDesc& D, int b, int& slab) {
-    int s = 2;
-    while (s < PML_MAXS - 1 && b >= D.scum[s + 1]) ++s;
-    slab = b - D.scum[s];
-    return s;
-}
-
-// one thread stages plane q of the slab (aux tile tq) into ring slot `slot`
-template <class T>
-__device__ __forceinline__ void slab_stage(T* slot, const T* src, int ncomp, uint32_t bar) {
-    const uint32_t bytes = PML_TILE * ncomp * (uint32_t)sizeof(T);
-    mbar_expect_tx(bar, bytes);
-    bulk_load(smem_addr(slot), src, bytes, bar);
-}
-
-// bounded wait for plane n on every thread; on a time-out every thread returns false after
-// the leader recorded ST_TIMEOUT and waited (bounded) for the plane still in flight
-__device__ __forceinline__ bool slab_wait(const uint64_t* sbar, unsigned n, bool more, int* status) {
-    const bool ok = mbar_wait(smem_addr(&sbar[slab_slot(n)]), slab_parity(n));
-    if (__syncthreads_or(!ok)) {
-        if (threadIdx.x == 0 && threadIdx.y == 0) {
-            atomicOr(status, ST_TIMEOUT);
-            mbar_wait(smem_addr(&sbar[slab_slot(n)]), slab_parity(n));
-            if (more) mbar_wait(smem_addr(&sbar[slab_slot(n + 1)]), slab_parity(n + 1));
-        }
-        __syncthreads();
-        return false;
-    }
-    return true;
-}
-
-template <class T>
-struct VelPlane { T xx0, xx1, xy0, xy1, xy2, xz0, xz1, xz2, yz0, yz1, yz2, zz0, zz1, yy0, yy1, d, vold; };
-
-// pml_uvw of one slab (fd3d_deriv.f90:1927-2293).  C = 1: the y strip, marching j over k-rows;
-// C = 2: a z strip, marching k over j-rows.  ring: two slots of PML_TILE * AUX_NV elements;
-// sbar: their two mbarriers; ps: planes this CTA staged so far.  Returns false on a time-out.
-template <class T, int C>
-__device__ __forceinline__ bool vel_pml_slab(const Grid& g, const Fields<T>& f, const PmlDesc& D, const PmlAux<T>& X,
-                                             const StepConst<T>& c, int s, int slab, T* ring, uint64_t* sbar,
-                                             unsigned& ps, int* status) {
-    constexpr int MX = split_mode(C, 0), MY = split_mode(C, 1), MZ = split_mode(C, 2);
-    const Strip& S = D.s[s];
-    const int tx = threadIdx.x, ty = threadIdx.y, l = ty * 32 + tx;
-    const bool leader = (l == 0);
-    const int ib = slab % S.nib, rb = slab / S.nib;
-    const int i = S.nxb + ib * 32 + tx, r = S.rlo + rb * 8 + ty;
-    const bool act = i <= S.nxe && r <= S.rhi;
-    const long long sy = g.px, sz = g.plane, dm = (C == 1) ? sy : sz;
-    const int nm = S.mhi - S.mlo + 1;
-    const long long tile0 = D.cum[s] / PML_TILE + (long long)rb * S.nib + ib, tstep = (long long)S.nrb * S.nib;
-    const bool dov = (C == 1) || (r <= S.nye);
-    const unsigned p0 = ps;
-    // stage the first two planes (the slots may still be read by this CTA's previous item)
-    fence_proxy_async_smem();
-    __syncthreads();
-    if (leader) {
-        fence_proxy_async_global();
-        for (int q = 0; q < nm && q < 2; ++q)
-            slab_stage(ring + (size_t)slab_slot(p0 + q) * PML_TILE * AUX_NV, X.vel + (tile0 + q * tstep) * PML_TILE * AUX_NV,
-                       AUX_NV, smem_addr(&sbar[slab_slot(p0 + q)]));
-    }
-    Damp<T> ox{}, oxS{}, oyr{};
-    if (act) {
-        ox = X.prof[S.ox_off + i - S.nxb];
-        oxS = X.prof[S.oxS_off + i - S.nxb];
-        if (C == 2) oyr = X.prof[S.oy_off + r - S.nyb];
-    }
-    // warp-uniform over the whole march: x damping depends on i only, y damping of a z strip on j
-    const bool wx = __any_sync(0xffffffffu, ox.o != (T)0 || oxS.o != (T)0);
-    const bool wy = (C == 2) && __any_sync(0xffffffffu, oyr.o != (T)0);
-    const int jm = (C == 1) ? S.mlo : r, km = (C == 1) ? r : S.mlo;  // cell of the first plane
-    long long p = act ? g.at(i, jm, km) : 0;
-    auto load_new = [&](VelPlane<T>& v, long long q, int jq) {
-        v.xx0 = f.xx[q]; v.xx1 = f.xx[q - 1]; v.xy0 = f.xy[q];
-        v.xz0 = f.xz[q]; v.xz2 = f.xz[q + 1]; v.yz0 = f.yz[q]; v.zz1 = f.zz[q + sz];
-        if (C == 2) { v.xy1 = f.xy[q - sy]; v.yz1 = f.yz[q - sy]; }
-        else        { v.xz1 = f.xz[q - sz]; v.yz2 = f.yz[q - sz]; v.zz0 = f.zz[q]; }
-        if (dov) {  // v, xy, yz rows end at nye (the fault plane has u, w only)
-            v.xy2 = f.xy[q + 1]; v.yy0 = f.yy[q + sy];
-            if (C == 2) v.yy1 = f.yy[q];
-        }
-        if (!f.lay) v.d = f.d[q];
-        v.vold = (C == 2 && jq == g.nyt - 1) ? f.v[q] : (T)0;
-    };
-    VelPlane<T> cur{}, nxt{};
-    if (act) {
-        load_new(cur, p, jm);
-        if (C == 2) { cur.xz1 = f.xz[p - sz]; cur.yz2 = f.yz[p - sz]; cur.zz0 = f.zz[p]; }
-        else        { cur.xy1 = f.xy[p - sy]; cur.yz1 = f.yz[p - sy]; cur.yy1 = f.yy[p]; }
-    }
-    const T dt = c.dt, dh = c.dh, rdh = c.rdh;
-    for (int q = 0; q < nm; ++q) {
-        const unsigned n = p0 + (unsigned)q;
-        const int m = S.mlo + q;
-        const int j = (C == 1) ? m : r, k = (C == 1) ? r : m;
-        if (act && q + 1 < nm) load_new(nxt, p + dm, (C == 1) ? m + 1 : r);
-        Damp<T> oy = oyr, oz{};
-        if (C == 1) oy = X.prof[S.oy_off + j - S.nyb];   // plane-uniform
-        if (C == 2) oz = X.prof[S.oz_off + k - S.nzb];
-        if (!slab_wait(sbar, n, q + 1 < nm, status)) return false;
-        if (act) {
-            const T* sm = ring + (size_t)slab_slot(n) * PML_TILE * AUX_NV;
-            T* gaux = X.vel + (tile0 + q * tstep) * PML_TILE * AUX_NV;
-            const T rr = f.lay ? f.lay[4 * g.nzt + k - 1] : dt / cur.d;
-            auto inc = [&](T diff) { return div_pre(rr * diff, dh, rdh); };
-            auto put = [&](int comp, T a) { gaux[aux_sm(l, AUX_NV, comp)] = a; return a; };
-            auto aux = [&](int comp) { return sm[aux_sm(l, AUX_NV, comp)]; };
-            const VelPlane<T>& v = cur;
-            const T u0 = put(AX_U0, pml_split<T, MX>(aux(AX_U0), inc(v.xx0 - v.xx1), ox, wx));
-            const T u1 = put(AX_U1, pml_split<T, MY>(aux(AX_U1), inc(v.xy0 - v.xy1), oy, wy));
-            const T u2 = put(AX_U2, pml_split<T, MZ>(aux(AX_U2), inc(v.xz0 - v.xz1), oz, false));
-            const T w0 = put(AX_W0, pml_split<T, MX>(aux(AX_W0), inc(v.xz2 - v.xz0), oxS, wx));
-            const T w1 = put(AX_W1, pml_split<T, MY>(aux(AX_W1), inc(v.yz0 - v.yz1), oy, wy));
-            const T w2 = put(AX_W2, pml_split<T, MZ>(aux(AX_W2), inc(v.zz1 - v.zz0), oz, false));
-            f.u[p] = u0 + u1 + u2;
-            f.w[p] = w0 + w1 + w2;
-            if (dov) {
-                const T v0 = put(AX_V0, pml_split<T, MX>(aux(AX_V0), inc(v.xy2 - v.xy0), oxS, wx));
-                const T v1 = put(AX_V1, pml_split<T, MY>(aux(AX_V1), inc(v.yy0 - v.yy1), oy, wy));
-                const T v2 = put(AX_V2, pml_split<T, MZ>(aux(AX_V2), inc(v.yz0 - v.yz2), oz, false));
-                if (C == 2 && j == g.nyt - 1) f.v[p + sy] = v.vold;  // bnd2d mirror of the value before this update
-                f.v[p] = v0 + v1 + v2;
-            }
-        }
-        fence_proxy_async_smem();
-        __syncthreads();  // every thread is done with the slot
-        if (leader && q + 2 < nm) {
-            fence_proxy_async_global();
-            slab_stage(ring + (size_t)slab_slot(n) * PML_TILE * AUX_NV, X.vel + (tile0 + (q + 2) * tstep) * PML_TILE * AUX_NV,
-                       AUX_NV, smem_addr(&sbar[slab_slot(n)]));
-        }
-        if (q + 1 < nm) {  // march: the neighbour behind the next cell is this cell
-            if (C == 2) { nxt.xz1 = cur.xz0; nxt.yz2 = cur.yz0; nxt.zz0 = cur.zz1; }
-            else        { nxt.xy1 = cur.xy0; nxt.yz1 = cur.yz0; nxt.yy1 = cur.yy0; }
-            cur = nxt;
-            p += dm;
-        }
-    }
-    ps = p0 + (unsigned)nm;
-    return true;
-}
-
-template <class T>
-struct StrPlane { T ux, uy, uz, up, vp, vx, vy, vz, wp, wx, wy, wz, xl, xm, mz, my, md, xyo, yzo; };
-
-// pml_xyz of one slab (fd3d_deriv.f90:2304-3143), as vel_pml_slab; ring slots of PML_TILE * AUX_NS
-template <class T, int C>
-__device__ __forceinline__ bool str_pml_slab(const Grid& g, const Fields<T>& f, const PmlDesc& D, const PmlAux<T>& X,
-                                             const StepConst<T>& c, int s, int slab, T* ring, uint64_t* sbar,
-                                             unsigned& ps, int* status) {
-    constexpr int MX = split_mode(C, 0), MY = split_mode(C, 1), MZ = split_mode(C, 2);
-    const Strip& S = D.s[s];
-    const int tx = threadIdx.x, ty = threadIdx.y, l = ty * 32 + tx;
-    const bool leader = (l == 0);
-    const int ib = slab % S.nib, rb = slab / S.nib;
-    const int i = S.nxb + ib * 32 + tx, r = S.rlo + rb * 8 + ty;
-    const bool act = i <= S.nxe && r <= S.rhi;
-    const long long sy = g.px, sz = g.plane, dm = (C == 1) ? sy : sz;
-    const int nm = S.mhi - S.mlo + 1;
-    const long long tile0 = D.cum[s] / PML_TILE + (long long)rb * S.nib + ib, tstep = (long long)S.nrb * S.nib;
-    const bool dxy = (C == 1) || (r <= S.nye);
-    const unsigned p0 = ps;
-    fence_proxy_async_smem();
-    __syncthreads();
-    if (leader) {
-        fence_proxy_async_global();
-        for (int q = 0; q < nm && q < 2; ++q)
-            slab_stage(ring + (size_t)slab_slot(p0 + q) * PML_TILE * AUX_NS, X.str + (tile0 + q * tstep) * PML_TILE * AUX_NS,
-                       AUX_NS, smem_addr(&sbar[slab_slot(p0 + q)]));
-    }
-    Damp<T> ox{}, oxS{}, oyr{}, oySr{};
-    if (act) {
-        ox = X.prof[S.ox_off + i - S.nxb];
-        oxS = X.prof[S.oxS_off + i - S.nxb];
-        if (C == 2) { oyr = X.prof[S.oy_off + r - S.nyb]; oySr = X.prof[S.oyS_off + r - S.nyb]; }
-    }
-    const bool dx = __any_sync(0xffffffffu, ox.o != (T)0 || oxS.o != (T)0);
-    const bool dy = (C == 2) && __any_sync(0xffffffffu, oyr.o != (T)0 || oySr.o != (T)0);
-    const int jm = (C == 1) ? S.mlo : r, km = (C == 1) ? r : S.mlo;
-    long long p = act ? g.at(i, jm, km) : 0;
-    // values of plane q at cell q_ (k = kq, j = jq); the medium of a y-strip row is constant
-    auto load_new = [&](StrPlane<T>& v, long long q_, int kq, int jq) {
-        v.ux = f.u[q_ + 1]; v.uz = f.u[q_ + sz]; v.vz = f.v[q_ + sz];  // vz is the next plane's vp
-        v.wx = f.w[q_ - 1];
-        if (C == 2) { v.vy = f.v[q_ - sy]; v.wp = f.w[q_]; }
-        else        { v.vp = f.v[q_]; v.wz = f.w[q_ - sz]; }
-        if (f.lay) {
-            v.xl = f.lay[kq - 1]; v.xm = f.lay[g.nzt + kq - 1]; v.mz = f.lay[g.nzt + kq];
-            v.my = v.xm; v.md = v.mz;
-        } else {
-            v.xl = f.lam[q_]; v.xm = f.mu[q_]; v.mz = f.mu[q_ + sz];
-        }
-        if (dxy) {  // xy and yz rows end at nye (the fault plane has the normal stresses and xz only)
-            v.uy = f.u[q_ + sy]; v.vx = f.v[q_ - 1]; v.wy = f.w[q_ + sy];
-            if (!f.lay) { v.my = f.mu[q_ + sy]; v.md = f.mu[q_ + 1 + sy + sz]; }
-        }
-        if (C == 2 && jq == g.nyt - 1) { v.xyo = f.xy[q_]; v.yzo = f.yz[q_]; }
-    };
-    StrPlane<T> cur{}, nxt{};
-    if (act) {
-        load_new(cur, p, km, jm);
-        if (C == 2) { cur.up = f.u[p]; cur.vp = f.v[p]; cur.wz = f.w[p - sz]; }
-        else        { cur.up = f.u[p]; cur.vy = f.v[p - sy]; cur.wp = f.w[p]; }
-    }
-    const T dt = c.dt, dh = c.dh, rdh = c.rdh;
-    for (int q = 0; q < nm; ++q) {
-        const unsigned n = p0 + (unsigned)q;
-        const int m = S.mlo + q;
-        const int j = (C == 1) ? m : r, k = (C == 1) ? r : m;
-        if (act && q + 1 < nm) load_new(nxt, p + dm, (C == 1) ? r : m + 1, (C == 1) ? m + 1 : r);
-        Damp<T> oy = oyr, oyS = oySr, oz{}, ozS{};
-        if (C == 1) { oy = X.prof[S.oy_off + j - S.nyb]; oyS = X.prof[S.oyS_off + j - S.nyb]; }
-        if (C == 2) { oz = X.prof[S.oz_off + k - S.nzb]; ozS = X.prof[S.ozS_off + k - S.nzb]; }
-        if (!slab_wait(sbar, n, q + 1 < nm, status)) return false;
-        if (act) {
-            const T* sm = ring + (size_t)slab_slot(n) * PML_TILE * AUX_NS;
-            T* gaux = X.str + (tile0 + q * tstep) * PML_TILE * AUX_NS;
-            const StrPlane<T>& v = cur;
-            const bool top = !g.fspace && (C <= 1) && (k == S.nze);  // xz/yz aux zeroed at the top row of strip 3
-            const T a = v.xl + (T)2 * v.xm, b = v.xl;
-            const T diff1 = v.ux - v.up, diff2 = v.vp - v.vy, diff3 = v.wp - v.wz;
-            auto inc = [&](T mod, T diff) { return div_pre(dt * mod * diff, dh, rdh); };
-            auto aux = [&](int comp) { return sm[aux_sm(l, AUX_NS, comp - AUX_NV)]; };
-            auto put = [&](int comp, T x_) { gaux[aux_sm(l, AUX_NS, comp - AUX_NV)] = x_; return x_; };
-            const T x0 = put(AX_XX0, pml_split<T, MX>(aux(AX_XX0), inc(a, diff1), oxS, dx));
-            const T x1 = put(AX_XX1, pml_split<T, MY>(aux(AX_XX1), inc(b, diff2), oy, dy));
-            const T x2 = put(AX_XX2, pml_split<T, MZ>(aux(AX_XX2), inc(b, diff3), oz, false));
-            f.xx[p] = x0 + x1 + x2;
-            const T y0 = put(AX_YY0, pml_split<T, MX>(aux(AX_YY0), inc(b, diff1), oxS, dx));
-            const T y1 = put(AX_YY1, pml_split<T, MY>(aux(AX_YY1), inc(a, diff2), oy, dy));
-            const T y2 = put(AX_YY2, pml_split<T, MZ>(aux(AX_YY2), inc(b, diff3), oz, false));
-            f.yy[p] = y0 + y1 + y2;
-            const T z0 = put(AX_ZZ0, pml_split<T, MX>(aux(AX_ZZ0), inc(b, diff1), oxS, dx));
-            const T z1 = put(AX_ZZ1, pml_split<T, MY>(aux(AX_ZZ1), inc(b, diff2), oy, dy));
-            const T z2 = put(AX_ZZ2, pml_split<T, MZ>(aux(AX_ZZ2), inc(a, diff3), oz, false));
-            f.zz[p] = z0 + z1 + z2;
-            {   // xz (j up to jend_uw)
-                const T xmu = (v.xm + v.mz) / (T)2;
-                const T q0 = put(AX_XZ0, pml_split<T, MZ>(aux(AX_XZ0), inc(xmu, v.uz - v.up), ozS, false));
-                const T q1 = put(AX_XZ1, pml_split<T, MX>(aux(AX_XZ1), inc(xmu, v.wp - v.wx), ox, dx));
-                f.xz[p] = q0 + q1;
-                if (top) { put(AX_XZ0, (T)0); put(AX_XZ1, (T)0); }
-            }
-            if (dxy) {
-                T xmu = (v.xm + v.my) / (T)2;
-                const T e0 = put(AX_XY0, pml_split<T, MY>(aux(AX_XY0), inc(xmu, v.uy - v.up), oyS, dy));
-                const T e1 = put(AX_XY1, pml_split<T, MX>(aux(AX_XY1), inc(xmu, v.vp - v.vx), ox, dx));
-                xmu = (v.xm + v.md) / (T)2;
-                const T h0 = put(AX_YZ0, pml_split<T, MZ>(aux(AX_YZ0), inc(xmu, v.vz - v.vp), ozS, false));
-                const T h1 = put(AX_YZ1, pml_split<T, MY>(aux(AX_YZ1), inc(xmu, v.wy - v.wp), oyS, dy));
-                if (C == 2 && j == g.nyt - 1) { f.xy[p + sy] = v.xyo; f.yz[p + sy] = v.yzo; }  // strbnd mirror
-                f.xy[p] = e0 + e1;
-                f.yz[p] = h0 + h1;
-                if (top) { put(AX_YZ0, (T)0); put(AX_YZ1, (T)0); }
-            }
-        }
-        fence_proxy_async_smem();
-        __syncthreads();
-        if (leader && q + 2 < nm) {
-            fence_proxy_async_global();
-            slab_stage(ring + (size_t)slab_slot(n) * PML_TILE * AUX_NS, X.str + (tile0 + (q + 2) * tstep) * PML_TILE * AUX_NS,
-                       AUX_NS, smem_addr(&sbar[slab_slot(n)]));
-        }
-        if (q + 1 < nm) {
-            if (C == 2) { nxt.up = cur.uz; nxt.vp = cur.vz; nxt.wz = cur.wp; }
-            else        { nxt.up = cur.uy; nxt.vy = cur.vp; nxt.wp = cur.wy; }
-            cur = nxt;
-            p += dm;
-        }
-    }
-    ps = p0 + (unsigned)nm;
-    return true;
-}
-
-// CTA b of a slab sweep: its strip, its class, the march
-template <class T>
-__device__ __forceinline__ bool vel_pml_slab_cta(const Grid& g, const Fields<T>& f, const PmlDesc& D,
-                                                 const PmlAux<T>& X, const StepConst<T>& c, int b, T* ring,
-                                                 uint64_t* sbar, unsigned& ps, int* status) {
-    int slab;
-    const int s = pml_slab_strip(D, b, slab);
-    if (pml_class(s) == 1) return vel_pml_slab<T, 1>(g, f, D, X, c, s, slab, ring, sbar, ps, status);
-    return vel_pml_slab<T, 2>(g, f, D, X, c, s, slab, ring, sbar, ps, status);
-}
-template <class T>
-__device__ __forceinline__ bool str_pml_slab_cta(const Grid& g, const Fields<T>& f, const PmlDesc& D,
-                                                 const PmlAux<T>& X, const StepConst<T>& c, int b, T* ring,
-                                                 uint64_t* sbar, unsigned& ps, int* status) {
-    int slab;
-    const int s = pml_slab_strip(D, b, slab);
-    if (pml_class(s) == 1) return str_pml_slab<T, 1>(g, f, D, X, c, s, slab, ring, sbar, ps, status);
-    return str_pml_slab<T, 2>(g, f, D, X, c, s, slab, ring, sbar, ps, status);
-}
-
-// shared memory of a slab CTA: two aux slots (+ alignment slack)
-template <class T>
-constexpr int pml_slab_smem(bool stress) { return 2 * PML_TILE * (stress ? AUX_NS : AUX_NV) * (int)sizeof(T) + 128; }
-
-
 
 // fres (fd3d_deriv.f90:1067-1104)
 template <class T>
@@ -1493,49 +1182,11 @@ __global__ void __launch_bounds__(PML_TILE, MINB) k_str_pml(Grid g, Fields<T> f,
     str_pml_tile<T>(g, f, D, X, c, blockIdx.x, sm, smem_addr(&bar), 0u, status);
 }
 
-// One slab of the y or z strips per CTA of 32 x 8 threads (dynamic shared memory:
-// pml_slab_smem<T>(STRESS)).  FP32: capped at 80 registers so that 3 CTAs share an SM.
-template <class T, bool STRESS>
-__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 1) k_pml_slab(Grid g, Fields<T> f, const __grid_constant__ PmlDesc D,
-                                                  const __grid_constant__ PmlAux<T> X, StepConst<T> c, int* status) {
-    extern __shared__ __align__(128) unsigned char smem_raw[];
-    T* ring = reinterpret_cast<T*>(smem_raw + ((128u - (smem_addr(smem_raw) & 127u)) & 127u));
-    __shared__ __align__(8) uint64_t sbar[2];
-    if (threadIdx.x == 0 && threadIdx.y == 0) {
-        mbar_init(smem_addr(&sbar[0]), 1);
-        mbar_init(smem_addr(&sbar[1]), 1);
-        fence_mbar_init();
-    }
-    __syncthreads();
-    unsigned ps = 0;
-    if (STRESS) str_pml_slab_cta<T>(g, f, D, X, c, blockIdx.x, ring, sbar, ps, status);
-    else vel_pml_slab_cta<T>(g, f, D, X, c, blockIdx.x, ring, sbar, ps, status);
-}
-
-// Allows the slab kernels more than 48 KB of dynamic shared memory (the FP64 stress slab);
-// false if the device refuses.
-template <class T>
-inline bool prepare_pml_slab_kernels() {
-    bool ok = cudaFuncSetAttribute(k_pml_slab<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   pml_slab_smem<T>(false)) == cudaSuccess;
-    ok &= cudaFuncSetAttribute(k_pml_slab<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               pml_slab_smem<T>(true)) == cudaSuccess;
-    if (!ok) cudaGetLastError();
-    return ok;
-}
-
-// launch of a PML sweep: tiles of the x strips with a register cap picked at run time, then
-// the slabs of the y and z strips
+// launch of a PML sweep with a register cap picked at run time
 template <class T>
 inline void launch_pml(bool stress, int minb, cudaStream_t st, const Grid& g, const Fields<T>& f, const PmlDesc& D,
                        const PmlAux<T>& X, const StepConst<T>& c, int* status) {
-    if (D.scum[PML_MAXS] > 0) {
-        if (stress)
-            k_pml_slab<T, true><<<D.scum[PML_MAXS], dim3(32, 8), pml_slab_smem<T>(true), st>>>(g, f, D, X, c, status);
-        else
-            k_pml_slab<T, false><<<D.scum[PML_MAXS], dim3(32, 8), pml_slab_smem<T>(false), st>>>(g, f, D, X, c, status);
-    }
-    const unsigned nblk = (unsigned)(D.cum[2] / PML_TILE);  // tiles of the x strips
+    const unsigned nblk = (unsigned)((D.cum[PML_MAXS] + PML_TILE - 1) / PML_TILE);
     if (nblk == 0) return;
 #define FD3D_PML_CASE(MB)                                                               \
     case MB:                                                                            \

@@ -52,7 +52,6 @@ void make_pml(const fd3d_params& p, PmlDesc& D, std::vector<Damp<T>>& prof) {
     prof.clear();
     D.ns = p.fspace ? 5 : 4;
     D.cum[0] = 0;
-    D.scum[0] = 0;
     std::vector<std::vector<T>> ox(PML_MAXS), oxS(PML_MAXS), oy(PML_MAXS), oyS(PML_MAXS), oz(PML_MAXS), ozS(PML_MAXS);
     for (int s = 0; s < PML_MAXS; ++s) {
         if (s >= D.ns) {  // absent strip: empty range
@@ -60,7 +59,6 @@ void make_pml(const fd3d_params& p, PmlDesc& D, std::vector<Damp<T>>& prof) {
             D.s[s].ncells = 0;
             D.cnt[s] = 0;
             D.cum[s + 1] = D.cum[s];
-            D.scum[s + 1] = D.scum[s];
             continue;
         }
         Strip& S = D.s[s];
@@ -72,18 +70,7 @@ void make_pml(const fd3d_params& p, PmlDesc& D, std::vector<Damp<T>>& prof) {
         base += S.ncells;
         // every strip starts on a tile boundary, so a tile's cells share a strip
         D.cnt[s] = (long long)S.ni * (S.jend_uw - S.nyb + 1) * S.nk;
-        S.rlo = S.rhi = S.mlo = S.mhi = S.nib = S.nrb = 0;
-        if (s >= 2) {  // slabs: the y strip marches j over k-rows, the z strips k over j-rows
-            if (s == 2) { S.rlo = S.nzb; S.rhi = S.nze; S.mlo = S.nyb; S.mhi = S.jend_uw; }
-            else        { S.rlo = S.nyb; S.rhi = S.jend_uw; S.mlo = S.nzb; S.mhi = S.nze; }
-            S.nib = (S.ni + 31) / 32;
-            S.nrb = (S.rhi - S.rlo + 1 + 7) / 8;
-            D.cum[s + 1] = D.cum[s] + (long long)(S.mhi - S.mlo + 1) * S.nrb * S.nib * PML_TILE;
-            D.scum[s + 1] = D.scum[s] + S.nrb * S.nib;
-        } else {
-            D.cum[s + 1] = D.cum[s] + (D.cnt[s] + PML_TILE - 1) / PML_TILE * PML_TILE;
-            D.scum[s + 1] = D.scum[s];
-        }
+        D.cum[s + 1] = D.cum[s] + (D.cnt[s] + PML_TILE - 1) / PML_TILE * PML_TILE;
         S.rni = 1.0f / (float)S.ni;
         S.rnj = 1.0f / (float)(S.jend_uw - S.nyb + 1);
         S.fastdiv = D.cnt[s] < (1LL << 24);
