@@ -139,9 +139,9 @@ struct StepConst {
 // The fallback is out of line: the PML sweeps divide up to 20 times per cell, and inlining
 // the FP64 division at every site filled the instruction cache with code that rarely runs.
 // |x| in [2^-98, 2^98] is tested on the bit pattern: (bits & 0x7fffffff) - 0x0E800000, as
-// an unsigned number, is at most 0x62000000 exactly when 2^-98 <= |x| <= 2^98 (the
-// patterns 0x0E800000 and 0x70800000); zero, subnormals, infinities and NaN fall outside.
-static __device__ __noinline__ float div_pre_slow(float x, float b, float y) {
+// an unsigned number, is at most 0x62000000 exactly when the biased exponent lies in
+// [29, 225]; zero, subnormals, infinities and NaN fall outside.
+__device__ __noinline__ float div_pre_slow(float x, float b, float y) {
     return (x == 0.0f && y == y) ? __fmul_rn(x, y) : __double2float_rn(__ddiv_rn((double)x, (double)b));
 }
 __device__ __forceinline__ float div_pre(float x, float b, float y) {
