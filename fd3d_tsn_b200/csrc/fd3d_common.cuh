@@ -135,23 +135,15 @@ struct StepConst {
 // an exhaustive GPU test over all 2^32 dividends (fd3d_check_division) holds it to
 // that.  (The wave field's leading edge carries long runs of tiny values, so the
 // fallback must not be the slow path of a single-precision division.)
-//
-// The fallback is out of line: the PML sweeps divide up to 20 times per cell, and inlining
-// the FP64 division at every site filled the instruction cache with code that rarely runs.
-// |x| in [2^-98, 2^98] is tested on the bit pattern: (bits & 0x7fffffff) - 0x0E800000, as
-// an unsigned number, is at most 0x62000000 exactly when the biased exponent lies in
-// [29, 225]; zero, subnormals, infinities and NaN fall outside.
-__device__ __noinline__ float div_pre_slow(float x, float b, float y) {
-    return (x == 0.0f && y == y) ? __fmul_rn(x, y) : __double2float_rn(__ddiv_rn((double)x, (double)b));
-}
 __device__ __forceinline__ float div_pre(float x, float b, float y) {
     float q = __fmul_rn(x, y);
     float r = __fmaf_rn(-q, b, x);
     q = __fmaf_rn(r, y, q);
     r = __fmaf_rn(-q, b, x);
     float q2 = __fmaf_rn(r, y, q);
-    const unsigned e = __float_as_uint(x) & 0x7fffffffu;
-    if (e - 0x0E800000u > 0x62000000u || q2 != q2) q2 = div_pre_slow(x, b, y);
+    const float a = fabsf(x);
+    if (!(a >= 0x1p-98f && a <= 0x1p98f && q2 == q2))
+        q2 = (a == 0.0f && y == y) ? __fmul_rn(x, y) : __double2float_rn(__ddiv_rn((double)x, (double)b));
     return q2;
 }
 // the FP64 build divides directly (parity build, not the fast path)
