@@ -173,7 +173,7 @@ struct CtxBase {
     bool split_bc = false;
     float last_ms = 0.f;
     bool profiling = false;
-    int pml_minb_vel = 1, pml_minb_str = 3;  // register caps of the PML sweeps (CTAs per SM; 3 keeps the stress sweep unspilled)
+    int pml_minb_vel = 1, pml_minb_str = 1;  // register caps of the PML sweeps (CTAs per SM; 1: none, measured fastest)
     std::vector<cudaEvent_t> kev;   // 2 per kernel id
     float ktimes[FD3D_NKERNELS] = {0};
     int klaunch[FD3D_NKERNELS] = {0};
