@@ -461,6 +461,7 @@ struct fd3d_batch {
     static constexpr int NGRAPH = 6;
     cudaGraphExec_t gx[NGRAPH] = {};
     int graph_kchunk = -1;
+    int branches = 1;            // graph schedule: fault-band and PML sweeps on side streams
     int** d_stptr = nullptr;     // status words of the live models (k_or_status)
     int n_stptr = 0;
     int* d_status_or = nullptr;
@@ -617,12 +618,17 @@ int enqueue_graph_step(fd3d_batch* b) {
         const int n = b->tbeg[t1] - b->tbeg[t0];
         if (n > 0) k_bplane<<<n, blk, 0, s>>>(b->d_models, b->d_work_t, b->tbeg[t0], b->d_limit, b->d_run_step);
     };
+    // the fault-band and PML sweeps on side streams beside the interior sweep, or (branches
+    // off) all on the main stream one after another
+    cudaStream_t s0 = b->branches ? b->side[0] : b->st, s1 = b->branches ? b->side[1] : b->st;
     for (int half = 0; half < 2; ++half) {
         const int ti = half ? W_STR_INT : W_VEL_INT, tf = half ? W_STR_FAULT : W_VEL_FAULT;
         const int tp = half ? W_STR_PML : W_VEL_PML, tfs = half ? W_STR_FS : W_VEL_FS;
-        BCK(cudaEventRecord(b->evf[0], b->st));
-        BCK(cudaStreamWaitEvent(b->side[0], b->evf[0], 0));
-        BCK(cudaStreamWaitEvent(b->side[1], b->evf[0], 0));
+        if (b->branches) {
+            BCK(cudaEventRecord(b->evf[0], b->st));
+            BCK(cudaStreamWaitEvent(b->side[0], b->evf[0], 0));
+            BCK(cudaStreamWaitEvent(b->side[1], b->evf[0], 0));
+        }
         if (n_of(ti) > 0) {
             if (half)
                 k_bint<true><<<n_of(ti), blk, tma_ring_bytes<float>(), b->st>>>(
@@ -631,19 +637,21 @@ int enqueue_graph_step(fd3d_batch* b) {
                 k_bint<false><<<n_of(ti), blk, tma_ring_bytes<float>(), b->st>>>(
                     b->d_models, b->d_maps, b->d_work_t, b->tbeg[ti], b->d_limit, b->d_run_step, kc, b->d_status);
         }
-        plane(b->side[0], tf, tf + 1);
+        plane(s0, tf, tf + 1);
         if (n_of(tp) > 0) {
             if (half)
-                k_bpml<true><<<n_of(tp), blk, 0, b->side[1]>>>(b->d_models, b->d_work_t, b->tbeg[tp], b->d_limit,
-                                                               b->d_run_step, b->d_status);
+                k_bpml<true><<<n_of(tp), blk, 0, s1>>>(b->d_models, b->d_work_t, b->tbeg[tp], b->d_limit,
+                                                       b->d_run_step, b->d_status);
             else
-                k_bpml<false><<<n_of(tp), blk, 0, b->side[1]>>>(b->d_models, b->d_work_t, b->tbeg[tp], b->d_limit,
-                                                                b->d_run_step, b->d_status);
+                k_bpml<false><<<n_of(tp), blk, 0, s1>>>(b->d_models, b->d_work_t, b->tbeg[tp], b->d_limit,
+                                                        b->d_run_step, b->d_status);
         }
-        BCK(cudaEventRecord(b->evf[1], b->side[0]));
-        BCK(cudaEventRecord(b->evf[2], b->side[1]));
-        BCK(cudaStreamWaitEvent(b->st, b->evf[1], 0));
-        BCK(cudaStreamWaitEvent(b->st, b->evf[2], 0));
+        if (b->branches) {
+            BCK(cudaEventRecord(b->evf[1], b->side[0]));
+            BCK(cudaEventRecord(b->evf[2], b->side[1]));
+            BCK(cudaStreamWaitEvent(b->st, b->evf[1], 0));
+            BCK(cudaStreamWaitEvent(b->st, b->evf[2], 0));
+        }
         plane(b->st, tfs, half ? W_FBC + 1 : tfs + 1);  // after the stresses: fres and the fault BC tiles
     }
     plane(b->st, W_NUC, W_NUC + 1);
@@ -847,6 +855,8 @@ int fd3d_batch_create(size_t arena_bytes, int max_models, fd3d_batch** out) {
     }
     if (const char* e = std::getenv("FD3D_BATCH_KCHUNK")) b->tun.kchunk = std::max(1, std::atoi(e));
     if (const char* e = std::getenv("FD3D_BATCH_PER_SM")) b->tun.per_sm = std::max(0, std::atoi(e));
+    // FD3D_BATCH_BRANCHES=0: the graph schedule runs every region on the main stream
+    if (const char* e = std::getenv("FD3D_BATCH_BRANCHES")) b->branches = std::atoi(e) != 0;
     // FD3D_BATCH_MODE=persistent|graph
     if (const char* e = std::getenv("FD3D_BATCH_MODE"))
         b->tun.mode = std::strcmp(e, "persistent") == 0 ? MODE_PERSISTENT : MODE_GRAPH;
