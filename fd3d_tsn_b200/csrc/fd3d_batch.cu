@@ -461,7 +461,8 @@ struct fd3d_batch {
     static constexpr int NGRAPH = 6;
     cudaGraphExec_t gx[NGRAPH] = {};
     int graph_kchunk = -1;
-    int branches = 1;            // graph schedule: fault-band and PML sweeps on side streams
+    int branches = 0;            // graph schedule: fault-band and PML sweeps on side streams (1) or in
+                                 // series on the main stream (0, measured 9-11% faster: the branches interfered)
     int** d_stptr = nullptr;     // status words of the live models (k_or_status)
     int n_stptr = 0;
     int* d_status_or = nullptr;
@@ -855,7 +856,7 @@ int fd3d_batch_create(size_t arena_bytes, int max_models, fd3d_batch** out) {
     }
     if (const char* e = std::getenv("FD3D_BATCH_KCHUNK")) b->tun.kchunk = std::max(1, std::atoi(e));
     if (const char* e = std::getenv("FD3D_BATCH_PER_SM")) b->tun.per_sm = std::max(0, std::atoi(e));
-    // FD3D_BATCH_BRANCHES=0: the graph schedule runs every region on the main stream
+    // FD3D_BATCH_BRANCHES=1: the graph schedule runs the fault-band and PML sweeps on side streams
     if (const char* e = std::getenv("FD3D_BATCH_BRANCHES")) b->branches = std::atoi(e) != 0;
     // FD3D_BATCH_MODE=persistent|graph
     if (const char* e = std::getenv("FD3D_BATCH_MODE"))
