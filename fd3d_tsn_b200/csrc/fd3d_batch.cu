@@ -264,23 +264,34 @@ __global__ void __launch_bounds__(PML_TILE, STRESS ? 3 : 4) k_bpml(const ModelDe
     else vel_pml_tile<float>(M.g, M.f, M.D, M.X, M.c, it.bx, sm, smem_addr(&bar), 0u, gstatus);
 }
 
+// Plane items in three kernels by register need, so that light items are not held to a
+// heavy body's register count: KIND 1 the fused fault-BC tiles (and the fres items launched
+// with them, 78 registers), KIND 2 the fault-band velocity (its rate-and-state Newton path
+// takes 114), KIND 0 the rest (free surface, stress fault band, nucleation ramp).
+template <int KIND>
 __global__ void __launch_bounds__(256) k_bplane(const ModelDev* __restrict__ models, const Work* __restrict__ work,
                                                 int b0, const int* __restrict__ limit, const int* run_step) {
-    __shared__ float sm[FBC_SMEM];
+    __shared__ float sm[KIND == 1 ? FBC_SMEM : 1];
     const Work it = work[b0 + blockIdx.x];
     int m;
     if (!item_live(it, limit, run_step, m)) return;
     const ModelDev& M = models[m];
-    switch (it.tm & 255) {
-        case W_VEL_FAULT:
+    if (KIND == 2) {
+        if ((it.tm & 255) == W_VEL_FAULT)
             vel_fault_body<float>(M.g, M.f, M.q, M.c, M.law, M.fs, M.it_dev, M.status, it.bx, it.by, 0);
-            break;
+        return;
+    }
+    if (KIND == 1) {
+        if ((it.tm & 255) == W_FBC)
+            fault_bc_body<float>(M.g, M.f, M.q, M.c, M.law, M.fs, M.it_dev, M.h, M.status, it.bx, it.by, sm);
+        else if ((it.tm & 255) == W_STR_FS)
+            str_fs_body<float>(M.g, M.f, it.bx, it.by, 0);
+        return;
+    }
+    switch (it.tm & 255) {
         case W_VEL_FS: vel_fs_body<float>(M.g, M.f, it.bx, it.by, 0); break;
         case W_STR_FAULT: str_fault_body<float>(M.g, M.f, M.q, M.c, it.bx, it.by, 0); break;
         case W_STR_FS: str_fs_body<float>(M.g, M.f, it.bx, it.by, 0); break;
-        case W_FBC:
-            fault_bc_body<float>(M.g, M.f, M.q, M.c, M.law, M.fs, M.it_dev, M.h, M.status, it.bx, it.by, sm);
-            break;
         case W_NUC: nucleation_body<float>(M.g, M.q, M.c, M.fs, M.it_dev, it.bx, it.by, 0); break;
         default: break;
     }
@@ -617,7 +628,11 @@ int enqueue_graph_step(fd3d_batch* b) {
     auto n_of = [&](int t) { return b->tbeg[t + 1] - b->tbeg[t]; };
     auto plane = [&](cudaStream_t s, int t0, int t1) {  // item types [t0, t1) in one launch
         const int n = b->tbeg[t1] - b->tbeg[t0];
-        if (n > 0) k_bplane<<<n, blk, 0, s>>>(b->d_models, b->d_work_t, b->tbeg[t0], b->d_limit, b->d_run_step);
+        if (n == 0) return;
+        const int* lim = b->d_limit;
+        if (t0 <= W_FBC && W_FBC < t1) k_bplane<1><<<n, blk, 0, s>>>(b->d_models, b->d_work_t, b->tbeg[t0], lim, b->d_run_step);
+        else if (t0 == W_VEL_FAULT) k_bplane<2><<<n, blk, 0, s>>>(b->d_models, b->d_work_t, b->tbeg[t0], lim, b->d_run_step);
+        else k_bplane<0><<<n, blk, 0, s>>>(b->d_models, b->d_work_t, b->tbeg[t0], lim, b->d_run_step);
     };
     // the fault-band and PML sweeps on side streams beside the interior sweep, or (branches
     // off) all on the main stream one after another
