@@ -444,8 +444,13 @@ def batch_section(args, world, rank, local, pg):
     t_setup = time.perf_counter()
     b = Batch(arena, len(models) + 8)
     slots = [b.add(m) for m in models]
-    tune = b.autotune(steps=10, cache_path=os.path.join(tempfile.gettempdir(), "fd3d_batch_tune.jsonl"),
-                      key=f"batch{len(models)}-seed{2024 + rank}")
+    if args.batch_schedule == "auto":
+        tune = b.autotune(steps=10, cache_path=os.path.join(tempfile.gettempdir(), "fd3d_batch_tune.jsonl"),
+                          key=f"batch{len(models)}-seed{2024 + rank}")
+    else:  # a fixed schedule at its usual tile depth, no tuning launches
+        b.set_schedule(args.batch_schedule)
+        b.set_tuning(32 if args.batch_schedule == "graph" else 8, 3 if args.batch_schedule == "persistent" else 0)
+        tune = b.tuning()
     t_setup = time.perf_counter() - t_setup
     barrier(pg, local)
     t0 = time.perf_counter()
@@ -565,6 +570,8 @@ def relaunch(ngpus):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--models", type=int, default=256, help="batched workload: number of models")
+    ap.add_argument("--batch-schedule", default="auto", choices=["auto", "graph", "persistent"],
+                    help="batched workload: tune the schedule on the live batch, or fix it")
     ap.add_argument("--requests", type=int, default=500, help="serving workload: number of requests")
     ap.add_argument("--load", type=float, default=0.7,
                     help="serving workload: offered Poisson rate as a fraction of the measured capacity")

@@ -125,25 +125,28 @@ struct StepConst {
 // approximation and no branch on the common path.
 //
 // The theorem assumes that nothing under- or overflows.  For |x| outside
-// [2^-98, 2^98], NaN, infinities and a divisor outside the range checked on the host
-// (y is NaN then) the quotient is formed in FP64 and rounded to FP32: both operands
-// are exact in FP64, and rounding a quotient first to 53 bits and then to 24 (or
-// fewer, for a subnormal result) gives the directly rounded quotient because
+// [2^-98, 2^98] (zero aside), NaN, infinities and a divisor outside the range checked
+// on the host (y is NaN then) the quotient is formed in FP64 and rounded to FP32: both
+// operands are exact in FP64, and rounding a quotient first to 53 bits and then to 24
+// (or fewer, for a subnormal result) gives the directly rounded quotient because
 // 53 >= 2*24 + 2 (S. A. Figueroa, "When is double rounding innocuous?", SIGNUM
-// Newsletter 30(3), 1995).  A zero dividend returns x*y, which keeps the sign of the
-// zero as x/b does.  The result is therefore the IEEE FP32 quotient for every input;
-// an exhaustive GPU test over all 2^32 dividends (fd3d_check_division) holds it to
-// that.  (The wave field's leading edge carries long runs of tiny values, so the
-// fallback must not be the slow path of a single-precision division.)
+// Newsletter 30(3), 1995).  A zero dividend stays on the common path: every step then
+// yields a zero, and the sign of x put on the result makes it the signed zero x/b is
+// (for any other x in range the quotient already has the sign of x, since b > 0).  Zero
+// is the value of every cell ahead of the wavefront, so it must cost no more than a
+// normal value.  The result is therefore the IEEE FP32 quotient for every input; an
+// exhaustive GPU test over all 2^32 dividends (fd3d_check_division) holds it to that.
+// (The wave field's leading edge carries long runs of tiny values, so the fallback must
+// not be the slow path of a single-precision division.)
 __device__ __forceinline__ float div_pre(float x, float b, float y) {
     float q = __fmul_rn(x, y);
     float r = __fmaf_rn(-q, b, x);
     q = __fmaf_rn(r, y, q);
     r = __fmaf_rn(-q, b, x);
-    float q2 = __fmaf_rn(r, y, q);
+    float q2 = copysignf(__fmaf_rn(r, y, q), x);
     const float a = fabsf(x);
-    if (!(a >= 0x1p-98f && a <= 0x1p98f && q2 == q2))
-        q2 = (a == 0.0f && y == y) ? __fmul_rn(x, y) : __double2float_rn(__ddiv_rn((double)x, (double)b));
+    if (!((a >= 0x1p-98f || a == 0.0f) && a <= 0x1p98f && q2 == q2))
+        q2 = __double2float_rn(__ddiv_rn((double)x, (double)b));
     return q2;
 }
 // the FP64 build divides directly (parity build, not the fast path)

@@ -38,7 +38,8 @@ def test_division_matches_ieee_on_every_dividend(gpu_available):
     rng = np.random.default_rng(7)
     # significands near 1, sqrt 2 and 2, powers of two, both ends of the fast range
     extra = [1.0, 2.0, 0.5, 1.0000001, 1.4142135, 1.9999999, 1.99999988, 3.0, 7.0, 1e-6, 2.0 ** -20,
-             2.0 ** 20, 1e6, 2.0 ** 21, 2.0 ** -21, 12.5, 37.5]
+             2.0 ** 20, 1e6, 2.0 ** 21, 2.0 ** -21, 12.5, 37.5,
+             -3.0, -1.0, 0.0]   # outside the checked range: every quotient by the FP64 path
     divs.update(float(np.float32(x)) for x in extra)
     divs.update(float(np.float32(x)) for x in rng.uniform(1.0, 2.0, 8))
     divs = sorted(divs)
