@@ -158,6 +158,16 @@ def load_library(path: str | None = None) -> C.CDLL:
         "fd3d_fetch_moment_rate": (i, [vp, i, i, dp]),
         "fd3d_post_process": (i, [vp, dp]),
         "fd3d_upload_fault_model": (i, [vp, i, i, dp, dp, dp, C.c_double, i]),
+        "fd3d_ctx_create_slab": (i, [C.POINTER(Params), i, i, C.POINTER(vp)]),
+        "fd3d_slab_range": (i, [vp, C.POINTER(i), C.POINTER(i)]),
+        "fd3d_slab_plan": (i, [C.POINTER(Params), i, C.POINTER(i), C.POINTER(i)]),
+        "fd3d_slab_group_create": (i, [C.POINTER(vp), i, C.POINTER(vp)]),
+        "fd3d_slab_group_run": (i, [vp, i]),
+        "fd3d_slab_group_sync": (i, [vp, fp]),
+        "fd3d_slab_group_destroy": (i, [vp]),
+        "fd3d_nccl_unique_id": (i, [C.c_char_p]),
+        "fd3d_slab_connect": (i, [vp, C.c_char_p, i, i]),
+        "fd3d_slab_run": (i, [vp, i]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

@@ -67,7 +67,7 @@ def build_gpu(force: bool = False, verbose: bool = False) -> str:
         subprocess.run(cmd, check=True)
         objs.append(obj)
     tmp = LIB + ".tmp"
-    cmd = [NVCC, *ARCH, "-shared", "-o", tmp, *objs, "-lcudart"]
+    cmd = [NVCC, *ARCH, "-shared", "-o", tmp, *objs, "-lcudart", "-ldl"]
     subprocess.run(cmd, check=True)
     os.replace(tmp, LIB)
     return LIB

@@ -23,7 +23,12 @@ struct Grid {
     int px;          // row pitch (elements)
     int off;         // x offset of i=1 inside a row
     long long plane; // px*nyt
-    long long n3;    // plane*nzt + tail pad
+    long long n3;    // plane*nzl + tail pad: the elements of one stored 3-D array
+    // z-slab of a model decomposed over several contexts: the context updates planes
+    // klo..khi and stores planes kofs+1 .. kofs+nzl (its own and the halo planes of its
+    // neighbours).  Field pointers are offset by -kofs planes, so at() takes the global k
+    // everywhere.  A whole model: klo = 1, khi = nzt, kofs = 0, nzl = nzt.
+    int klo, khi, kofs, nzl;
 
     __host__ __device__ __forceinline__ long long at(int i, int j, int k) const {
         return (long long)off + (i - 1) + (long long)px * (j - 1) + plane * (k - 1);
@@ -31,6 +36,10 @@ struct Grid {
     __host__ __device__ __forceinline__ int at2(int i, int k) const { return (i - 1) + nxt * (k - 1); }
     __host__ __device__ __forceinline__ int ks() const { return nzt - nfs; }  // free-surface row (top row of the
                                                                               // interior box under FSPACE)
+    __host__ __device__ __forceinline__ bool owns(int k) const { return k >= klo && k <= khi; }
+    // the planes of the interior box (and fault rows) this context updates
+    __host__ __device__ __forceinline__ int kin_lo() const { return klo > nabc + 1 ? klo : nabc + 1; }
+    __host__ __device__ __forceinline__ int kin_hi() const { return khi < ks() ? khi : ks(); }
 };
 
 // Split-field PML strip (strip s = 1 x-low, 2 x-high, 3 y-low, 4 z-low, 5 z-high under FSPACE).

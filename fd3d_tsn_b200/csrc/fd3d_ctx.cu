@@ -1,8 +1,10 @@
 // fd3d_ctx.cu -- C ABI of the single-model B200 path (include/fd3d_gpu.h).
 //
-// Owns the device state of one forward model, enqueues the eleven launches of a
+// Owns the device state of one forward model, enqueues the eight launches of a
 // time step on the context's stream, captures chunks of steps in a CUDA graph,
-// and drains the device history ring into the reference's result files.
+// and drains the device history ring into the reference's result files.  A context
+// can also own a z-slab of a model (a range of planes) that steps with the model's other
+// slabs, in one process or over NCCL, exchanging halos between the phases of a step.
 #include <cuda_runtime.h>
 #include <algorithm>
 #include <cmath>
@@ -11,6 +13,7 @@
 #include <cstring>
 #include <string>
 #include <vector>
+#include "fd3d_nccl.h"
 #include "../../include/fd3d_gpu.h"
 #include "fd3d_common.cuh"
 #include "fd3d_kernels.cuh"
@@ -39,12 +42,12 @@ namespace fd3d {
 // goes to tab (lam, mu, d and dth/d, nzt values each).
 template <class T>
 __global__ void k_layer_check(Grid g, const T* lam, const T* mu, const T* d, T dth, T dt, T* tab, int* nonuniform) {
-    const long long n = (long long)g.nxt * g.nyt * g.nzt;
+    const long long n = (long long)g.nxt * g.nyt * g.nzl;  // the stored planes, from kofs+1
     int bad = 0;
     for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
         const int i = 1 + (int)(q % g.nxt);
         const long long r = q / g.nxt;
-        const int j = 1 + (int)(r % g.nyt), k = 1 + (int)(r / g.nyt);
+        const int j = 1 + (int)(r % g.nyt), k = g.kofs + 1 + (int)(r / g.nyt);
         const long long p = g.at(i, j, k), p0 = g.at(1, 1, k);
         bad |= (lam[p] != lam[p0]) | (mu[p] != mu[p0]) | (d[p] != d[p0]);
         if (i == 1 && j == 1) {
@@ -91,11 +94,11 @@ __global__ void k_model_to_fd3d(Grid g, int nli, const T* T0I, const T* TsI, con
 // layout (element type converted when the host's real kind differs from the field type)
 template <class T, class S>
 __global__ void k_repack(Grid g, const S* __restrict__ src, T* __restrict__ dst) {
-    const long long n = (long long)g.nxt * g.nyt * g.nzt;
+    const long long n = (long long)g.nxt * g.nyt * g.nzl;  // the stored planes, from kofs+1
     for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
         const int i = 1 + (int)(q % g.nxt);
         const long long r = q / g.nxt;
-        const int j = 1 + (int)(r % g.nyt), k = 1 + (int)(r / g.nyt);
+        const int j = 1 + (int)(r % g.nyt), k = g.kofs + 1 + (int)(r / g.nyt);
         dst[g.at(i, j, k)] = (T)src[q];
     }
 }
@@ -124,6 +127,18 @@ struct DeviceGuard {
     ~DeviceGuard() {
         if (changed) cudaSetDevice(prev);
     }
+};
+
+// A step in phases, and what a z-slab's neighbours need after each: the velocities
+// after phase 0, the stresses after phase 1, the trial tractions and their damped parts
+// after phase 2 (the friction law averages neighbouring nodes), the tractions after phase 3
+// (the output averages them).
+enum { STEP_PHASES = 5 };
+enum HaloSet { HALO_NONE = -1, HALO_VEL = 0, HALO_STR = 1, HALO_TRIAL = 2, HALO_TRACTION = 3 };
+inline int halo_after_phase(int ph) { return ph <= 3 ? ph : HALO_NONE; }
+struct HaloArray {
+    void* base;           // element of global plane / row 1 sits at base (index unit*(k-1))
+    size_t elem, unit;    // bytes per element, elements per plane or row
 };
 
 struct CtxBase {
@@ -171,6 +186,14 @@ struct CtxBase {
     // the fault boundary condition as separate launches (fres, traction, friction, output)
     // with the trial tractions in q.txt / q.tzt instead of the fused kernel
     bool split_bc = false;
+    // z-slab of a model decomposed over several contexts (fd3d_ctx_create_slab): the
+    // planes it updates; it steps only inside a slab group, which exchanges the halos
+    bool slab = false;
+    int slab_lo = 0, slab_hi = 0;
+    // a slab in its own process (fd3d_slab_connect): the NCCL communicator of the model's
+    // slabs, this slab's rank (from the bottom) and their number
+    ncclComm_t comm = nullptr;
+    int slab_rank = -1, slab_nranks = 0;
     float last_ms = 0.f;
     bool profiling = false;
     int pml_minb_vel = 1, pml_minb_str = 1;  // register caps of the PML sweeps (CTAs per SM; 1: none, measured fastest)
@@ -188,6 +211,11 @@ struct CtxBase {
     virtual int upload_fault_model(int, int, const double*, const double*, const double*, double, int) = 0;
     virtual int reset() = 0;
     virtual int enqueue_step() = 0;
+    // one of the STEP_PHASES parts of a step (enqueue_step runs them in order)
+    virtual int enqueue_phase(int ph) = 0;
+    // the arrays of halo set `set` (HaloSet) with their element size and elements per
+    // plane (3-D fields) or row (fault planes); base pointers take the global index
+    virtual int halo_arrays(int set, std::vector<HaloArray>& out) = 0;
     virtual int fetch_field(int, void*, int) = 0;
     virtual int fetch_plane(int, double*) = 0;
     virtual int moment_rate(int rec0, int nrec, double* host) = 0;
@@ -242,6 +270,7 @@ struct Ctx : CtxBase {
     }
 
     ~Ctx() override {
+        if (comm) nccl().CommDestroy(comm);
         for (cudaGraphExec_t& gx : gexec) if (gx) cudaGraphExecDestroy(gx);
         for (void* v : allocs) cudaFree(v);
         if (block) cudaFree(block);
@@ -265,13 +294,16 @@ struct Ctx : CtxBase {
         CK(cudaEventCreate(&ev1));
         kev.resize(2 * FD3D_NKERNELS);
         for (auto& e : kev) CK(cudaEventCreate(&e));
-        g = make_grid(p);
+        g = slab ? make_slab_grid(p, slab_lo, slab_hi) : make_grid(p);
+        if (slab) { split_bc = true; overlap = 0; }
         c = make_const<T>(p);
         law = p.law;
         nf = (law == FD3D_LAW_FVW) ? 5 : 4;
         std::vector<Damp<T>> prof;
         make_pml<T>(p, D, prof);
         if (!pml_modes_hold(D, prof)) return FD3D_ERR_ARG;
+        D.klo = g.klo;
+        D.khi = g.khi;
         const int stride = std::max(1, p.history_stride);
         p.history_stride = stride;
         const long long plane = (long long)(p.nxt - 2 * p.nabc) * (p.nzt - p.nfs - p.nabc);
@@ -291,7 +323,7 @@ struct Ctx : CtxBase {
                           carve((size_t)cap * std::max(1, p.nstations) * 3 * sizeof(T)) +
                           carve((size_t)LAY_N * p.nzt * sizeof(T)) + carve(sizeof(int)) + 2 * carve(n2 * sizeof(double)) +
                           carve((size_t)POST_BLOCKS * POST_NSUM * sizeof(double)) + carve(POST_NSUM * sizeof(double)) +
-                          carve((size_t)cap * sizeof(double));
+                          carve((size_t)cap * sizeof(double)) + (slab ? 2 * carve(n2 * sizeof(T)) : 0);
             void* v = nullptr;
             if (cudaMalloc(&v, block_bytes) != cudaSuccess) { cudaGetLastError(); return FD3D_ERR_NOMEM; }
             block = (char*)v;
@@ -299,7 +331,7 @@ struct Ctx : CtxBase {
         }
         // 12 arrays of the 3-D grid in one pool
         if (dalloc(&fieldpool, (size_t)g.n3 * 12)) return FD3D_ERR_NOMEM;
-        T* b = fieldpool;
+        T* b = fieldpool - g.plane * g.kofs;  // a z-slab: global plane k at b + plane*(k-1)
         T** outs[9] = {&f.u, &f.v, &f.w, &f.xx, &f.yy, &f.zz, &f.xy, &f.yz, &f.xz};
         for (int a = 0; a < 9; ++a) *outs[a] = b + (size_t)a * g.n3;
         f.lam = b + 9 * (size_t)g.n3;
@@ -318,6 +350,7 @@ struct Ctx : CtxBase {
         if (dalloc(&q.distX, 2 * n2)) return FD3D_ERR_NOMEM;
         q.n2 = (int)n2;
         q.txt = q.tzt = nullptr;  // trial tractions live in shared memory (fault_bc_body)
+        if (slab && (dalloc(&q.txt, n2) || dalloc(&q.tzt, n2))) return FD3D_ERR_NOMEM;  // separate-launch fault BC
         T* pool = nullptr;
         if (dalloc(&pool, pml_aux_elems(D))) return FD3D_ERR_NOMEM;
         pml_aux_bind(X, pool, D);
@@ -326,6 +359,7 @@ struct Ctx : CtxBase {
         CK(cudaMemcpyAsync(dprof, prof.data(), prof.size() * sizeof(Damp<T>), cudaMemcpyHostToDevice, st));
         X.prof = dprof;
         tma_ok = make_interior_maps<T>(g, f, vmaps, smaps) && prepare_tma_kernels<T>();
+        if (slab && !tma_ok) return FD3D_ERR_CUDA;
         if (!tma_ok && icfg.variant == IV_TMA) {
             std::fprintf(stderr, "fd3d: tensor maps of the interior sweeps could not be encoded for this grid; "
                                  "the interior sweeps fall back to plain loads (fd3d_ctx_info reports it)\n");
@@ -366,18 +400,21 @@ struct Ctx : CtxBase {
 
     int upload_medium(const void* l, const void* m, const void* d, int rk) override {
         if (rk != 4 && rk != 8) return FD3D_ERR_ARG;
-        const size_t n = (size_t)p.nxt * p.nyt * p.nzt;
+        // the planes this context stores: all of them, or a z-slab's own and halo planes
+        const size_t nrow = (size_t)p.nxt * p.nyt;
+        const size_t n = nrow * g.nzl, src0 = nrow * g.kofs;
         const void* src[3] = {l, m, d};
-        T* dst[3] = {(T*)f.lam, (T*)f.mu, (T*)f.d};
+        T* dst[3] = {(T*)f.lam + g.plane * g.kofs, (T*)f.mu + g.plane * g.kofs, (T*)f.d + g.plane * g.kofs};
         for (int a = 0; a < 3; ++a)
             if (!src[a]) return FD3D_ERR_ARG;
         if (steps_done == 0 && n * (size_t)rk <= (size_t)g.n3 * 9 * sizeof(T)) {
             // The wave field is still zero: use it as the staging buffer of one contiguous
             // copy per array (the host array as it lies), repack on the device, zero it again.
             for (int a = 0; a < 3; ++a) {
-                CK(cudaMemcpyAsync(fieldpool, src[a], n * (size_t)rk, cudaMemcpyHostToDevice, st));
-                if (rk == 8) k_repack<T, double><<<1184, 256, 0, st>>>(g, (const double*)fieldpool, dst[a]);
-                else k_repack<T, float><<<1184, 256, 0, st>>>(g, (const float*)fieldpool, dst[a]);
+                CK(cudaMemcpyAsync(fieldpool, (const char*)src[a] + src0 * rk, n * (size_t)rk, cudaMemcpyHostToDevice, st));
+                T* at_k = dst[a] - g.plane * g.kofs;  // indexed by the global plane
+                if (rk == 8) k_repack<T, double><<<1184, 256, 0, st>>>(g, (const double*)fieldpool, at_k);
+                else k_repack<T, float><<<1184, 256, 0, st>>>(g, (const float*)fieldpool, at_k);
                 CK(cudaGetLastError());
             }
             CK(cudaMemsetAsync(fieldpool, 0, n * (size_t)rk, st));
@@ -387,8 +424,9 @@ struct Ctx : CtxBase {
         if ((size_t)rk == sizeof(T)) {
             // same element type: one pitched copy per array straight into the padded rows
             for (int a = 0; a < 3; ++a) {
-                CK(cudaMemcpy2DAsync(dst[a] + g.off, (size_t)g.px * sizeof(T), src[a], (size_t)p.nxt * sizeof(T),
-                                     (size_t)p.nxt * sizeof(T), (size_t)p.nyt * p.nzt, cudaMemcpyHostToDevice, st));
+                CK(cudaMemcpy2DAsync(dst[a] + g.off, (size_t)g.px * sizeof(T), (const char*)src[a] + src0 * rk,
+                                     (size_t)p.nxt * sizeof(T), (size_t)p.nxt * sizeof(T), (size_t)p.nyt * g.nzl,
+                                     cudaMemcpyHostToDevice, st));
             }
             CK(cudaStreamSynchronize(st));
             return medium_uploaded();
@@ -397,12 +435,12 @@ struct Ctx : CtxBase {
         for (int a = 0; a < 3; ++a) {
             // pack k-slabs into the padded layout on the host, one copy per slab
             const int kb = 16;
-            for (int k0 = 0; k0 < p.nzt; k0 += kb) {
-                const int nk = std::min(kb, p.nzt - k0);
+            for (int k0 = 0; k0 < g.nzl; k0 += kb) {
+                const int nk = std::min(kb, g.nzl - k0);
                 std::fill(row.begin(), row.end(), (T)0);
                 for (int kk = 0; kk < nk; ++kk)
                     for (int j = 0; j < p.nyt; ++j) {
-                        const size_t so = (size_t)p.nxt * ((size_t)j + (size_t)p.nyt * (k0 + kk));
+                        const size_t so = src0 + (size_t)p.nxt * ((size_t)j + (size_t)p.nyt * (k0 + kk));
                         T* o = row.data() + (size_t)g.px * ((size_t)j + (size_t)p.nyt * kk) + g.off;
                         if (rk == 8) { const double* s = (const double*)src[a] + so; for (int i = 0; i < p.nxt; ++i) o[i] = (T)s[i]; }
                         else         { const float* s = (const float*)src[a] + so;  for (int i = 0; i < p.nxt; ++i) o[i] = (T)s[i]; }
@@ -412,22 +450,21 @@ struct Ctx : CtxBase {
                 CK(cudaStreamSynchronize(st));
             }
         }
-        (void)n;
         return medium_uploaded();
     }
 
     int upload_medium_layers(const double* l, const double* m, const double* d) override {
         if (!l || !m || !d) return FD3D_ERR_ARG;
-        std::vector<T> slab((size_t)g.plane);
+        std::vector<T> slab_((size_t)g.plane);
         T* dst[3] = {(T*)f.lam, (T*)f.mu, (T*)f.d};
         const double* src[3] = {l, m, d};
         for (int a = 0; a < 3; ++a)
-            for (int k = 0; k < p.nzt; ++k) {
-                std::fill(slab.begin(), slab.end(), (T)0);
+            for (int k = g.kofs; k < g.kofs + g.nzl; ++k) {
+                std::fill(slab_.begin(), slab_.end(), (T)0);
                 const T v = (T)src[a][k];
                 for (int j = 0; j < p.nyt; ++j)
-                    for (int i = 0; i < p.nxt; ++i) slab[(size_t)g.px * j + g.off + i] = v;
-                CK(cudaMemcpyAsync(dst[a] + (size_t)g.plane * k, slab.data(), (size_t)g.plane * sizeof(T),
+                    for (int i = 0; i < p.nxt; ++i) slab_[(size_t)g.px * j + g.off + i] = v;
+                CK(cudaMemcpyAsync(dst[a] + (size_t)g.plane * k, slab_.data(), (size_t)g.plane * sizeof(T),
                                    cudaMemcpyHostToDevice, st));
                 CK(cudaStreamSynchronize(st));
             }
@@ -535,6 +572,7 @@ struct Ctx : CtxBase {
     };
     static constexpr size_t CKPT_CHUNK = 64ull << 20;
     int save_state(std::FILE* fp) override {
+        if (slab) return FD3D_ERR_STATE;  // the slab range is not part of the file
         if (!allocs.empty()) return FD3D_ERR_STATE;  // state outside the block: not restorable
         CK(cudaStreamSynchronize(st));
         SavedHost h{};
@@ -630,63 +668,106 @@ struct Ctx : CtxBase {
     }
 
     int enqueue_step() override {
+        for (int ph = 0; ph < STEP_PHASES; ++ph) {
+            const int rc = enqueue_phase(ph);
+            if (rc) return rc;
+        }
+        return FD3D_OK;
+    }
+
+    // Phase 0 the velocity half-step, 1 the stress sweeps, 2-4 the fault boundary
+    // condition (fused into phase 2 for a whole model; fres + traction, friction, output
+    // as separate launches for a z-slab or when split_bc is set) and the nucleation ramp.
+    int enqueue_phase(int ph) override {
         const int nxT = p.nxt - 2 * p.nabc;
-        const int nzT = g.ks() - p.nabc;
+        const int nzT = std::max(1, g.kin_hi() - g.kin_lo() + 1);  // fault rows updated (a launch has one at least)
         const dim3 b2(32, 8);
         const bool ov = overlap > 0 && !profiling;
+        const bool top = g.owns(g.ks());  // the free-surface rows are this context's
         cudaStream_t sp = ov ? st2 : st;  // fault band and PML
         auto fork = [&](int e) { cudaEventRecord(evf[e], st); cudaStreamWaitEvent(st2, evf[e], 0); };
         auto join = [&](int e) { cudaEventRecord(evf[e], st2); cudaStreamWaitEvent(st, evf[e], 0); };
-        // velocity half-step
-        if (ov) fork(0);
-        kbeg(0);
-        if (icfg.variant == IV_TMA) launch_vel_interior_tma<T>(vmaps, icfg, g, f, c, status, st);
-        else launch_vel_interior<T>(icfg, g, f, c, st);
-        kend(0);
-        kbeg(1);
-        k_vel_fault<T><<<dim3((std::max(nxT, p.nxt) + 31) / 32, (nzT + 7) / 8), b2, 0, sp>>>(g, f, q, c, law, fs, it_dev, status);
-        kend(1);
-        kbeg(2);
-        launch_pml<T>(false, pml_minb_vel, sp, g, f, D, X, c, status);
-        kend(2);
-        if (ov) join(1);
-        kbeg(3);
-        if (!p.fspace) k_vel_fs<T><<<dim3((p.nxt + 31) / 32, (p.nyt + 7) / 8), b2, 0, st>>>(g, f);  // fuvw
-        kend(3);
-        // stress half-step
-        if (ov) fork(2);
-        kbeg(4);
-        if (icfg.variant == IV_TMA) launch_str_interior_tma<T>(smaps, icfg, g, f, c, status, st);
-        else launch_str_interior<T>(icfg, g, f, c, st);
-        kend(4);
-        kbeg(5);
-        k_str_fault<T><<<dim3((nxT + 31) / 32, (nzT + 7) / 8), b2, 0, sp>>>(g, f, q, c);
-        kend(5);
-        kbeg(6);
-        launch_pml<T>(true, pml_minb_str, sp, g, f, D, X, c, status);
-        kend(6);
-        if (ov) join(3);
-        // fault boundary condition
-        kbeg(7);
         HistDesc h;
-        h.ring = ring; h.cap = hist_cap; h.stride = p.history_stride; h.nf = nf; h.nst = p.nstations;
-        for (int s = 0; s < p.nstations; ++s) { h.sta[3 * s] = p.staX[s]; h.sta[3 * s + 1] = p.staY[s]; h.sta[3 * s + 2] = p.staZ[s]; }
-        h.seis = seis;
-        if (!split_bc) {   // fres and the fused trial traction, friction and output tiles in one launch
-            int nfres, tiles_x, tiles;
-            fault_bc_grid(g, nfres, tiles_x, tiles);
-            k_fault_bc<T><<<nfres + tiles, b2, 0, st>>>(g, f, q, c, law, fs, it_dev, h, status, nfres, tiles_x);
-        } else {           // the same as separate launches, trial tractions in q.txt / q.tzt
-            if (!p.fspace) k_str_fs<T><<<dim3((p.nxt + 31) / 32, (p.nyt + 7) / 8), b2, 0, st>>>(g, f);  // fres
-            k_traction<T><<<dim3((nxT + 31) / 32, (nzT + 7) / 8), b2, 0, st>>>(g, f, q, c, it_dev);
-            k_friction<T><<<dim3((nxT + 31) / 32, (nzT + 7) / 8), b2, 0, st>>>(g, f, q, c, law, fs, it_dev);
-            k_output<T><<<dim3((nxT + 31) / 32, (nzT + 7) / 8), b2, 0, st>>>(g, f, q, law, it_dev, h, status);
+        if (ph >= 2) {
+            h.ring = ring; h.cap = hist_cap; h.stride = p.history_stride; h.nf = nf; h.nst = p.nstations;
+            for (int s = 0; s < p.nstations; ++s) { h.sta[3 * s] = p.staX[s]; h.sta[3 * s + 1] = p.staY[s]; h.sta[3 * s + 2] = p.staZ[s]; }
+            h.seis = seis;
         }
-        if (law == FD3D_LAW_FVW && fs.nucleation) {
-            const int ni = (p.nxt - p.nabc) - (p.nabc - 1) + 1, nk = g.ks() - (p.nabc - 1) + 1;
-            k_nucleation<T><<<dim3((ni + 31) / 32, (nk + 7) / 8), b2, 0, st>>>(g, q, c, fs, it_dev);
+        switch (ph) {
+        case 0:  // velocity half-step
+            if (ov) fork(0);
+            kbeg(0);
+            if (icfg.variant == IV_TMA) launch_vel_interior_tma<T>(vmaps, icfg, g, f, c, status, st);
+            else launch_vel_interior<T>(icfg, g, f, c, st);
+            kend(0);
+            kbeg(1);
+            k_vel_fault<T><<<dim3((std::max(nxT, p.nxt) + 31) / 32, (nzT + 7) / 8), b2, 0, sp>>>(g, f, q, c, law, fs, it_dev, status);
+            kend(1);
+            kbeg(2);
+            launch_pml<T>(false, pml_minb_vel, sp, g, f, D, X, c, status);
+            kend(2);
+            if (ov) join(1);
+            kbeg(3);
+            if (!p.fspace && top) k_vel_fs<T><<<dim3((p.nxt + 31) / 32, (p.nyt + 7) / 8), b2, 0, st>>>(g, f);  // fuvw
+            kend(3);
+            break;
+        case 1:  // stress sweeps
+            if (ov) fork(2);
+            kbeg(4);
+            if (icfg.variant == IV_TMA) launch_str_interior_tma<T>(smaps, icfg, g, f, c, status, st);
+            else launch_str_interior<T>(icfg, g, f, c, st);
+            kend(4);
+            kbeg(5);
+            k_str_fault<T><<<dim3((nxT + 31) / 32, (nzT + 7) / 8), b2, 0, sp>>>(g, f, q, c);
+            kend(5);
+            kbeg(6);
+            launch_pml<T>(true, pml_minb_str, sp, g, f, D, X, c, status);
+            kend(6);
+            if (ov) join(3);
+            break;
+        case 2:  // fault boundary condition
+            kbeg(7);
+            if (!split_bc) {   // fres and the fused trial traction, friction and output tiles in one launch
+                int nfres, tiles_x, tiles;
+                fault_bc_grid(g, nfres, tiles_x, tiles);
+                k_fault_bc<T><<<nfres + tiles, b2, 0, st>>>(g, f, q, c, law, fs, it_dev, h, status, nfres, tiles_x);
+            } else {           // the same as separate launches, trial tractions in q.txt / q.tzt
+                if (!p.fspace && top) k_str_fs<T><<<dim3((p.nxt + 31) / 32, (p.nyt + 7) / 8), b2, 0, st>>>(g, f);  // fres
+                k_traction<T><<<dim3((nxT + 31) / 32, (nzT + 7) / 8), b2, 0, st>>>(g, f, q, c, it_dev);
+            }
+            break;
+        case 3:
+            if (split_bc) k_friction<T><<<dim3((nxT + 31) / 32, (nzT + 7) / 8), b2, 0, st>>>(g, f, q, c, law, fs, it_dev);
+            break;
+        default:
+            if (split_bc) k_output<T><<<dim3((nxT + 31) / 32, (nzT + 7) / 8), b2, 0, st>>>(g, f, q, law, it_dev, h, status);
+            if (law == FD3D_LAW_FVW && fs.nucleation) {  // every node of the plane (a z-slab too: no halo needed)
+                const int ni = (p.nxt - p.nabc) - (p.nabc - 1) + 1, nk = g.ks() - (p.nabc - 1) + 1;
+                k_nucleation<T><<<dim3((ni + 31) / 32, (nk + 7) / 8), b2, 0, st>>>(g, q, c, fs, it_dev);
+            }
+            kend(7);
+            break;
         }
-        kend(7);
+        return FD3D_OK;
+    }
+
+    int halo_arrays(int set, std::vector<HaloArray>& out) override {
+        out.clear();
+        const size_t e = sizeof(T), pl = (size_t)g.plane, row = (size_t)p.nxt;
+        T* vel[] = {f.u, f.v, f.w};
+        T* str[] = {f.xx, f.yy, f.zz, f.xy, f.yz, f.xz};
+        T* trial[] = {q.txt, q.tzt, q.RFx, q.RFz};
+        T* trac[] = {q.tx, q.tz};
+        T** a = nullptr;
+        size_t na = 0, unit = pl;
+        switch (set) {
+            case HALO_VEL: a = vel; na = 3; break;
+            case HALO_STR: a = str; na = 6; break;
+            case HALO_TRIAL: a = trial; na = 4; unit = row; break;
+            case HALO_TRACTION: a = trac; na = 2; unit = row; break;
+            default: return FD3D_ERR_ARG;
+        }
+        for (size_t k = 0; k < na; ++k) out.push_back(HaloArray{a[k], e, unit});
         return FD3D_OK;
     }
 
@@ -701,8 +782,10 @@ struct Ctx : CtxBase {
             case FD3D_FIELD_XZ: src = f.xz; break;
             default: return FD3D_ERR_ARG;
         }
+        // the planes this context owns (all of them for a whole model); the host array
+        // keeps its other planes, so the z-slabs of a model fill one array between them
         std::vector<T> slab((size_t)g.plane);
-        for (int k = 0; k < p.nzt; ++k) {
+        for (int k = g.klo - 1; k < g.khi; ++k) {
             CK(cudaMemcpyAsync(slab.data(), src + (size_t)g.plane * k, (size_t)g.plane * sizeof(T), cudaMemcpyDeviceToHost, st));
             CK(cudaStreamSynchronize(st));
             for (int j = 0; j < p.nyt; ++j) {
@@ -745,6 +828,7 @@ struct Ctx : CtxBase {
     }
 
     int moment_rate(int rec0, int nrec, double* host) override {
+        if (slab) return FD3D_ERR_STATE;  // a sum over the whole fault plane
         for (int r0 = 0; r0 < nrec; r0 += hist_cap) {  // at most one ring of records per pass
             const int n = std::min(hist_cap, nrec - r0);
             k_moment_rate<T><<<n, POST_THREADS, 0, st>>>(g, f, (const T*)ring, hist_cap, nf, rec0 + r0, (double)c.dh,
@@ -757,6 +841,7 @@ struct Ctx : CtxBase {
     }
 
     int post(double* out4) override {
+        if (slab) return FD3D_ERR_STATE;  // sums over the whole fault plane
         const double dh2 = (double)(c.dh * c.dh);  // dh*dh in the field type, as the reference
         k_post<T><<<POST_BLOCKS, POST_THREADS, 0, st>>>(g, f, q, (double)c.dh, dh2, rvel_d, czone_d, part_d);
         k_post_sum<<<1, POST_THREADS, 0, st>>>(part_d, POST_BLOCKS, sums_d);
@@ -823,15 +908,20 @@ int fd3d_set_device(int dev) {
     return FD3D_OK;
 }
 
-int fd3d_ctx_create(const fd3d_params* p, fd3d_ctx** out) {
+static int create_ctx(const fd3d_params* p, int slab_lo, int slab_hi, fd3d_ctx** out) {
     if (!out) return FD3D_ERR_ARG;
     *out = nullptr;
     int rc = validate_params(p);
     if (rc) return rc;
+    const bool slab = slab_lo > 0;
+    if (slab && !slab_range_ok(*p, slab_lo, slab_hi)) return FD3D_ERR_ARG;
     int n = 0;
     if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) { cudaGetLastError(); return FD3D_ERR_NODEV; }
     CtxBase* c = (p->precision == FD3D_PREC_F64) ? (CtxBase*)new Ctx<double>() : (CtxBase*)new Ctx<float>();
     c->p = *p;
+    c->slab = slab;
+    c->slab_lo = slab_lo;
+    c->slab_hi = slab_hi;
     // manual override of the interior sweep variant: FD3D_INTERIOR=point|tiled|pipe,
     // FD3D_KCHUNK=<planes per CTA>, FD3D_BY=<CTA rows of the point kernel>
     if (const char* e = std::getenv("FD3D_INTERIOR")) {
@@ -850,12 +940,27 @@ int fd3d_ctx_create(const fd3d_params* p, fd3d_ctx** out) {
         c->pml_minb_vel = std::min(4, std::max(1, v));
         c->pml_minb_str = n == 2 ? std::min(4, std::max(1, s)) : c->pml_minb_vel;
     }
+    if (slab && c->icfg.variant != IV_TMA) { delete c; return FD3D_ERR_ARG; }  // z-slabs: the TMA sweeps only
     rc = c->alloc();
     if (rc) {
         delete c;
         return rc == FD3D_ERR_CUDA ? FD3D_ERR_NOMEM : rc;
     }
     *out = new fd3d_ctx{c};
+    return FD3D_OK;
+}
+
+int fd3d_ctx_create(const fd3d_params* p, fd3d_ctx** out) { return create_ctx(p, 0, 0, out); }
+
+int fd3d_ctx_create_slab(const fd3d_params* p, int k_lo, int k_hi, fd3d_ctx** out) {
+    if (k_lo < 1) return FD3D_ERR_ARG;
+    return create_ctx(p, k_lo, k_hi, out);
+}
+
+int fd3d_slab_range(fd3d_ctx* ctx, int* k_lo, int* k_hi) {
+    if (!ctx || !k_lo || !k_hi) return FD3D_ERR_ARG;
+    *k_lo = ctx->impl->g.klo;
+    *k_hi = ctx->impl->g.khi;
     return FD3D_OK;
 }
 
@@ -950,7 +1055,7 @@ int fd3d_run(fd3d_ctx* ctx, int nsteps) {
     if (!ctx || nsteps < 0) return FD3D_ERR_ARG;
     CtxBase* c = ctx->impl;
     DeviceGuard dg(c->device);
-    if (!c->medium_ok || !c->fault_ok) return FD3D_ERR_STATE;
+    if (!c->medium_ok || !c->fault_ok || c->slab) return FD3D_ERR_STATE;  // a z-slab steps in its group
     CK(cudaEventRecord(c->ev0, c->st));
     int left = nsteps;
     if (!c->profiling) {
@@ -1146,7 +1251,277 @@ int fd3d_fetch_final(fd3d_ctx* ctx, double* slipX, double* slipZ, double* ruptim
 int fd3d_write_results(fd3d_ctx* ctx, const char* dir, int rk) {
     fd3d::TraceRange trace_("fd3d_write_results");
     if (!ctx || !dir || (rk != 4 && rk != 8)) return FD3D_ERR_ARG;
+    if (ctx->impl->slab) return FD3D_ERR_STATE;  // a z-slab holds part of the planes
     return fd3d::write_results(ctx, ctx->impl->p, ctx->impl->nf, ctx->impl->rec_written, dir, rk);
+}
+
+
+// ---------------------------------------------------------------- z-slab groups
+// One model over several contexts (GPUs), each owning a range of planes.  A step runs in
+// STEP_PHASES phases; after phases 0-3 every slab pulls the halo planes (or fault-plane
+// rows) of the arrays its neighbours just updated, two on each side, into its own memory:
+// one contiguous copy per array and side, since planes are the slowest index.  Each pull
+// waits (cudaStreamWaitEvent) for the neighbour's phase; what a neighbour writes next is
+// never what was just pulled from it until the next exchange of the same set, which in
+// turn waits for this slab, so no slab overwrites data another is still copying.
+
+// Planes 1..nzt in n slabs of about equal cost (a PML cell moves about 2.2 times the
+// bytes of an interior cell), every slab valid for slab_range_ok.
+int fd3d_slab_plan(const fd3d_params* p, int n, int* k_lo, int* k_hi) {
+    if (!p || n < 1 || !k_lo || !k_hi) return FD3D_ERR_ARG;
+    int rc = validate_params(p);
+    if (rc) return rc;
+    const int nzt = p->nzt, nab = p->nabc, ks = nzt - p->nfs;
+    std::vector<double> w(nzt + 1, 0.0), cum(nzt + 1, 0.0);
+    const double plane = (double)p->nxt * p->nyt;
+    const double pml_cols = 2.0 * nab * p->nyt + (double)nab * (p->nxt - 2 * nab);
+    for (int k = 1; k <= nzt; ++k) {
+        const bool zpml = k <= nab || (p->fspace && k > ks);
+        w[k] = zpml ? 2.2 * plane : (plane - pml_cols) + 2.2 * pml_cols;
+        cum[k] = cum[k - 1] + w[k];
+    }
+    int k = 0;
+    for (int r = 0; r < n; ++r) {
+        k_lo[r] = k + 1;
+        if (r == n - 1) { k_hi[r] = nzt; break; }
+        const double target = cum[nzt] * (r + 1) / n;
+        int e = k + SLAB_MIN;
+        while (e < nzt && cum[e] < target) ++e;
+        e = std::min(e, ks - 3);                                  // the top slab owns ks-2 .. nzt
+        e = std::min(e, ks - 3 - SLAB_MIN * (n - 2 - r));         // room for the slabs still to come
+        k_hi[r] = e;
+        k = e;
+    }
+    for (int r = 0; r < n; ++r)
+        if (!slab_range_ok(*p, k_lo[r], k_hi[r]) || (r > 0 && k_lo[r] != k_hi[r - 1] + 1)) return FD3D_ERR_ARG;
+    return FD3D_OK;
+}
+
+struct fd3d_slab_group {
+    std::vector<fd3d::CtxBase*> r;
+    std::vector<cudaEvent_t> ev;   // per slab: its last phase is enqueued up to here
+};
+
+int fd3d_slab_group_create(fd3d_ctx* const* ctxs, int n, fd3d_slab_group** out) {
+    if (!ctxs || n < 1 || !out) return FD3D_ERR_ARG;
+    *out = nullptr;
+    std::vector<CtxBase*> r(n);
+    for (int i = 0; i < n; ++i) {
+        if (!ctxs[i] || !ctxs[i]->impl->slab) return FD3D_ERR_ARG;
+        r[i] = ctxs[i]->impl;
+    }
+    // one model: same parameters, same field type, planes 1..nzt covered in order
+    for (int i = 0; i < n; ++i) {
+        const fd3d_params &a = r[i]->p, &b = r[0]->p;
+        if (a.nxt != b.nxt || a.nyt != b.nyt || a.nzt != b.nzt || a.nabc != b.nabc || a.fspace != b.fspace ||
+            a.law != b.law || a.precision != b.precision || a.dt != b.dt || a.dh != b.dh)
+            return FD3D_ERR_ARG;
+        if (r[i]->g.klo != (i == 0 ? 1 : r[i - 1]->g.khi + 1)) return FD3D_ERR_ARG;
+    }
+    if (r[n - 1]->g.khi != r[0]->p.nzt) return FD3D_ERR_ARG;
+    auto* G = new fd3d_slab_group;
+    G->r = r;
+    G->ev.assign(n, nullptr);
+    for (int i = 0; i < n; ++i) {
+        DeviceGuard dg(r[i]->device);
+        if (cudaEventCreateWithFlags(&G->ev[i], cudaEventDisableTiming) != cudaSuccess) {
+            cudaGetLastError();
+            for (auto e : G->ev) if (e) cudaEventDestroy(e);
+            delete G;
+            return FD3D_ERR_CUDA;
+        }
+        // neighbours on other devices: peer access for the pulls (a copy still works without)
+        for (int nb : {i - 1, i + 1})
+            if (nb >= 0 && nb < n && r[nb]->device != r[i]->device) {
+                int can = 0;
+                if (cudaDeviceCanAccessPeer(&can, r[i]->device, r[nb]->device) == cudaSuccess && can)
+                    cudaDeviceEnablePeerAccess(r[nb]->device, 0);
+                cudaGetLastError();  // already enabled is fine
+            }
+    }
+    *out = G;
+    return FD3D_OK;
+}
+
+int fd3d_slab_group_destroy(fd3d_slab_group* G) {
+    if (!G) return FD3D_ERR_ARG;
+    for (size_t i = 0; i < G->r.size(); ++i) {
+        DeviceGuard dg(G->r[i]->device);
+        cudaStreamSynchronize(G->r[i]->st);
+        if (G->ev[i]) cudaEventDestroy(G->ev[i]);
+    }
+    delete G;
+    return FD3D_OK;
+}
+
+// pull two planes / rows of every array of the set from the slab below (its top two) and
+// from the slab above (its bottom two) into slab i's halo
+static int slab_exchange(fd3d_slab_group* G, int set) {
+    const int n = (int)G->r.size();
+    std::vector<std::vector<HaloArray>> arr(n);
+    for (int i = 0; i < n; ++i) {
+        DeviceGuard dg(G->r[i]->device);
+        int rc = G->r[i]->halo_arrays(set, arr[i]);
+        if (rc) return rc;
+        CK(cudaEventRecord(G->ev[i], G->r[i]->st));
+    }
+    for (int i = 0; i < n; ++i) {
+        CtxBase* c = G->r[i];
+        DeviceGuard dg(c->device);
+        for (int side = 0; side < 2; ++side) {
+            const int nb = side == 0 ? i - 1 : i + 1;
+            if (nb < 0 || nb >= n) continue;
+            CK(cudaStreamWaitEvent(c->st, G->ev[nb], 0));
+            const long long k0 = side == 0 ? c->g.klo - 2 : c->g.khi + 1;  // first halo plane / row
+            for (size_t a = 0; a < arr[i].size(); ++a) {
+                const HaloArray &d = arr[i][a], &s = arr[nb][a];
+                const size_t off = d.unit * (size_t)(k0 - 1) * d.elem, bytes = 2 * d.unit * d.elem;
+                CK(cudaMemcpyAsync((char*)d.base + off, (const char*)s.base + off, bytes, cudaMemcpyDefault, c->st));
+            }
+        }
+    }
+    return FD3D_OK;
+}
+
+int fd3d_slab_group_run(fd3d_slab_group* G, int nsteps) {
+    fd3d::TraceRange trace_("fd3d_slab_group_run");
+    if (!G || nsteps < 0) return FD3D_ERR_ARG;
+    for (CtxBase* c : G->r)
+        if (!c->medium_ok || !c->fault_ok) return FD3D_ERR_STATE;
+    for (CtxBase* c : G->r) {
+        DeviceGuard dg(c->device);
+        CK(cudaEventRecord(c->ev0, c->st));
+    }
+    for (int s = 0; s < nsteps; ++s)
+        for (int ph = 0; ph < STEP_PHASES; ++ph) {
+            for (CtxBase* c : G->r) {
+                DeviceGuard dg(c->device);
+                int rc = c->enqueue_phase(ph);
+                if (rc) return rc;
+            }
+            const int set = halo_after_phase(ph);
+            if (set != HALO_NONE && G->r.size() > 1) {
+                int rc = slab_exchange(G, set);
+                if (rc) return rc;
+            }
+        }
+    for (CtxBase* c : G->r) {
+        DeviceGuard dg(c->device);
+        CK(cudaGetLastError());
+        CK(cudaEventRecord(c->ev1, c->st));
+        c->steps_done += nsteps;
+        c->mark_run();
+    }
+    return FD3D_OK;
+}
+
+// wait for every slab; the run time is the longest slab's; the first error status of any
+int fd3d_slab_group_sync(fd3d_slab_group* G, float* ms) {
+    if (!G) return FD3D_ERR_ARG;
+    int first = FD3D_OK;
+    float worst = 0.f;
+    for (size_t i = 0; i < G->r.size(); ++i) {
+        DeviceGuard dg(G->r[i]->device);
+        fd3d_ctx tmp{G->r[i]};
+        const int rc = fd3d_sync(&tmp);
+        if (rc && !first) first = rc;
+        worst = std::max(worst, G->r[i]->last_ms);
+    }
+    if (ms) *ms = worst;
+    return first;
+}
+
+
+// ---- z-slabs in separate processes (one GPU each): the halo exchange over NCCL --------
+int fd3d_nccl_unique_id(unsigned char* id) {
+    if (!id) return FD3D_ERR_ARG;
+    const NcclApi& n = nccl();
+    if (!n.ok) return FD3D_ERR_NODEV;
+    ncclUniqueId u;
+    if (n.GetUniqueId(&u) != ncclSuccess) return FD3D_ERR_CUDA;
+    std::memcpy(id, u.internal, NCCL_UNIQUE_ID_BYTES);
+    return FD3D_OK;
+}
+
+int fd3d_slab_connect(fd3d_ctx* ctx, const unsigned char* id, int rank, int nranks) {
+    if (!ctx || !id || nranks < 1 || rank < 0 || rank >= nranks) return FD3D_ERR_ARG;
+    CtxBase* c = ctx->impl;
+    if (!c->slab || c->comm) return FD3D_ERR_STATE;
+    const NcclApi& n = nccl();
+    if (!n.ok) return FD3D_ERR_NODEV;
+    DeviceGuard dg(c->device);
+    ncclUniqueId u;
+    std::memcpy(u.internal, id, NCCL_UNIQUE_ID_BYTES);
+    ncclComm_t comm = nullptr;
+    if (n.CommInitRank(&comm, nranks, u, rank) != ncclSuccess) return FD3D_ERR_CUDA;
+    // every rank's plane range: rank r must hold the r-th slab from the bottom
+    int* d = nullptr;
+    std::vector<int> all(2 * (size_t)nranks);
+    const int mine[2] = {c->g.klo, c->g.khi};
+    bool ok = cudaMalloc(&d, sizeof(int) * 2 * (nranks + 1)) == cudaSuccess &&
+              cudaMemcpyAsync(d, mine, sizeof mine, cudaMemcpyHostToDevice, c->st) == cudaSuccess &&
+              n.AllGather(d, d + 2, 2, ncclInt, comm, c->st) == ncclSuccess &&
+              cudaMemcpyAsync(all.data(), d + 2, sizeof(int) * 2 * nranks, cudaMemcpyDeviceToHost, c->st) == cudaSuccess &&
+              cudaStreamSynchronize(c->st) == cudaSuccess;
+    if (d) cudaFree(d);
+    cudaGetLastError();
+    for (int r = 0; ok && r < nranks; ++r)
+        ok = all[2 * r] == (r == 0 ? 1 : all[2 * r - 1] + 1) && (r < nranks - 1 || all[2 * r + 1] == c->p.nzt);
+    if (!ok) { n.CommDestroy(comm); return FD3D_ERR_ARG; }
+    c->comm = comm;
+    c->slab_rank = rank;
+    c->slab_nranks = nranks;
+    return FD3D_OK;
+}
+
+// the exchange of one halo set with the ranks below and above: the same planes / rows as
+// slab_exchange, each sent as two contiguous planes / rows and received into the halo
+static int nccl_exchange(CtxBase* c, int set) {
+    std::vector<HaloArray> arr;
+    int rc = c->halo_arrays(set, arr);
+    if (rc) return rc;
+    const NcclApi& n = nccl();
+    if (n.GroupStart() != ncclSuccess) return FD3D_ERR_CUDA;
+    bool ok = true;
+    for (int side = 0; side < 2; ++side) {
+        const int nb = side == 0 ? c->slab_rank - 1 : c->slab_rank + 1;
+        if (nb < 0 || nb >= c->slab_nranks) continue;
+        const long long send_k0 = side == 0 ? c->g.klo : c->g.khi - 1;
+        const long long recv_k0 = side == 0 ? c->g.klo - 2 : c->g.khi + 1;
+        for (const HaloArray& a : arr) {
+            const size_t bytes = 2 * a.unit * a.elem;
+            ok &= n.Send((const char*)a.base + a.unit * (size_t)(send_k0 - 1) * a.elem, bytes, ncclChar, nb, c->comm,
+                         c->st) == ncclSuccess;
+            ok &= n.Recv((char*)a.base + a.unit * (size_t)(recv_k0 - 1) * a.elem, bytes, ncclChar, nb, c->comm,
+                         c->st) == ncclSuccess;
+        }
+    }
+    ok &= n.GroupEnd() == ncclSuccess;
+    return ok ? FD3D_OK : FD3D_ERR_CUDA;
+}
+
+int fd3d_slab_run(fd3d_ctx* ctx, int nsteps) {
+    fd3d::TraceRange trace_("fd3d_slab_run");
+    if (!ctx || nsteps < 0) return FD3D_ERR_ARG;
+    CtxBase* c = ctx->impl;
+    if (!c->slab || !c->comm || !c->medium_ok || !c->fault_ok) return FD3D_ERR_STATE;
+    DeviceGuard dg(c->device);
+    CK(cudaEventRecord(c->ev0, c->st));
+    for (int s = 0; s < nsteps; ++s)
+        for (int ph = 0; ph < STEP_PHASES; ++ph) {
+            int rc = c->enqueue_phase(ph);
+            if (rc) return rc;
+            const int set = halo_after_phase(ph);
+            if (set != HALO_NONE && c->slab_nranks > 1) {
+                rc = nccl_exchange(c, set);
+                if (rc) return rc;
+            }
+        }
+    CK(cudaGetLastError());
+    CK(cudaEventRecord(c->ev1, c->st));
+    c->steps_done += nsteps;
+    c->mark_run();
+    return FD3D_OK;
 }
 
 }  // extern "C"
@@ -1228,7 +1603,7 @@ extern "C" int fd3d_run_noalloc(fd3d_ctx* ctx, int nsteps) {
     fd3d::TraceRange trace_("fd3d_run_noalloc");
     if (!ctx || nsteps < 0) return FD3D_ERR_ARG;
     CtxBase* c = ctx->impl;
-    if (!c->medium_ok || !c->fault_ok) return FD3D_ERR_STATE;
+    if (!c->medium_ok || !c->fault_ok || c->slab) return FD3D_ERR_STATE;
     const long long n2 = (long long)c->p.nxt * c->p.nzt;
     if (n2 > FD3D_NOALLOC_MAX_PLANE) {
         std::fprintf(stderr, "fd3d_run_noalloc: fault plane nxt*nzt = %lld nodes exceeds the limit of %d\n", n2,

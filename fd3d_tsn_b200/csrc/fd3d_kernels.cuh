@@ -37,8 +37,8 @@ __global__ void __launch_bounds__(256) k_vel_interior(Grid g, Fields<T> f, StepC
     const int i = g.nabc + 1 + blockIdx.x * blockDim.x + threadIdx.x;
     const int j = g.nabc + 1 + blockIdx.y * blockDim.y + threadIdx.y;
     if (i > g.nxt - g.nabc || j > g.nyt - 2) return;
-    const int kb = g.nabc + 1 + blockIdx.z * kchunk;
-    const int ke = min(kb + kchunk - 1, g.ks());
+    const int kb = g.kin_lo() + blockIdx.z * kchunk;
+    const int ke = min(kb + kchunk - 1, g.kin_hi());
     const long long sy = g.px, sz = g.plane;
     const T c1 = c.c1, c2 = c.c2;
     const T* __restrict__ xx = f.xx; const T* __restrict__ yy = f.yy; const T* __restrict__ zz = f.zz;
@@ -86,12 +86,12 @@ __device__ __forceinline__ void vel_fault_body(Grid g, Fields<T> f, Fault<T> q, 
     const long long sy = g.px, sz = g.plane;
     // ghost row k=ks+1: v(:,nyt,ks+1) = v(:,nyt-1,ks+1)  (bnd2d mirror, fd3d_deriv.f90:225-232);
     // under FSPACE that row belongs to the top PML strip, whose tiles mirror it
-    if (!g.fspace && kk == 0 && ii < g.nxt) {
+    if (!g.fspace && kk == 0 && ii < g.nxt && g.owns(ks + 1)) {
         const long long p = g.at(ii + 1, g.nyt - 1, ks + 1);
         f.v[p + sy] = f.v[p];
     }
-    const int i = g.nabc + 1 + ii, k = g.nabc + 1 + kk;
-    if (i > g.nxt - g.nabc || k > ks) return;
+    const int i = g.nabc + 1 + ii, k = g.kin_lo() + kk;
+    if (i > g.nxt - g.nabc || k > g.kin_hi()) return;
     const int n2 = g.at2(i, k);
     {   // uxx0a / vyy0a / wzz0a  (fd3d_deriv.f90:284-508)
         const long long p = g.at(i, g.nyt - 1, k);
@@ -162,6 +162,7 @@ struct PmlDesc {
     long long cum[PML_MAXS + 1];  // first compact index of each strip (a multiple of PML_TILE); cum[PML_MAXS] = end
     long long cnt[PML_MAXS];      // cells of each strip's u/w loop range (0 for an absent strip)
     int ns;                       // strips present: 4, or 5 under FSPACE
+    int klo, khi;                 // planes updated (Grid::klo, khi)
 };
 
 // PML auxiliary components (the 24 split fields that init_pml allocates per strip,
@@ -231,7 +232,9 @@ __device__ __forceinline__ int pml_tile_strip(const PmlDesc& D, long long t0) {
     return (t0 >= D.cum[1]) + (t0 >= D.cum[2]) + (t0 >= D.cum[3]) + (t0 >= D.cum[4]);
 }
 
-// (i,j,k) of compact cell index t of strip s; false past the strip's last cell
+// (i,j,k) of compact cell index t of strip s; false past the strip's last cell and, for
+// a z-slab (SLAB), outside its planes
+template <bool SLAB>
 __device__ __forceinline__ bool pml_cell(const PmlDesc& D, int s, long long t, int& i, int& j, int& k) {
     const long long r0 = t - D.cum[s];
     if (r0 >= D.cnt[s]) return false;
@@ -248,7 +251,7 @@ __device__ __forceinline__ bool pml_cell(const PmlDesc& D, int s, long long t, i
         k2 = q1 / nj; rj = q1 - k2 * nj;
     }
     i = S.nxb + (int)ri; j = S.nyb + (int)rj; k = S.nzb + (int)k2;
-    return true;
+    return !SLAB || (k >= D.klo && k <= D.khi);
 }
 
 // Start of a tile: every thread orders its earlier generic accesses of the staging
@@ -279,7 +282,7 @@ __device__ __forceinline__ bool pml_tile_wait(uint32_t bar, uint32_t parity, int
 }
 
 // pml_uvw in one tile of strip class C (fd3d_deriv.f90:1927-2293): one cell per thread.
-template <class T, int C>
+template <class T, int C, bool SLAB>
 __device__ __forceinline__ bool vel_pml_tile_c(const Grid& g, const Fields<T>& f, const PmlDesc& D,
                                                const PmlAux<T>& X, const StepConst<T>& c, int s, long long t0, T* sm,
                                                uint32_t bar, uint32_t parity, int* status) {
@@ -288,7 +291,7 @@ __device__ __forceinline__ bool vel_pml_tile_c(const Grid& g, const Fields<T>& f
     T* gaux = X.vel + t0 * AUX_NV;
     pml_tile_begin(sm, gaux, AUX_NV, bar);
     int i = 0, j = 0, k = 0;
-    const bool act = pml_cell(D, s, t0 + l, i, j, k);
+    const bool act = pml_cell<SLAB>(D, s, t0 + l, i, j, k);
     T d = 1, rl = 0, xx0 = 0, xx1 = 0, xy0 = 0, xy1 = 0, xz0 = 0, xz1 = 0, xz2 = 0, yz0 = 0, yz1 = 0, zz0 = 0, zz1 = 0;
     T xy2 = 0, yy0 = 0, yy1 = 0, yz2 = 0, vold = 0;
     Damp<T> ox{}, oxS{}, oy{}, oz{};
@@ -346,16 +349,16 @@ __device__ __forceinline__ bool vel_pml_tile_c(const Grid& g, const Fields<T>& f
 // pml_uvw: split-field PML velocity in the strips (fd3d_deriv.f90:1927-2293), one
 // tile of PML_TILE consecutive cells per CTA of PML_TILE threads.  Returns false if the
 // staging copy timed out.
-template <class T>
+template <class T, bool SLAB = false>
 __device__ __forceinline__ bool vel_pml_tile(const Grid& g, const Fields<T>& f, const PmlDesc& D, const PmlAux<T>& X,
                                              const StepConst<T>& c, int tile, T* sm, uint32_t bar, uint32_t parity,
                                              int* status) {
     const long long t0 = (long long)tile * PML_TILE;
     const int s = pml_tile_strip(D, t0);
     switch (pml_class(s)) {
-        case 0: return vel_pml_tile_c<T, 0>(g, f, D, X, c, s, t0, sm, bar, parity, status);
-        case 1: return vel_pml_tile_c<T, 1>(g, f, D, X, c, s, t0, sm, bar, parity, status);
-        default: return vel_pml_tile_c<T, 2>(g, f, D, X, c, s, t0, sm, bar, parity, status);
+        case 0: return vel_pml_tile_c<T, 0, SLAB>(g, f, D, X, c, s, t0, sm, bar, parity, status);
+        case 1: return vel_pml_tile_c<T, 1, SLAB>(g, f, D, X, c, s, t0, sm, bar, parity, status);
+        default: return vel_pml_tile_c<T, 2, SLAB>(g, f, D, X, c, s, t0, sm, bar, parity, status);
     }
 }
 
@@ -408,8 +411,8 @@ __global__ void __launch_bounds__(256) k_str_interior(Grid g, Fields<T> f, StepC
     const int i = g.nabc + 1 + blockIdx.x * blockDim.x + threadIdx.x;
     const int j = g.nabc + 1 + blockIdx.y * blockDim.y + threadIdx.y;
     if (i > g.nxt - g.nabc || j > g.nyt - 2) return;
-    const int kb = g.nabc + 1 + blockIdx.z * kchunk;
-    const int ke = min(kb + kchunk - 1, g.ks());
+    const int kb = g.kin_lo() + blockIdx.z * kchunk;
+    const int ke = min(kb + kchunk - 1, g.kin_hi());
     const long long sy = g.px, sz = g.plane;
     const T c1 = c.c1, c2 = c.c2, dth = c.dth;
     const T* __restrict__ u = f.u; const T* __restrict__ v = f.v; const T* __restrict__ w = f.w;
@@ -440,8 +443,8 @@ __global__ void __launch_bounds__(256) k_str_interior(Grid g, Fields<T> f, StepC
 template <class T>
 __device__ __forceinline__ void str_fault_body(Grid g, Fields<T> f, Fault<T> q, StepConst<T> c, int bx_, int by_, int bz_) {
     const int i = g.nabc + 1 + bx_ * blockDim.x + threadIdx.x;
-    const int k = g.nabc + 1 + by_ * blockDim.y + threadIdx.y;
-    if (i > g.nxt - g.nabc || k > g.ks()) return;
+    const int k = g.kin_lo() + by_ * blockDim.y + threadIdx.y;
+    if (i > g.nxt - g.nabc || k > g.kin_hi()) return;
     const long long sy = g.px, sz = g.plane;
     const T dth = c.dth, dth2 = c.dth2, c1 = c.c1, c2 = c.c2;
     {   // sxx, sxy0, sxz0, syz0 at j=nyt-1 (fd3d_deriv.f90:818-1012)
@@ -483,7 +486,7 @@ __device__ __forceinline__ void str_fault_body(Grid g, Fields<T> f, Fault<T> q, 
 }
 
 // pml_xyz in one tile of strip class C (fd3d_deriv.f90:2304-3143), as vel_pml_tile_c
-template <class T, int C>
+template <class T, int C, bool SLAB>
 __device__ __forceinline__ bool str_pml_tile_c(const Grid& g, const Fields<T>& f, const PmlDesc& D,
                                                const PmlAux<T>& X, const StepConst<T>& c, int s, long long t0, T* sm,
                                                uint32_t bar, uint32_t parity, int* status) {
@@ -492,7 +495,7 @@ __device__ __forceinline__ bool str_pml_tile_c(const Grid& g, const Fields<T>& f
     T* gaux = X.str + t0 * AUX_NS;
     pml_tile_begin(sm, gaux, AUX_NS, bar);
     int i = 0, j = 0, k = 0;
-    const bool act = pml_cell(D, s, t0 + l, i, j, k);
+    const bool act = pml_cell<SLAB>(D, s, t0 + l, i, j, k);
     long long p = 0;
     bool dxy = false, top = false;
     const long long sy = g.px, sz = g.plane;
@@ -572,16 +575,16 @@ __device__ __forceinline__ bool str_pml_tile_c(const Grid& g, const Fields<T>& f
 }
 
 // pml_xyz in the strips (fd3d_deriv.f90:2304-3143), one tile per CTA as vel_pml_tile
-template <class T>
+template <class T, bool SLAB = false>
 __device__ __forceinline__ bool str_pml_tile(const Grid& g, const Fields<T>& f, const PmlDesc& D, const PmlAux<T>& X,
                                              const StepConst<T>& c, int tile, T* sm, uint32_t bar, uint32_t parity,
                                              int* status) {
     const long long t0 = (long long)tile * PML_TILE;
     const int s = pml_tile_strip(D, t0);
     switch (pml_class(s)) {
-        case 0: return str_pml_tile_c<T, 0>(g, f, D, X, c, s, t0, sm, bar, parity, status);
-        case 1: return str_pml_tile_c<T, 1>(g, f, D, X, c, s, t0, sm, bar, parity, status);
-        default: return str_pml_tile_c<T, 2>(g, f, D, X, c, s, t0, sm, bar, parity, status);
+        case 0: return str_pml_tile_c<T, 0, SLAB>(g, f, D, X, c, s, t0, sm, bar, parity, status);
+        case 1: return str_pml_tile_c<T, 1, SLAB>(g, f, D, X, c, s, t0, sm, bar, parity, status);
+        default: return str_pml_tile_c<T, 2, SLAB>(g, f, D, X, c, s, t0, sm, bar, parity, status);
     }
 }
 
@@ -609,9 +612,9 @@ template <class T>
 __device__ __forceinline__ void traction_body(Grid g, Fields<T> f, Fault<T> q, StepConst<T> c, const int* it_dev,
                                               int bx_, int by_, int bz_) {
     const int i = g.nabc + 1 + bx_ * blockDim.x + threadIdx.x;
-    const int k = g.nabc + 1 + by_ * blockDim.y + threadIdx.y;
+    const int k = g.kin_lo() + by_ * blockDim.y + threadIdx.y;
     const int ks = g.ks();
-    if (i > g.nxt - g.nabc || k > ks) return;
+    if (i > g.nxt - g.nabc || k > g.kin_hi()) return;
     const long long sy = g.px, sz = g.plane;
     const long long p = g.at(i, g.nyt, k);
     const int n2 = g.at2(i, k);
@@ -654,8 +657,8 @@ template <class T>
 __device__ __forceinline__ void friction_body(Grid g, Fields<T> f, Fault<T> q, StepConst<T> c, int law, FvwScalars s,
                            const int* it_dev, int bx_, int by_, int bz_) {
     const int i = g.nabc + 1 + bx_ * blockDim.x + threadIdx.x;
-    const int k = g.nabc + 1 + by_ * blockDim.y + threadIdx.y;
-    if (i > g.nxt - g.nabc || k > g.ks()) return;
+    const int k = g.kin_lo() + by_ * blockDim.y + threadIdx.y;
+    if (i > g.nxt - g.nabc || k > g.kin_hi()) return;
     const int it = *it_dev;
     const double time = (double)it * c.dtA;
     const double* distX_rd = pp_rd(q.distX, it, q.n2);
@@ -776,13 +779,13 @@ __device__ __forceinline__ void output_body(Grid g, Fields<T> f, Fault<T> q, int
     const bool rec = (it % h.stride) == 0;
     const long long slot = (long long)((it / h.stride - 1) % h.cap);
     const int nxT = g.nxt - 2 * g.nabc, nzT = g.ks() - g.nabc;
-    if (rec && ii < h.nst && kk == 0) {
+    if (rec && ii < h.nst && kk == 0 && g.owns(h.sta[3 * ii + 2])) {
         const long long p = g.at(h.sta[3 * ii], h.sta[3 * ii + 1], h.sta[3 * ii + 2]);
         T* sp = (T*)h.seis + slot * (3 * h.nst) + 3 * ii;
         sp[0] = f.u[p]; sp[1] = f.v[p]; sp[2] = f.w[p];
     }
-    if (ii >= nxT || kk >= nzT) return;
-    const int i = g.nabc + 1 + ii, k = g.nabc + 1 + kk;
+    const int i = g.nabc + 1 + ii, k = g.kin_lo() + kk;
+    if (ii >= nxT || k > g.kin_hi()) return;
     const bool top = (k == g.ks());
     const long long p = g.at(i, g.nyt, k), sz = g.plane;
     const int n2 = g.at2(i, k), e1 = g.at2(i + 1, k), e2 = g.at2(i, k + 1), e3 = g.at2(i + 1, k + 1);
@@ -811,7 +814,7 @@ __device__ __forceinline__ void output_body(Grid g, Fields<T> f, Fault<T> q, int
         atomicOr(status, ST_NONFINITE);
     if (rec) {
         const long long plane = (long long)nxT * nzT;
-        T* r = (T*)h.ring + slot * h.nf * plane + (long long)kk * nxT + ii;
+        T* r = (T*)h.ring + slot * h.nf * plane + (long long)(k - g.nabc - 1) * nxT + ii;
         r[0] = srx;
         r[plane] = srz;
         r[2 * plane] = scx;
@@ -1152,14 +1155,14 @@ __global__ void k_vel_fault(Grid g, Fields<T> f, Fault<T> q, StepConst<T> c, int
 
 // One PML tile per CTA of PML_TILE threads.  MINB: CTAs that must fit one SM
 // (register cap); 1 leaves it free.
-template <class T, int MINB = 1>
+template <class T, int MINB = 1, bool SLAB = false>
 __global__ void __launch_bounds__(PML_TILE, MINB) k_vel_pml(Grid g, Fields<T> f, const __grid_constant__ PmlDesc D,
                                                              const __grid_constant__ PmlAux<T> X, StepConst<T> c,
-                                                             int* status) {
+                                                             int* status, long long tile0) {
     __shared__ __align__(128) T sm[PML_TILE * AUX_NV];
     __shared__ __align__(8) uint64_t bar;
     if (threadIdx.x == 0) { mbar_init(smem_addr(&bar), 1); fence_mbar_init(); }
-    vel_pml_tile<T>(g, f, D, X, c, blockIdx.x, sm, smem_addr(&bar), 0u, status);
+    vel_pml_tile<T, SLAB>(g, f, D, X, c, tile0 + blockIdx.x, sm, smem_addr(&bar), 0u, status);
 }
 
 template <class T>
@@ -1172,34 +1175,57 @@ __global__ void k_str_fault(Grid g, Fields<T> f, Fault<T> q, StepConst<T> c) {
     str_fault_body<T>(g, f, q, c, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
-template <class T, int MINB = 1>
+template <class T, int MINB = 1, bool SLAB = false>
 __global__ void __launch_bounds__(PML_TILE, MINB) k_str_pml(Grid g, Fields<T> f, const __grid_constant__ PmlDesc D,
                                                              const __grid_constant__ PmlAux<T> X, StepConst<T> c,
-                                                             int* status) {
+                                                             int* status, long long tile0) {
     __shared__ __align__(128) T sm[PML_TILE * AUX_NS];
     __shared__ __align__(8) uint64_t bar;
     if (threadIdx.x == 0) { mbar_init(smem_addr(&bar), 1); fence_mbar_init(); }
-    str_pml_tile<T>(g, f, D, X, c, blockIdx.x, sm, smem_addr(&bar), 0u, status);
+    str_pml_tile<T, SLAB>(g, f, D, X, c, tile0 + blockIdx.x, sm, smem_addr(&bar), 0u, status);
 }
 
-// launch of a PML sweep with a register cap picked at run time
+// The tiles of strip s that hold cells of planes klo..khi: [t0, t1) (k is the slowest
+// index of a strip's compact range)
+inline void pml_strip_tiles(const PmlDesc& D, int s, long long& t0, long long& t1) {
+    const Strip& S = D.s[s];
+    const int kb = std::max(S.nzb, D.klo), ke = std::min(S.nze, D.khi);
+    t0 = t1 = D.cum[s] / PML_TILE;
+    if (D.cnt[s] == 0 || kb > ke) return;
+    const long long per_k = D.cnt[s] / S.nk;
+    t0 = (D.cum[s] + (long long)(kb - S.nzb) * per_k) / PML_TILE;
+    t1 = (D.cum[s] + (long long)(ke - S.nzb + 1) * per_k + PML_TILE - 1) / PML_TILE;
+}
+
+// launch of a PML sweep: one launch over every tile for a whole model (with a register
+// cap picked at run time), one per strip over the tiles of its planes for a z-slab
 template <class T>
 inline void launch_pml(bool stress, int minb, cudaStream_t st, const Grid& g, const Fields<T>& f, const PmlDesc& D,
                        const PmlAux<T>& X, const StepConst<T>& c, int* status) {
+    if (D.klo > 1 || D.khi < g.nzt) {  // a z-slab: the tiles of its planes, strip by strip
+        for (int s = 0; s < D.ns; ++s) {
+            long long t0, t1;
+            pml_strip_tiles(D, s, t0, t1);
+            if (t1 <= t0) continue;
+            if (stress) k_str_pml<T, 1, true><<<(unsigned)(t1 - t0), PML_TILE, 0, st>>>(g, f, D, X, c, status, t0);
+            else k_vel_pml<T, 1, true><<<(unsigned)(t1 - t0), PML_TILE, 0, st>>>(g, f, D, X, c, status, t0);
+        }
+        return;
+    }
     const unsigned nblk = (unsigned)((D.cum[PML_MAXS] + PML_TILE - 1) / PML_TILE);
     if (nblk == 0) return;
-#define FD3D_PML_CASE(MB)                                                               \
-    case MB:                                                                            \
-        if (stress) k_str_pml<T, MB><<<nblk, PML_TILE, 0, st>>>(g, f, D, X, c, status);  \
-        else k_vel_pml<T, MB><<<nblk, PML_TILE, 0, st>>>(g, f, D, X, c, status);         \
+#define FD3D_PML_CASE(MB)                                                                  \
+    case MB:                                                                               \
+        if (stress) k_str_pml<T, MB><<<nblk, PML_TILE, 0, st>>>(g, f, D, X, c, status, 0);  \
+        else k_vel_pml<T, MB><<<nblk, PML_TILE, 0, st>>>(g, f, D, X, c, status, 0);         \
         break;
     switch (minb) {
         FD3D_PML_CASE(2)
         FD3D_PML_CASE(3)
         FD3D_PML_CASE(4)
         default:
-            if (stress) k_str_pml<T, 1><<<nblk, PML_TILE, 0, st>>>(g, f, D, X, c, status);
-            else k_vel_pml<T, 1><<<nblk, PML_TILE, 0, st>>>(g, f, D, X, c, status);
+            if (stress) k_str_pml<T, 1><<<nblk, PML_TILE, 0, st>>>(g, f, D, X, c, status, 0);
+            else k_vel_pml<T, 1><<<nblk, PML_TILE, 0, st>>>(g, f, D, X, c, status, 0);
     }
 #undef FD3D_PML_CASE
 }

@@ -41,8 +41,8 @@ __global__ void __launch_bounds__(NT) k_vel_interior_tiled(Grid g, Fields<T> f, 
     const int i0 = g.nabc + 1 + blockIdx.x * TX, j0 = g.nabc + 1 + blockIdx.y * TY;
     const int i = i0 + tx, j = j0 + ty;
     const bool act = (i <= g.nxt - g.nabc) && (j <= g.nyt - 2);
-    const int kb = g.nabc + 1 + blockIdx.z * kchunk;
-    const int ke = min(kb + kchunk - 1, g.ks());
+    const int kb = g.kin_lo() + blockIdx.z * kchunk;
+    const int ke = min(kb + kchunk - 1, g.kin_hi());
     const int ic = min(i, g.nxt), jc = min(j, g.nyt);
     const long long sz = g.plane;
     const long long pc = g.at(ic, jc, kb);
@@ -88,8 +88,8 @@ __global__ void __launch_bounds__(NT) k_str_interior_tiled(Grid g, Fields<T> f, 
     const int i0 = g.nabc + 1 + blockIdx.x * TX, j0 = g.nabc + 1 + blockIdx.y * TY;
     const int i = i0 + tx, j = j0 + ty;
     const bool act = (i <= g.nxt - g.nabc) && (j <= g.nyt - 2);
-    const int kb = g.nabc + 1 + blockIdx.z * kchunk;
-    const int ke = min(kb + kchunk - 1, g.ks());
+    const int kb = g.kin_lo() + blockIdx.z * kchunk;
+    const int ke = min(kb + kchunk - 1, g.kin_hi());
     const int ic = min(i, g.nxt), jc = min(j, g.nyt);
     const long long sy = g.px, sz = g.plane;
     const long long pc = g.at(ic, jc, kb);
@@ -177,8 +177,8 @@ __device__ __forceinline__ void vel_interior_pipe_body(Grid g, Fields<T> f, Step
     const int i0 = g.nabc + 1 + bx_ * TX, j0 = g.nabc + 1 + by_ * TY;
     const int i = i0 + tx, j = j0 + ty;
     const bool act = (i <= g.nxt - g.nabc) && (j <= g.nyt - 2);
-    const int kb = g.nabc + 1 + bz_ * kchunk;
-    const int ke = min(kb + kchunk - 1, g.ks());
+    const int kb = g.kin_lo() + bz_ * kchunk;
+    const int ke = min(kb + kchunk - 1, g.kin_hi());
     const int ic = min(i, g.nxt), jc = min(j, g.nyt);
     const long long sz = g.plane;
     const long long pc = g.at(ic, jc, kb);
@@ -238,8 +238,8 @@ __device__ __forceinline__ void str_interior_pipe_body(Grid g, Fields<T> f, Step
     const int i0 = g.nabc + 1 + bx_ * TX, j0 = g.nabc + 1 + by_ * TY;
     const int i = i0 + tx, j = j0 + ty;
     const bool act = (i <= g.nxt - g.nabc) && (j <= g.nyt - 2);
-    const int kb = g.nabc + 1 + bz_ * kchunk;
-    const int ke = min(kb + kchunk - 1, g.ks());
+    const int kb = g.kin_lo() + bz_ * kchunk;
+    const int ke = min(kb + kchunk - 1, g.kin_hi());
     const int ic = min(i, g.nxt - 1), jc = min(j, g.nyt - 1);  // keeps the (i+1,j+1) taps in range
     const long long sy = g.px, sz = g.plane;
     const long long pc = g.at(ic, jc, kb);
@@ -324,12 +324,13 @@ struct InteriorCfg {
     int by = 8;          // CTA rows (IV_POINT: block = 32 x by)
 };
 
-inline int interior_nz(const Grid& g) { return g.ks() - g.nabc; }
+inline int interior_nz(const Grid& g) { return std::max(0, g.kin_hi() - g.kin_lo() + 1); }  // planes updated
 
 template <class T>
 void launch_vel_interior(const InteriorCfg& cfg, const Grid& g, const Fields<T>& f, const StepConst<T>& c,
                          cudaStream_t st) {
     const int nxT = g.nxt - 2 * g.nabc, nyI = g.nyt - 2 - g.nabc, nzT = interior_nz(g);
+    if (nzT <= 0) return;  // a z-slab without interior planes
     const int kch = std::max(1, std::min(cfg.kchunk, nzT));
     if (cfg.variant == IV_POINT) {
         const int by = cfg.by;
@@ -346,6 +347,7 @@ template <class T>
 void launch_str_interior(const InteriorCfg& cfg, const Grid& g, const Fields<T>& f, const StepConst<T>& c,
                          cudaStream_t st) {
     const int nxT = g.nxt - 2 * g.nabc, nyI = g.nyt - 2 - g.nabc, nzT = interior_nz(g);
+    if (nzT <= 0) return;  // a z-slab without interior planes
     const int kch = std::max(1, std::min(cfg.kchunk_str, nzT));
     if (cfg.variant == IV_POINT) {
         const int by = cfg.by;
@@ -387,12 +389,14 @@ template <class T>
 bool encode_field_map(CUtensorMap* m, const T* base, const Grid& g, int box_x, int box_y) {
     auto enc = tensor_map_encoder();
     if (!enc) return false;
-    cuuint64_t dims[3] = {(cuuint64_t)g.px, (cuuint64_t)g.nyt, (cuuint64_t)g.nzt};
+    // the stored planes only (a z-slab holds kofs+1 .. kofs+nzl); z = k - 1 - kofs
+    cuuint64_t dims[3] = {(cuuint64_t)g.px, (cuuint64_t)g.nyt, (cuuint64_t)g.nzl};
     cuuint64_t strides[2] = {(cuuint64_t)g.px * sizeof(T), (cuuint64_t)g.plane * sizeof(T)};
     cuuint32_t box[3] = {(cuuint32_t)box_x, (cuuint32_t)box_y, 1};
     cuuint32_t es[3] = {1, 1, 1};
     CUresult r = enc(m, sizeof(T) == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3,
-                     (void*)base, dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                     (void*)(base + g.plane * g.kofs), dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                     CU_TENSOR_MAP_SWIZZLE_NONE,
                      CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     return r == CUDA_SUCCESS;
 }
@@ -439,6 +443,7 @@ template <class T>
 void launch_vel_interior_tma(const VelMaps& M, const InteriorCfg& cfg, const Grid& g, const Fields<T>& f,
                              const StepConst<T>& c, int* status, cudaStream_t st) {
     const int nxT = g.nxt - 2 * g.nabc, nyI = g.nyt - 2 - g.nabc, nzT = interior_nz(g);
+    if (nzT <= 0) return;  // a z-slab without interior planes
     const int kch = std::max(1, std::min(cfg.kchunk, nzT));
     dim3 grid((nxT + 31) / 32, (nyI + 7) / 8, (nzT + kch - 1) / kch);
     const size_t sm = TMA_NS * VelSlot::ELEMS * sizeof(T) + TMA_SMEM_PAD;
@@ -450,6 +455,7 @@ template <class T>
 void launch_str_interior_tma(const StrMaps& M, const InteriorCfg& cfg, const Grid& g, const Fields<T>& f,
                              const StepConst<T>& c, int* status, cudaStream_t st) {
     const int nxT = g.nxt - 2 * g.nabc, nyI = g.nyt - 2 - g.nabc, nzT = interior_nz(g);
+    if (nzT <= 0) return;  // a z-slab without interior planes
     const int kch = std::max(1, std::min(cfg.kchunk_str, nzT));
     dim3 grid((nxT + 31) / 32, (nyI + 7) / 8, (nzT + kch - 1) / kch);
     const size_t sm = TMA_NS * StrSlot::ELEMS * sizeof(T) + TMA_SMEM_PAD;

@@ -2,6 +2,7 @@
 // parameter checks, the padded layout, the PML boxes/profiles (init_pml) and the
 // per-step scalars in the field type.
 #pragma once
+#include <algorithm>
 #include <vector>
 #include "../../include/fd3d_gpu.h"
 #include "fd3d_common.cuh"
@@ -35,8 +36,36 @@ inline Grid make_grid(const fd3d_params& p) {
     g.off = (32 - (p.nabc % 32)) % 32;
     g.px = ((p.nxt + g.off + 31) / 32) * 32;
     g.plane = (long long)g.px * p.nyt;
+    g.klo = 1; g.khi = p.nzt; g.kofs = 0; g.nzl = p.nzt;
     g.n3 = g.plane * p.nzt + 64;
     return g;
+}
+
+// Halo planes a z-slab stores on each side of the planes it owns: the 4th-order sweeps
+// read two planes beyond their own, one more is kept as a margin.
+constexpr int SLAB_HALO = 3;
+
+// The grid of the z-slab that owns planes klo..khi of the model
+inline Grid make_slab_grid(const fd3d_params& p, int klo, int khi) {
+    Grid g = make_grid(p);
+    g.klo = klo; g.khi = khi;
+    const int kb = std::max(1, klo - SLAB_HALO), ke = std::min(p.nzt, khi + SLAB_HALO);
+    g.kofs = kb - 1;
+    g.nzl = ke - kb + 1;
+    g.n3 = g.plane * g.nzl + 64;
+    return g;
+}
+
+// A valid slab range: at least SLAB_MIN planes, and the top slab of a model with a free
+// surface owns the two planes below it (the free-surface rows its fres and fuvw write stay
+// out of every neighbour's halo).
+constexpr int SLAB_MIN = 4;
+inline bool slab_range_ok(const fd3d_params& p, int klo, int khi) {
+    if (klo < 1 || khi > p.nzt || khi - klo + 1 < SLAB_MIN) return false;
+    const int ks = p.nzt - p.nfs;
+    if (khi >= ks && klo > ks - 2) return false;
+    if (khi < p.nzt && khi >= ks - 2) return false;  // the slab above would not own ks-2 .. nzt
+    return true;
 }
 
 // init_pml (fd3d_deriv.f90:1319-1493): strip boxes and damping profiles, in T.
@@ -51,6 +80,8 @@ void make_pml(const fd3d_params& p, PmlDesc& D, std::vector<Damp<T>>& prof) {
     long long base = 0;
     prof.clear();
     D.ns = p.fspace ? 5 : 4;
+    D.klo = 1;
+    D.khi = p.nzt;
     D.cum[0] = 0;
     std::vector<std::vector<T>> ox(PML_MAXS), oxS(PML_MAXS), oy(PML_MAXS), oyS(PML_MAXS), oz(PML_MAXS), ozS(PML_MAXS);
     for (int s = 0; s < PML_MAXS; ++s) {

@@ -52,7 +52,7 @@ struct VelSlot {
 template <class T, bool LAYERED>
 __device__ __forceinline__ void vel_issue(const VelMaps& M, T* slot, uint32_t bar, int x0, int y0, int k) {
     mbar_expect_tx(bar, (VelSlot::LOADED - (LAYERED ? 256 : 0)) * sizeof(T));
-    const int z = k - 1;
+    const int z = k - 1;  // k counts the stored planes (global plane - kofs)
     tma_load_3d(smem_addr(slot + VelSlot::XX), &M.xx, x0 - 4, y0, z, bar);
     tma_load_3d(smem_addr(slot + VelSlot::XY), &M.xy, x0 - 4, y0 - 2, z, bar);
     tma_load_3d(smem_addr(slot + VelSlot::YY), &M.yy, x0, y0 - 1, z, bar);
@@ -96,15 +96,15 @@ __device__ __forceinline__ bool vel_interior_tma_body(const VelMaps& M, const Gr
     const int i0 = g.nabc + 1 + bx_ * 32, j0 = g.nabc + 1 + by_ * 8;
     const int i = i0 + tx, j = j0 + ty;
     const bool act = (i <= g.nxt - g.nabc) && (j <= g.nyt - 2);
-    const int kb = g.nabc + 1 + bz_ * kchunk;
-    const int ke = min(kb + kchunk - 1, g.ks());
+    const int kb = g.kin_lo() + bz_ * kchunk;
+    const int ke = min(kb + kchunk - 1, g.kin_hi());
     const int x0 = g.off + i0 - 1, y0 = j0 - 1;  // tensor coordinates of the tile origin
     const bool leader = (tx == 0 && ty == 0);
     const unsigned p0 = pc;
     if (leader)
         for (int k = kb; k <= min(ke, kb + TMA_NS - 1); ++k) {
             const unsigned n = p0 + (unsigned)(k - kb);
-            vel_issue<T, LAYERED>(M, ring + (size_t)ring_slot(n) * VelSlot::ELEMS, smem_addr(&bars[ring_slot(n)]), x0, y0, k);
+            vel_issue<T, LAYERED>(M, ring + (size_t)ring_slot(n) * VelSlot::ELEMS, smem_addr(&bars[ring_slot(n)]), x0, y0, k - g.kofs);
         }
     // z queues of the own column (plain loads, one plane ahead)
     const int ic = min(i, g.nxt), jc = min(j, g.nyt);
@@ -152,7 +152,7 @@ __device__ __forceinline__ bool vel_interior_tma_body(const VelMaps& M, const Gr
         __syncthreads();  // every thread is done with slot s
         if (leader && k + TMA_NS <= ke) {
             fence_proxy_async_smem();
-            vel_issue<T, LAYERED>(M, ring + (size_t)s * VelSlot::ELEMS, smem_addr(&bars[s]), x0, y0, k + TMA_NS);
+            vel_issue<T, LAYERED>(M, ring + (size_t)s * VelSlot::ELEMS, smem_addr(&bars[s]), x0, y0, k + TMA_NS - g.kofs);
         }
     }
     pc = p0 + (unsigned)(ke - kb + 1);
@@ -185,7 +185,7 @@ struct StrSlot {
 template <class T, bool LAYERED>
 __device__ __forceinline__ void str_issue(const StrMaps& M, T* slot, uint32_t bar, int x0, int y0, int k) {
     mbar_expect_tx(bar, (StrSlot::LOADED - (LAYERED ? 256 + 288 : 0)) * sizeof(T));
-    const int z = k - 1;
+    const int z = k - 1;  // k counts the stored planes (global plane - kofs)
     tma_load_3d(smem_addr(slot + StrSlot::U), &M.u, x0 - 4, y0 - 2, z, bar);
     tma_load_3d(smem_addr(slot + StrSlot::V), &M.v, x0 - 4, y0 - 2, z, bar);
     tma_load_3d(smem_addr(slot + StrSlot::W), &M.w, x0 - 4, y0 - 2, z, bar);
@@ -207,15 +207,15 @@ __device__ __forceinline__ bool str_interior_tma_body(const StrMaps& M, const Gr
     const int i0 = g.nabc + 1 + bx_ * 32, j0 = g.nabc + 1 + by_ * 8;
     const int i = i0 + tx, j = j0 + ty;
     const bool act = (i <= g.nxt - g.nabc) && (j <= g.nyt - 2);
-    const int kb = g.nabc + 1 + bz_ * kchunk;
-    const int ke = min(kb + kchunk - 1, g.ks());
+    const int kb = g.kin_lo() + bz_ * kchunk;
+    const int ke = min(kb + kchunk - 1, g.kin_hi());
     const int x0 = g.off + i0 - 1, y0 = j0 - 1;
     const bool leader = (tx == 0 && ty == 0);
     const unsigned p0 = pc;
     if (leader)
         for (int k = kb; k <= min(ke, kb + TMA_NS - 1); ++k) {
             const unsigned n = p0 + (unsigned)(k - kb);
-            str_issue<T, LAYERED>(M, ring + (size_t)ring_slot(n) * StrSlot::ELEMS, smem_addr(&bars[ring_slot(n)]), x0, y0, k);
+            str_issue<T, LAYERED>(M, ring + (size_t)ring_slot(n) * StrSlot::ELEMS, smem_addr(&bars[ring_slot(n)]), x0, y0, k - g.kofs);
         }
     const int ic = min(i, g.nxt - 1), jc = min(j, g.nyt - 1);  // keeps the (i+1,j+1) tap in range
     const long long sy = g.px, sz = g.plane;
@@ -276,7 +276,7 @@ __device__ __forceinline__ bool str_interior_tma_body(const StrMaps& M, const Gr
         __syncthreads();
         if (leader && k + TMA_NS <= ke) {
             fence_proxy_async_smem();
-            str_issue<T, LAYERED>(M, ring + (size_t)s * StrSlot::ELEMS, smem_addr(&bars[s]), x0, y0, k + TMA_NS);
+            str_issue<T, LAYERED>(M, ring + (size_t)s * StrSlot::ELEMS, smem_addr(&bars[s]), x0, y0, k + TMA_NS - g.kofs);
         }
     }
     pc = p0 + (unsigned)(ke - kb + 1);

@@ -41,11 +41,17 @@ def device_count() -> int:
 
 
 class Solver:
-    def __init__(self, model: dict, medium3d: bool = False):
+    def __init__(self, model: dict, medium3d: bool = False, slab: tuple[int, int] | None = None):
+        """slab = (k_lo, k_hi): a context for those planes of the model only (a z-slab,
+        stepped by :class:`fd3d_tsn_b200.slab.SlabSolver`)."""
         self.model = model
         self.p = abi.make_params(model)
         self.h = C.c_void_p()
-        _ck(lib().fd3d_ctx_create(C.byref(self.p), C.byref(self.h)), "fd3d_ctx_create")
+        if slab is None:
+            _ck(lib().fd3d_ctx_create(C.byref(self.p), C.byref(self.h)), "fd3d_ctx_create")
+        else:
+            _ck(lib().fd3d_ctx_create_slab(C.byref(self.p), int(slab[0]), int(slab[1]), C.byref(self.h)),
+                "fd3d_ctx_create_slab")
         self.nxT = model["nxt"] - 2 * model["nabc"]
         self.nzT = model["nzt"] - model["nfs"] - model["nabc"]
         self.nf = 5 if model.get("law", "sw") == "fvw" else 4

@@ -257,8 +257,9 @@ int fd3d_ctx_info(fd3d_ctx* ctx, int* interior_variant, int* layered_medium);
  * nsteps steps (each stops at its own ntfd).  Two schedules run the same work items:
  * FD3D_BATCH_PERSISTENT, one cooperative kernel per run whose CTAs walk the items
  * phase by phase between grid barriers, and FD3D_BATCH_GRAPH, CUDA graphs of 32, 16,
- * 8, 4, 2 or 1 steps with one kernel per region and step over all models (the
- * interior, fault-band and PML sweeps of a half-step as parallel branches).
+ * 8, 4, 2 or 1 steps with one kernel per region and step over all models, in series
+ * on one stream (FD3D_BATCH_BRANCHES=1 runs the interior, fault-band and PML sweeps of
+ * a half-step as parallel branches instead).
  * fd3d_batch_autotune picks the schedule and its tile shape.  Models use the FP32
  * build, a 1-D layered medium (one value per k, as readcrustalmodel builds) and keep
  * the last history_capacity records (default 16) of their history planes.  A model's
@@ -292,6 +293,42 @@ int fd3d_batch_get_schedule(fd3d_batch* b, int* mode);
 /* times the tile-shape candidates on the live models (all at step 0), keeps the fastest,
  * resets the models; cache_path/key (optional) persist the choice as JSON lines */
 int fd3d_batch_autotune(fd3d_batch* b, int steps, const char* cache_path, const char* key);
+
+/* ---- one model over several GPUs: z-slabs ------------------------------
+ * No counterpart in the reference, which runs one model in one process on one GPU
+ * (src/dynamicsolver.f90:66; its -DGPUMPI switch is unused).  The model's planes
+ * k = 1..nzt are split into slabs of consecutive planes, one context each (on one
+ * device or several); a slab stores its own planes and three halo planes on either side,
+ * the full fault plane and the full PML split-component pool, and updates only its own
+ * planes and fault rows.  The slabs of one model step together in a group: after the
+ * velocity sweeps, the stress sweeps, the trial traction and the friction law each slab
+ * pulls two halo planes (or fault-plane rows) of what its neighbours just updated.  The
+ * results are the same bits as one context's.  Uploads take the whole model's arrays on
+ * every slab; fd3d_fetch_field, fd3d_fetch_history, fd3d_fetch_stations and
+ * fd3d_fetch_plane return the slab's own planes / rows / stations (the rest untouched in
+ * the host array, or zero), so the slabs of a model fill one result between them.
+ * fd3d_run, fd3d_run_noalloc, fd3d_checkpoint, fd3d_post_process,
+ * fd3d_fetch_moment_rate and fd3d_write_results refuse a slab context (FD3D_ERR_STATE). */
+/* a slab of at least 4 planes; the top slab (k_hi = nzt) owns nzt-nfs-2 .. nzt */
+int fd3d_ctx_create_slab(const fd3d_params* p, int k_lo, int k_hi, fd3d_ctx** out);
+int fd3d_slab_range(fd3d_ctx* ctx, int* k_lo, int* k_hi);
+/* n slabs of about equal cost (host arithmetic only: no device is needed) */
+int fd3d_slab_plan(const fd3d_params* p, int n, int* k_lo, int* k_hi);
+typedef struct fd3d_slab_group fd3d_slab_group;
+/* ctxs: the slabs of one model from the bottom (k_lo = 1) up */
+int fd3d_slab_group_create(fd3d_ctx* const* ctxs, int n, fd3d_slab_group** out);
+int fd3d_slab_group_run(fd3d_slab_group* g, int nsteps);
+/* waits for every slab; *ms = the longest slab's time of the last run */
+int fd3d_slab_group_sync(fd3d_slab_group* g, float* ms);
+int fd3d_slab_group_destroy(fd3d_slab_group* g);   /* the contexts stay */
+/* The slabs in separate processes, one GPU each (torch.distributed ranks): the same
+ * exchange as a group's, as NCCL send/receive pairs with the ranks below and above on the
+ * slab's stream.  Rank r holds the r-th slab from the bottom.  NCCL (libnccl.so.2) is
+ * loaded on first use; FD3D_ERR_NODEV if it cannot be.  fd3d_nccl_unique_id fills the
+ * 128-byte id that rank 0 makes and every rank passes to fd3d_slab_connect. */
+int fd3d_nccl_unique_id(unsigned char* id);
+int fd3d_slab_connect(fd3d_ctx* ctx, const unsigned char* id, int rank, int nranks);
+int fd3d_slab_run(fd3d_ctx* ctx, int nsteps);       /* then fd3d_sync(ctx) */
 
 /* ---- self-test ----------------------------------------------------------
  * No counterpart in the reference.  The PML kernels divide by dh and by 1 + omega

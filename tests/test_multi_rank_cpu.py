@@ -93,3 +93,40 @@ def test_gpus_flag_must_match_the_rank_count():
     r = subprocess.run([sys.executable, "bench.py", "--impl", "reference", "--gpus", "3"], cwd=ROOT, env=env,
                        capture_output=True, text=True, timeout=120)
     assert r.returncode == 2 and "WORLD_SIZE=2" in r.stderr
+
+
+def _slab_rank_main(rank, world, port, out):
+    """The host side of z-slabs in separate processes: every rank gets its own plane
+    range and the id rank 0 made (the NCCL call itself needs GPUs; a fixed id stands
+    in for ncclGetUniqueId here)."""
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    sys.path.insert(0, ROOT)
+    import torch.distributed as dist
+    from fd3d_tsn_b200 import configs
+    from fd3d_tsn_b200.slab import rank_setup
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        m = configs.sw_small()
+        rng, uid = rank_setup(m, rank, world, lambda o: dist.broadcast_object_list(o, src=0),
+                              make_id=lambda: bytes(range(128)))
+        out.put((rank, rng, uid))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_slab_ranks_get_their_planes_and_one_id():
+    world = 3
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_slab_rank_main, args=(r, world, port, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(120)
+    assert all(p.exitcode == 0 for p in procs), [p.exitcode for p in procs]
+    got = sorted(q.get(timeout=5) for _ in range(world))
+    assert all(uid == bytes(range(128)) for _, _, uid in got)
+    ranges = [rng for _, rng, _ in got]
+    assert ranges[0][0] == 1 and ranges[-1][1] == 132          # sw_small: nzt = 132
+    assert all(ranges[r][0] == ranges[r - 1][1] + 1 for r in range(1, world))
