@@ -113,5 +113,34 @@ module fd3d_gpu
       character(kind=c_char), intent(in) :: path(*)
       type(c_ptr) :: ctx
     end function
+    ! one model over several GPUs: z-slabs (one MPI rank per GPU: fd3d_nccl_unique_id on
+    ! rank 0, MPI_Bcast of the 128 bytes, fd3d_slab_connect and fd3d_slab_run on every rank)
+    integer(c_int) function fd3d_slab_plan(p, n, k_lo, k_hi) bind(C)
+      import
+      type(fd3d_params), intent(in) :: p
+      integer(c_int), value :: n
+      integer(c_int) :: k_lo(*), k_hi(*)
+    end function
+    integer(c_int) function fd3d_ctx_create_slab(p, k_lo, k_hi, ctx) bind(C)
+      import
+      type(fd3d_params), intent(in) :: p
+      integer(c_int), value :: k_lo, k_hi
+      type(c_ptr) :: ctx
+    end function
+    integer(c_int) function fd3d_nccl_unique_id(id) bind(C)
+      import
+      character(kind=c_char) :: id(128)
+    end function
+    integer(c_int) function fd3d_slab_connect(ctx, id, rank, nranks) bind(C)
+      import
+      type(c_ptr), value :: ctx
+      character(kind=c_char), intent(in) :: id(128)
+      integer(c_int), value :: rank, nranks
+    end function
+    integer(c_int) function fd3d_slab_run(ctx, nsteps) bind(C)
+      import
+      type(c_ptr), value :: ctx
+      integer(c_int), value :: nsteps
+    end function
   end interface
 end module fd3d_gpu
