@@ -103,6 +103,12 @@ __global__ void k_repack(Grid g, const S* __restrict__ src, T* __restrict__ dst)
     }
 }
 
+// n copies of v (the reset values of the fault planes)
+template <class U>
+__global__ void k_fill(U* a, size_t n, U v) {
+    for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x) a[q] = v;
+}
+
 // interp_fric (fd3d_deriv.f90:3174-3189): X-node values are 4-point averages
 template <class T>
 __global__ void k_interp_fric(Grid g, Fault<T> q) {
@@ -629,12 +635,13 @@ struct Ctx : CtxBase {
         double* zd[] = {q.distZ, q.slipX, q.slipZ, q.rise};
         for (double* a : zd) CK(cudaMemsetAsync(a, 0, n2 * sizeof(double), st));
         CK(cudaMemsetAsync(q.distX, 0, 2 * n2 * sizeof(double), st));
-        std::vector<double> big(n2, 1.e4);
-        CK(cudaMemcpyAsync(q.ruptime, big.data(), n2 * sizeof(double), cudaMemcpyHostToDevice, st));
-        CK(cudaMemcpyAsync(q.sliptime, big.data(), n2 * sizeof(double), cudaMemcpyHostToDevice, st));
-        std::vector<T> t0(n2, law == FD3D_LAW_FVW ? (T)1 : (T)0);
-        CK(cudaMemcpyAsync(q.tabsX, t0.data(), n2 * sizeof(T), cudaMemcpyHostToDevice, st));
-        CK(cudaMemcpyAsync(q.tabsZ, t0.data(), n2 * sizeof(T), cudaMemcpyHostToDevice, st));
+        const unsigned fb = (unsigned)std::min<size_t>(1184, (n2 + 255) / 256);
+        k_fill<double><<<fb, 256, 0, st>>>(q.ruptime, n2, 1.e4);
+        k_fill<double><<<fb, 256, 0, st>>>(q.sliptime, n2, 1.e4);
+        const T t0 = law == FD3D_LAW_FVW ? (T)1 : (T)0;
+        k_fill<T><<<fb, 256, 0, st>>>(q.tabsX, n2, t0);
+        k_fill<T><<<fb, 256, 0, st>>>(q.tabsZ, n2, t0);
+        CK(cudaGetLastError());
         // initial state variable and prestress (the nucleation ramp rewrites T0X)
         CK(cudaMemcpyAsync(q.T0X, q.T0Xb, n2 * sizeof(T), cudaMemcpyDeviceToDevice, st));
         if (law == FD3D_LAW_FVW) {
