@@ -291,6 +291,7 @@ struct Ctx : CtxBase {
 
     int alloc() override {
         CK(cudaGetDevice(&device));
+        CK(cudaDeviceGetAttribute(&icfg.nsm, cudaDevAttrMultiProcessorCount, device));
         CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
         if (const char* e = std::getenv("FD3D_OVERLAP")) overlap = std::atoi(e);
         CK(cudaStreamCreateWithFlags(&st2, cudaStreamNonBlocking));
@@ -937,8 +938,14 @@ static int create_ctx(const fd3d_params* p, int slab_lo, int slab_hi, fd3d_ctx**
         else if (!std::strcmp(e, "pipe")) c->icfg.variant = IV_PIPE;
         else if (!std::strcmp(e, "tma")) c->icfg.variant = IV_TMA;
     }
-    if (const char* e = std::getenv("FD3D_KCHUNK")) c->icfg.kchunk = c->icfg.kchunk_str = std::max(1, std::atoi(e));
-    if (const char* e = std::getenv("FD3D_KCHUNK_STR")) c->icfg.kchunk_str = std::max(1, std::atoi(e));
+    if (const char* e = std::getenv("FD3D_KCHUNK")) {
+        c->icfg.kchunk = c->icfg.kchunk_str = std::max(1, std::atoi(e));
+        c->icfg.kchunk_auto = false;
+    }
+    if (const char* e = std::getenv("FD3D_KCHUNK_STR")) {
+        c->icfg.kchunk_str = std::max(1, std::atoi(e));
+        c->icfg.kchunk_auto = false;
+    }
     if (const char* e = std::getenv("FD3D_BY")) c->icfg.by = std::min(32, std::max(1, std::atoi(e)));
     // FD3D_PML_MINB=<v>[,<s>]: CTAs per SM the velocity / stress PML sweeps are compiled for
     if (const char* e = std::getenv("FD3D_PML_MINB")) {

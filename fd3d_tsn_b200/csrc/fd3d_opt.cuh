@@ -322,16 +322,28 @@ struct InteriorCfg {
     int kchunk = 32;      // z-planes per CTA of the velocity sweep
     int kchunk_str = 32;  // z-planes per CTA of the stress sweep
     int by = 8;          // CTA rows (IV_POINT: block = 32 x by)
+    // a grid too small to give every SM two CTAs at kchunk planes each gets fewer planes
+    // per CTA (halved down to 4); off when FD3D_KCHUNK sets the depth
+    bool kchunk_auto = true;
+    int nsm = 148;        // SMs of the context's device
 };
 
 inline int interior_nz(const Grid& g) { return std::max(0, g.kin_hi() - g.kin_lo() + 1); }  // planes updated
+
+// planes per CTA of an interior sweep of columns x nzT planes
+inline int interior_kchunk(const InteriorCfg& cfg, int k, long long columns, int nzT) {
+    k = std::max(1, std::min(k, nzT));
+    if (cfg.kchunk_auto)
+        while (k > 4 && columns * ((nzT + k - 1) / k) < 2LL * cfg.nsm) k = (k + 1) / 2;
+    return k;
+}
 
 template <class T>
 void launch_vel_interior(const InteriorCfg& cfg, const Grid& g, const Fields<T>& f, const StepConst<T>& c,
                          cudaStream_t st) {
     const int nxT = g.nxt - 2 * g.nabc, nyI = g.nyt - 2 - g.nabc, nzT = interior_nz(g);
     if (nzT <= 0) return;  // a z-slab without interior planes
-    const int kch = std::max(1, std::min(cfg.kchunk, nzT));
+    const int kch = interior_kchunk(cfg, cfg.kchunk, (long long)((nxT + 31) / 32) * ((nyI + 7) / 8), nzT);
     if (cfg.variant == IV_POINT) {
         const int by = cfg.by;
         dim3 grid((nxT + 31) / 32, (nyI + by - 1) / by, (nzT + kch - 1) / kch);
@@ -348,7 +360,7 @@ void launch_str_interior(const InteriorCfg& cfg, const Grid& g, const Fields<T>&
                          cudaStream_t st) {
     const int nxT = g.nxt - 2 * g.nabc, nyI = g.nyt - 2 - g.nabc, nzT = interior_nz(g);
     if (nzT <= 0) return;  // a z-slab without interior planes
-    const int kch = std::max(1, std::min(cfg.kchunk_str, nzT));
+    const int kch = interior_kchunk(cfg, cfg.kchunk_str, (long long)((nxT + 31) / 32) * ((nyI + 7) / 8), nzT);
     if (cfg.variant == IV_POINT) {
         const int by = cfg.by;
         dim3 grid((nxT + 31) / 32, (nyI + by - 1) / by, (nzT + kch - 1) / kch);
@@ -444,7 +456,7 @@ void launch_vel_interior_tma(const VelMaps& M, const InteriorCfg& cfg, const Gri
                              const StepConst<T>& c, int* status, cudaStream_t st) {
     const int nxT = g.nxt - 2 * g.nabc, nyI = g.nyt - 2 - g.nabc, nzT = interior_nz(g);
     if (nzT <= 0) return;  // a z-slab without interior planes
-    const int kch = std::max(1, std::min(cfg.kchunk, nzT));
+    const int kch = interior_kchunk(cfg, cfg.kchunk, (long long)((nxT + 31) / 32) * ((nyI + 7) / 8), nzT);
     dim3 grid((nxT + 31) / 32, (nyI + 7) / 8, (nzT + kch - 1) / kch);
     const size_t sm = TMA_NS * VelSlot::ELEMS * sizeof(T) + TMA_SMEM_PAD;
     if (f.lay) k_vel_interior_tma<T, true><<<grid, dim3(32, 8), sm, st>>>(M, g, f, c, kch, status);
@@ -456,7 +468,7 @@ void launch_str_interior_tma(const StrMaps& M, const InteriorCfg& cfg, const Gri
                              const StepConst<T>& c, int* status, cudaStream_t st) {
     const int nxT = g.nxt - 2 * g.nabc, nyI = g.nyt - 2 - g.nabc, nzT = interior_nz(g);
     if (nzT <= 0) return;  // a z-slab without interior planes
-    const int kch = std::max(1, std::min(cfg.kchunk_str, nzT));
+    const int kch = interior_kchunk(cfg, cfg.kchunk_str, (long long)((nxT + 31) / 32) * ((nyI + 7) / 8), nzT);
     dim3 grid((nxT + 31) / 32, (nyI + 7) / 8, (nzT + kch - 1) / kch);
     const size_t sm = TMA_NS * StrSlot::ELEMS * sizeof(T) + TMA_SMEM_PAD;
     if (f.lay) k_str_interior_tma<T, true><<<grid, dim3(32, 8), sm, st>>>(M, g, f, c, kch, status);
