@@ -161,6 +161,7 @@ def load_library(path: str | None = None) -> C.CDLL:
         "fd3d_ctx_create_slab": (i, [C.POINTER(Params), i, i, C.POINTER(vp)]),
         "fd3d_slab_range": (i, [vp, C.POINTER(i), C.POINTER(i)]),
         "fd3d_slab_plan": (i, [C.POINTER(Params), i, C.POINTER(i), C.POINTER(i)]),
+        "fd3d_slab_halo_plan": (i, [i, i, i, C.POINTER(i), C.POINTER(i)]),
         "fd3d_slab_group_create": (i, [C.POINTER(vp), i, C.POINTER(vp)]),
         "fd3d_slab_group_run": (i, [vp, i]),
         "fd3d_slab_group_sync": (i, [vp, fp]),

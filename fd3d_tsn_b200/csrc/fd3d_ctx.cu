@@ -1279,6 +1279,17 @@ int fd3d_write_results(fd3d_ctx* ctx, const char* dir, int rk) {
 // never what was just pulled from it until the next exchange of the same set, which in
 // turn waits for this slab, so no slab overwrites data another is still copying.
 
+// The two planes (or fault-plane rows) a slab owning k_lo..k_hi exchanges with its
+// neighbour below (side 0) or above (side 1): it sends its own first / last two and receives
+// the neighbour's into its halo.  Both transports use it; a slab's receive on one side is
+// its neighbour's send on the other.
+int fd3d_slab_halo_plan(int k_lo, int k_hi, int side, int* send_k0, int* recv_k0) {
+    if (!send_k0 || !recv_k0 || (side != 0 && side != 1) || k_hi - k_lo + 1 < SLAB_MIN) return FD3D_ERR_ARG;
+    *send_k0 = side == 0 ? k_lo : k_hi - 1;
+    *recv_k0 = side == 0 ? k_lo - 2 : k_hi + 1;
+    return FD3D_OK;
+}
+
 // Planes 1..nzt in n slabs of about equal cost (a PML cell moves about 2.2 times the
 // bytes of an interior cell), every slab valid for slab_range_ok.
 int fd3d_slab_plan(const fd3d_params* p, int n, int* k_lo, int* k_hi) {
@@ -1386,7 +1397,9 @@ static int slab_exchange(fd3d_slab_group* G, int set) {
             const int nb = side == 0 ? i - 1 : i + 1;
             if (nb < 0 || nb >= n) continue;
             CK(cudaStreamWaitEvent(c->st, G->ev[nb], 0));
-            const long long k0 = side == 0 ? c->g.klo - 2 : c->g.khi + 1;  // first halo plane / row
+            int send_k0 = 0, recv_k0 = 0;  // pull into the halo: the neighbour's send planes
+            fd3d_slab_halo_plan(c->g.klo, c->g.khi, side, &send_k0, &recv_k0);
+            const long long k0 = recv_k0;
             for (size_t a = 0; a < arr[i].size(); ++a) {
                 const HaloArray &d = arr[i][a], &s = arr[nb][a];
                 const size_t off = d.unit * (size_t)(k0 - 1) * d.elem, bytes = 2 * d.unit * d.elem;
@@ -1500,8 +1513,8 @@ static int nccl_exchange(CtxBase* c, int set) {
     for (int side = 0; side < 2; ++side) {
         const int nb = side == 0 ? c->slab_rank - 1 : c->slab_rank + 1;
         if (nb < 0 || nb >= c->slab_nranks) continue;
-        const long long send_k0 = side == 0 ? c->g.klo : c->g.khi - 1;
-        const long long recv_k0 = side == 0 ? c->g.klo - 2 : c->g.khi + 1;
+        int send_k0 = 0, recv_k0 = 0;
+        fd3d_slab_halo_plan(c->g.klo, c->g.khi, side, &send_k0, &recv_k0);
         for (const HaloArray& a : arr) {
             const size_t bytes = 2 * a.unit * a.elem;
             ok &= n.Send((const char*)a.base + a.unit * (size_t)(send_k0 - 1) * a.elem, bytes, ncclChar, nb, c->comm,

@@ -314,6 +314,9 @@ int fd3d_ctx_create_slab(const fd3d_params* p, int k_lo, int k_hi, fd3d_ctx** ou
 int fd3d_slab_range(fd3d_ctx* ctx, int* k_lo, int* k_hi);
 /* n slabs of about equal cost (host arithmetic only: no device is needed) */
 int fd3d_slab_plan(const fd3d_params* p, int n, int* k_lo, int* k_hi);
+/* the first of the two planes / fault rows a slab owning k_lo..k_hi sends to, and receives
+ * from, its neighbour below (side 0) or above (side 1); host arithmetic only */
+int fd3d_slab_halo_plan(int k_lo, int k_hi, int side, int* send_k0, int* recv_k0);
 typedef struct fd3d_slab_group fd3d_slab_group;
 /* ctxs: the slabs of one model from the bottom (k_lo = 1) up */
 int fd3d_slab_group_create(fd3d_ctx* const* ctxs, int n, fd3d_slab_group** out);

@@ -62,3 +62,27 @@ def test_invalid_slab_ranges_refused_before_any_device(rng):
     h = C.c_void_p()
     assert lib().fd3d_ctx_create_slab(C.byref(p), rng[0], rng[1], C.byref(h)) == -1  # FD3D_ERR_ARG
     assert not h.value
+
+
+def _halo(k_lo, k_hi, side):
+    s, r = C.c_int(), C.c_int()
+    assert lib().fd3d_slab_halo_plan(k_lo, k_hi, side, C.byref(s), C.byref(r)) == 0
+    return s.value, r.value
+
+
+@pytest.mark.parametrize("name,n", [("tiny_sw", 4), ("sw_small", 8), ("sw_large", 8), ("fvw_medium", 3)])
+def test_halo_plan_pairs_every_receive_with_the_neighbours_send(name, n):
+    """Both transports (the in-process pull and the NCCL send/receive pairs) take their
+    planes from fd3d_slab_halo_plan: what a slab receives on one side is exactly what its
+    neighbour sends on the other, two of the neighbour's own planes, landing in the
+    receiver's halo (stored, not owned)."""
+    m = getattr(configs, name)()
+    ranges = plan(m, n)
+    for (a_lo, a_hi), (b_lo, b_hi) in zip(ranges, ranges[1:]):
+        a_send_up, a_recv_up = _halo(a_lo, a_hi, 1)
+        b_send_dn, b_recv_dn = _halo(b_lo, b_hi, 0)
+        assert a_recv_up == b_send_dn and b_recv_dn == a_send_up
+        for k in (b_send_dn, b_send_dn + 1):
+            assert b_lo <= k <= b_hi and a_hi < k <= a_hi + 3      # B's own, A's halo
+        for k in (a_send_up, a_send_up + 1):
+            assert a_lo <= k <= a_hi and b_lo - 3 <= k < b_lo      # A's own, B's halo
