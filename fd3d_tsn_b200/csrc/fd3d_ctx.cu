@@ -42,20 +42,20 @@ namespace fd3d {
 // goes to tab (lam, mu, d and dth/d, nzt values each).
 template <class T>
 __global__ void k_layer_check(Grid g, const T* lam, const T* mu, const T* d, T dth, T dt, T* tab, int* nonuniform) {
-    const long long n = (long long)g.nxt * g.nyt * g.nzl;  // the stored planes, from kofs+1
+    const int nrows = g.nyt * g.nzl;  // rows (j,k) of the stored planes, from kofs+1; a CTA per row
     int bad = 0;
-    for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
-        const int i = 1 + (int)(q % g.nxt);
-        const long long r = q / g.nxt;
-        const int j = 1 + (int)(r % g.nyt), k = g.kofs + 1 + (int)(r / g.nyt);
-        const long long p = g.at(i, j, k), p0 = g.at(1, 1, k);
-        bad |= (lam[p] != lam[p0]) | (mu[p] != mu[p0]) | (d[p] != d[p0]);
-        if (i == 1 && j == 1) {
-            tab[k - 1] = lam[p0];
-            tab[g.nzt + k - 1] = mu[p0];
-            tab[2 * g.nzt + k - 1] = d[p0];
-            tab[3 * g.nzt + k - 1] = dth / d[p0];
-            tab[4 * g.nzt + k - 1] = dt / d[p0];
+    for (int r = blockIdx.x; r < nrows; r += gridDim.x) {
+        const int j = 1 + r % g.nyt, k = g.kofs + 1 + r / g.nyt;
+        const long long p0 = g.at(1, 1, k), row = g.at(1, j, k);
+        const T l0 = lam[p0], m0 = mu[p0], d0 = d[p0];
+        for (int i = threadIdx.x; i < g.nxt; i += blockDim.x)
+            bad |= (lam[row + i] != l0) | (mu[row + i] != m0) | (d[row + i] != d0);
+        if (j == 1 && threadIdx.x == 0) {
+            tab[k - 1] = l0;
+            tab[g.nzt + k - 1] = m0;
+            tab[2 * g.nzt + k - 1] = d0;
+            tab[3 * g.nzt + k - 1] = dth / d0;
+            tab[4 * g.nzt + k - 1] = dt / d0;
         }
     }
     if (__syncthreads_or(bad) && threadIdx.x == 0) atomicOr(nonuniform, 1);
@@ -94,12 +94,12 @@ __global__ void k_model_to_fd3d(Grid g, int nli, const T* T0I, const T* TsI, con
 // layout (element type converted when the host's real kind differs from the field type)
 template <class T, class S>
 __global__ void k_repack(Grid g, const S* __restrict__ src, T* __restrict__ dst) {
-    const long long n = (long long)g.nxt * g.nyt * g.nzl;  // the stored planes, from kofs+1
-    for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
-        const int i = 1 + (int)(q % g.nxt);
-        const long long r = q / g.nxt;
-        const int j = 1 + (int)(r % g.nyt), k = g.kofs + 1 + (int)(r / g.nyt);
-        dst[g.at(i, j, k)] = (T)src[q];
+    const int nrows = g.nyt * g.nzl;  // rows (j,k) of the stored planes, from kofs+1; a CTA per row
+    for (int r = blockIdx.x; r < nrows; r += gridDim.x) {
+        const int j = 1 + r % g.nyt, k = g.kofs + 1 + r / g.nyt;
+        const S* s = src + (long long)r * g.nxt;
+        T* o = dst + g.at(1, j, k);
+        for (int i = threadIdx.x; i < g.nxt; i += blockDim.x) o[i] = (T)s[i];
     }
 }
 
