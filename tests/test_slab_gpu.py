@@ -83,6 +83,28 @@ def test_slabs_match_one_context_3d_medium_fp64():
     compare(m, 60, nslabs=2, medium3d=True)
 
 
+def test_slabs_history_stride_and_wrapping_ring():
+    """Records every 3 steps into a ring of 8 records, read back in chunks as the run goes:
+    the merged records are the same bits as one context's."""
+    m = configs.tiny_sw(seed=77, nsteps=96, stride=3)
+    m["history_capacity"] = 8
+    ref = Solver(m)
+    sl = SlabSolver(m, nslabs=3)
+    for c in range(4):
+        ref.run(24)
+        sl.run(24)
+        ref.sync()
+        sl.sync()
+        rec0 = 8 * c        # 24 steps = 8 records per chunk, all still in the ring
+        for f in range(ref.nf):
+            np.testing.assert_array_equal(sl.history(f, rec0=rec0, nrec=8), ref.history(f, rec0=rec0, nrec=8),
+                                          err_msg=f"chunk {c} field {f}")
+        np.testing.assert_array_equal(sl.stations(rec0=rec0, nrec=8), ref.stations(rec0=rec0, nrec=8))
+    assert sl.history_records() == ref.history_records() == 32
+    ref.close()
+    sl.close()
+
+
 def test_slab_context_refuses_whole_model_calls():
     m = configs.tiny_sw(seed=76, nsteps=10)
     (a, b), _ = plan(m, 2)
