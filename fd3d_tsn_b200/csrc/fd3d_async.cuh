@@ -48,4 +48,11 @@ __device__ __forceinline__ void bulk_load(uint32_t dst, const void* src, uint32_
 }
 __device__ __forceinline__ void fence_proxy_async_global() { asm volatile("fence.proxy.async.global;" ::: "memory"); }
 
+// Programmatic dependent launch: a grid launched with programmatic stream serialization
+// waits here until the grid before it has completed and its memory is visible (a no-op
+// for a grid launched without it); once every CTA of a grid has passed
+// pdl_launch_dependents, the next grid's CTAs may be scheduled and wait in pdl_wait.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_launch_dependents() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
 }  // namespace fd3d

@@ -234,6 +234,8 @@ __global__ void __launch_bounds__(256) k_bint(const ModelDev* __restrict__ model
     extern __shared__ __align__(128) unsigned char smem_raw[];
     float* ring = reinterpret_cast<float*>(smem_raw + ((128u - (smem_addr(smem_raw) & 127u)) & 127u));
     __shared__ __align__(8) uint64_t bars[TMA_NS];
+    pdl_wait();
+    pdl_launch_dependents();
     const Work it = work[b0 + blockIdx.x];
     int m;
     if (!item_live(it, limit, run_step, m)) return;
@@ -255,6 +257,8 @@ __global__ void __launch_bounds__(PML_TILE, STRESS ? 3 : 4) k_bpml(const ModelDe
                                                       int* gstatus) {
     __shared__ __align__(128) float sm[PML_TILE * (STRESS ? AUX_NS : AUX_NV)];
     __shared__ __align__(8) uint64_t bar;
+    pdl_wait();
+    pdl_launch_dependents();
     const Work it = work[b0 + blockIdx.x];
     int m;
     if (!item_live(it, limit, run_step, m)) return;
@@ -272,6 +276,8 @@ template <int KIND>
 __global__ void __launch_bounds__(256) k_bplane(const ModelDev* __restrict__ models, const Work* __restrict__ work,
                                                 int b0, const int* __restrict__ limit, const int* run_step) {
     __shared__ float sm[KIND == 1 ? FBC_SMEM : 1];
+    pdl_wait();
+    pdl_launch_dependents();
     const Work it = work[b0 + blockIdx.x];
     int m;
     if (!item_live(it, limit, run_step, m)) return;
@@ -297,7 +303,30 @@ __global__ void __launch_bounds__(256) k_bplane(const ModelDev* __restrict__ mod
     }
 }
 
-__global__ void k_step_end(int* run_step) { *run_step += 1; }
+__global__ void k_step_end(int* run_step) {
+    pdl_wait();
+    pdl_launch_dependents();
+    *run_step += 1;
+}
+
+// A launch of the graph schedule, with programmatic stream serialization when pdl is set:
+// the kernel's CTAs may be scheduled while the kernel before it drains, and wait in
+// pdl_wait (every kernel of the schedule starts with it) for its completion.
+template <class... K, class... A>
+static cudaError_t launch_g(bool pdl, void (*kern)(K...), unsigned grid, dim3 blk, size_t smem, cudaStream_t s,
+                            A... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = blk;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = pdl ? 1 : 0;
+    return cudaLaunchKernelEx(&cfg, kern, args...);
+}
 
 // OR of the live models' device status words into out (one read-back per sync)
 __global__ void k_or_status(int* const* __restrict__ st, int n, int* out) {
@@ -472,6 +501,8 @@ struct fd3d_batch {
     static constexpr int NGRAPH = 6;
     cudaGraphExec_t gx[NGRAPH] = {};
     int graph_kchunk = -1;
+    int pdl = 0;                 // graph schedule: programmatic dependent launch between its kernels
+                                 // (measured 2.3-2.5% slower: the early CTAs hold SM slots in the tail)
     int branches = 0;            // graph schedule: fault-band and PML sweeps on side streams (1) or in
                                  // series on the main stream (0, measured 9-11% faster: the branches interfered)
     int** d_stptr = nullptr;     // status words of the live models (k_or_status)
@@ -625,14 +656,20 @@ int build_work(fd3d_batch* b) {
 int enqueue_graph_step(fd3d_batch* b) {
     const dim3 blk(32, 8);
     const int kc = b->tun.kchunk;
+    const bool pdl = b->pdl && !b->branches;  // on the one stream only
+    cudaError_t err = cudaSuccess;             // the first failed launch
+    auto chk = [&](cudaError_t e) { if (err == cudaSuccess) err = e; };
     auto n_of = [&](int t) { return b->tbeg[t + 1] - b->tbeg[t]; };
     auto plane = [&](cudaStream_t s, int t0, int t1) {  // item types [t0, t1) in one launch
         const int n = b->tbeg[t1] - b->tbeg[t0];
         if (n == 0) return;
         const int* lim = b->d_limit;
-        if (t0 <= W_FBC && W_FBC < t1) k_bplane<1><<<n, blk, 0, s>>>(b->d_models, b->d_work_t, b->tbeg[t0], lim, b->d_run_step);
-        else if (t0 == W_VEL_FAULT) k_bplane<2><<<n, blk, 0, s>>>(b->d_models, b->d_work_t, b->tbeg[t0], lim, b->d_run_step);
-        else k_bplane<0><<<n, blk, 0, s>>>(b->d_models, b->d_work_t, b->tbeg[t0], lim, b->d_run_step);
+        const int* rs = b->d_run_step;
+        const ModelDev* md = b->d_models;
+        const Work* wt = b->d_work_t;
+        if (t0 <= W_FBC && W_FBC < t1) chk(launch_g(pdl, k_bplane<1>, n, blk, 0, s, md, wt, b->tbeg[t0], lim, rs));
+        else if (t0 == W_VEL_FAULT) chk(launch_g(pdl, k_bplane<2>, n, blk, 0, s, md, wt, b->tbeg[t0], lim, rs));
+        else chk(launch_g(pdl, k_bplane<0>, n, blk, 0, s, md, wt, b->tbeg[t0], lim, rs));
     };
     // the fault-band and PML sweeps on side streams beside the interior sweep, or (branches
     // off) all on the main stream one after another
@@ -645,22 +682,20 @@ int enqueue_graph_step(fd3d_batch* b) {
             BCK(cudaStreamWaitEvent(b->side[0], b->evf[0], 0));
             BCK(cudaStreamWaitEvent(b->side[1], b->evf[0], 0));
         }
+        const ModelDev* md = b->d_models;
+        const ModelMaps* mp = b->d_maps;
+        const Work* wt = b->d_work_t;
+        const int* lim = b->d_limit;
+        const int* rs = b->d_run_step;
         if (n_of(ti) > 0) {
-            if (half)
-                k_bint<true><<<n_of(ti), blk, tma_ring_bytes<float>(), b->st>>>(
-                    b->d_models, b->d_maps, b->d_work_t, b->tbeg[ti], b->d_limit, b->d_run_step, kc, b->d_status);
-            else
-                k_bint<false><<<n_of(ti), blk, tma_ring_bytes<float>(), b->st>>>(
-                    b->d_models, b->d_maps, b->d_work_t, b->tbeg[ti], b->d_limit, b->d_run_step, kc, b->d_status);
+            const size_t sm = tma_ring_bytes<float>();
+            if (half) chk(launch_g(pdl, k_bint<true>, n_of(ti), blk, sm, b->st, md, mp, wt, b->tbeg[ti], lim, rs, kc, b->d_status));
+            else chk(launch_g(pdl, k_bint<false>, n_of(ti), blk, sm, b->st, md, mp, wt, b->tbeg[ti], lim, rs, kc, b->d_status));
         }
         plane(s0, tf, tf + 1);
         if (n_of(tp) > 0) {
-            if (half)
-                k_bpml<true><<<n_of(tp), blk, 0, s1>>>(b->d_models, b->d_work_t, b->tbeg[tp], b->d_limit,
-                                                       b->d_run_step, b->d_status);
-            else
-                k_bpml<false><<<n_of(tp), blk, 0, s1>>>(b->d_models, b->d_work_t, b->tbeg[tp], b->d_limit,
-                                                        b->d_run_step, b->d_status);
+            if (half) chk(launch_g(pdl, k_bpml<true>, n_of(tp), blk, 0, s1, md, wt, b->tbeg[tp], lim, rs, b->d_status));
+            else chk(launch_g(pdl, k_bpml<false>, n_of(tp), blk, 0, s1, md, wt, b->tbeg[tp], lim, rs, b->d_status));
         }
         if (b->branches) {
             BCK(cudaEventRecord(b->evf[1], b->side[0]));
@@ -671,7 +706,8 @@ int enqueue_graph_step(fd3d_batch* b) {
         plane(b->st, tfs, half ? W_FBC + 1 : tfs + 1);  // after the stresses: fres and the fault BC tiles
     }
     plane(b->st, W_NUC, W_NUC + 1);
-    k_step_end<<<1, 1, 0, b->st>>>(b->d_run_step);
+    chk(launch_g(pdl, k_step_end, 1, dim3(1), 0, b->st, b->d_run_step));
+    BCK(err);
     BCK(cudaGetLastError());
     return FD3D_OK;
 }
@@ -873,6 +909,8 @@ int fd3d_batch_create(size_t arena_bytes, int max_models, fd3d_batch** out) {
     if (const char* e = std::getenv("FD3D_BATCH_PER_SM")) b->tun.per_sm = std::max(0, std::atoi(e));
     // FD3D_BATCH_BRANCHES=1: the graph schedule runs the fault-band and PML sweeps on side streams
     if (const char* e = std::getenv("FD3D_BATCH_BRANCHES")) b->branches = std::atoi(e) != 0;
+    // FD3D_BATCH_PDL=1: the graph schedule's kernels with programmatic dependent launch
+    if (const char* e = std::getenv("FD3D_BATCH_PDL")) b->pdl = std::atoi(e) != 0;
     // FD3D_BATCH_MODE=persistent|graph
     if (const char* e = std::getenv("FD3D_BATCH_MODE"))
         b->tun.mode = std::strcmp(e, "persistent") == 0 ? MODE_PERSISTENT : MODE_GRAPH;
