@@ -339,3 +339,29 @@ def test_medium_upload_paths_agree():
     o.set_medium_arrays(*(a.astype(np.float64) for a in arrs))
     oh, _ = o.step(30)
     np.testing.assert_array_equal(runs[0][0], oh[:, 0])
+
+
+@pytest.mark.parametrize("case", ["tiny_sw_f32", "tiny_sw_f64", "tiny_sw_fspace_f32"])
+def test_gpu_matches_golden_fixture(case):
+    """The CUDA path against the committed fixture (digests of the oracle's outputs on seeded
+    small models, tests/golden/make_golden.py): histories, stations, wave fields and fault
+    planes bit for bit, with no oracle run on the GPU box."""
+    import json
+    import sys
+    here = os.path.dirname(os.path.abspath(__file__))
+    sys.path.insert(0, os.path.join(here, "golden"))
+    import make_golden as mg
+    with open(os.path.join(here, "golden", "oracle_tiny.json")) as f:
+        g = json.load(f)
+    m, _ = mg.cases()[case]
+    steps = g["steps"]
+    m["history_capacity"] = steps
+    s = Solver(m)
+    s.run(steps)
+    s.sync()
+    hist = np.stack([s.history(f) for f in range(4)], axis=1)
+    got = mg.outputs_digests(hist, s.stations(), s.field, s.plane)
+    s.close()
+    want = g["cases"][case]
+    for k, v in got.items():
+        assert v == want[k], k
