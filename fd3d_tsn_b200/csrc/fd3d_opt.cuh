@@ -441,12 +441,12 @@ bool make_interior_maps(const Grid& g, const Fields<T>& f, VelMaps& V, StrMaps& 
 
 template <class T>
 bool prepare_tma_kernels() {
-    const int vs = TMA_NS * VelSlot::ELEMS * (int)sizeof(T) + TMA_SMEM_PAD,
-              ss = TMA_NS * StrSlot::ELEMS * (int)sizeof(T) + TMA_SMEM_PAD;
+    const int vs = TMA_NS * VelSlot::ELEMS * (int)sizeof(T) + TMA_SMEM_PAD, ss = str_ring_bytes<T, false>(),
+              ssl = str_ring_bytes<T, true>();
     bool ok = cudaFuncSetAttribute(k_vel_interior_tma<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, vs) == cudaSuccess;
     ok &= cudaFuncSetAttribute(k_str_interior_tma<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, ss) == cudaSuccess;
     ok &= cudaFuncSetAttribute(k_vel_interior_tma<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, vs) == cudaSuccess;
-    ok &= cudaFuncSetAttribute(k_str_interior_tma<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, ss) == cudaSuccess;
+    ok &= cudaFuncSetAttribute(k_str_interior_tma<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, ssl) == cudaSuccess;
     if (!ok) cudaGetLastError();
     return ok;
 }
@@ -470,9 +470,8 @@ void launch_str_interior_tma(const StrMaps& M, const InteriorCfg& cfg, const Gri
     if (nzT <= 0) return;  // a z-slab without interior planes
     const int kch = interior_kchunk(cfg, cfg.kchunk_str, (long long)((nxT + 31) / 32) * ((nyI + 7) / 8), nzT);
     dim3 grid((nxT + 31) / 32, (nyI + 7) / 8, (nzT + kch - 1) / kch);
-    const size_t sm = TMA_NS * StrSlot::ELEMS * sizeof(T) + TMA_SMEM_PAD;
-    if (f.lay) k_str_interior_tma<T, true><<<grid, dim3(32, 8), sm, st>>>(M, g, f, c, kch, status);
-    else k_str_interior_tma<T, false><<<grid, dim3(32, 8), sm, st>>>(M, g, f, c, kch, status);
+    if (f.lay) k_str_interior_tma<T, true><<<grid, dim3(32, 8), str_ring_bytes<T, true>(), st>>>(M, g, f, c, kch, status);
+    else k_str_interior_tma<T, false><<<grid, dim3(32, 8), str_ring_bytes<T, false>(), st>>>(M, g, f, c, kch, status);
 }
 
 }  // namespace fd3d

@@ -182,9 +182,26 @@ struct StrSlot {
     static constexpr int LOADED = 3520;
 };
 
+// The 1-D-medium stress sweep loads no lam / mu windows: its slot packs the six stress
+// tiles right after u, v, w (2976 elements), so the ring takes 36 KB instead of 42 KB in FP32.
+struct StrSlotLayered {
+    static constexpr int U = 0, V = 480, W = 960, XX = 1440, YY = 1696, ZZ = 1952, XY = 2208, XZ = 2464,
+                         YZ = 2720;
+    static constexpr int LAM = 0, MU = 0;  // not loaded (the medium comes from the per-plane profile)
+    static constexpr int ELEMS = 2976;
+    static constexpr int LOADED = 2976;
+};
+template <bool LAYERED> struct StrSlotOf { using type = StrSlot; };
+template <> struct StrSlotOf<true> { using type = StrSlotLayered; };
+
+// dynamic shared memory of the stress sweep's ring
+template <class T, bool LAYERED>
+constexpr int str_ring_bytes() { return TMA_NS * StrSlotOf<LAYERED>::type::ELEMS * (int)sizeof(T) + TMA_SMEM_PAD; }
+
 template <class T, bool LAYERED>
 __device__ __forceinline__ void str_issue(const StrMaps& M, T* slot, uint32_t bar, int x0, int y0, int k) {
-    mbar_expect_tx(bar, (StrSlot::LOADED - (LAYERED ? 256 + 288 : 0)) * sizeof(T));
+    using StrSlot = typename StrSlotOf<LAYERED>::type;
+    mbar_expect_tx(bar, StrSlot::LOADED * sizeof(T));
     const int z = k - 1;  // k counts the stored planes (global plane - kofs)
     tma_load_3d(smem_addr(slot + StrSlot::U), &M.u, x0 - 4, y0 - 2, z, bar);
     tma_load_3d(smem_addr(slot + StrSlot::V), &M.v, x0 - 4, y0 - 2, z, bar);
@@ -203,6 +220,7 @@ template <class T, bool LAYERED = false>
 __device__ __forceinline__ bool str_interior_tma_body(const StrMaps& M, const Grid& g, const Fields<T>& f,
                                                       const StepConst<T>& c, int kchunk, int bx_, int by_, int bz_,
                                                       T* ring, uint64_t* bars, unsigned& pc, int* status) {
+    using StrSlot = typename StrSlotOf<LAYERED>::type;
     const int tx = threadIdx.x, ty = threadIdx.y;
     const int i0 = g.nabc + 1 + bx_ * 32, j0 = g.nabc + 1 + by_ * 8;
     const int i = i0 + tx, j = j0 + ty;
