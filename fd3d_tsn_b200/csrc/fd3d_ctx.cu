@@ -202,7 +202,7 @@ struct CtxBase {
     int slab_rank = -1, slab_nranks = 0;
     float last_ms = 0.f;
     bool profiling = false;
-    int pml_minb_vel = 1, pml_minb_str = 1;  // register caps of the PML sweeps (CTAs per SM; 1: none, measured fastest)
+    int pml_minb_vel = 1, pml_minb_str = 4;  // register caps of the PML sweeps (CTAs per SM; 1: none), measured fastest
     std::vector<cudaEvent_t> kev;   // 2 per kernel id
     float ktimes[FD3D_NKERNELS] = {0};
     int klaunch[FD3D_NKERNELS] = {0};

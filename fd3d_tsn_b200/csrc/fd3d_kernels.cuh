@@ -525,7 +525,6 @@ __device__ __forceinline__ bool str_pml_tile_c(const Grid& g, const Fields<T>& f
             if (f.lay) { my = xm; md = mz; }
             else { my = f.mu[p + sy]; md = f.mu[p + 1 + sy + sz]; }
             uy = f.u[p + sy]; vx = f.v[p - 1]; vz = f.v[p + sz]; wy = f.w[p + sy];
-            if (j == g.nyt - 1) { xyo = f.xy[p]; yzo = f.yz[p]; }
         }
     }
     if (!pml_tile_wait(bar, parity, status)) return false;
@@ -565,7 +564,12 @@ __device__ __forceinline__ bool str_pml_tile_c(const Grid& g, const Fields<T>& f
             xmu = (xm + md) / (T)2;
             const T h0 = put(AX_YZ0, pml_split<T, MZ>(aux(AX_YZ0), inc(xmu, vz - vp), ozS, false));
             const T h1 = put(AX_YZ1, pml_split<T, MY>(aux(AX_YZ1), inc(xmu, wy - wp), oyS, dy));
-            if (j == g.nyt - 1) { f.xy[p + sy] = xyo; f.yz[p + sy] = yzo; }  // strbnd mirror
+            if (j == g.nyt - 1) {  // strbnd mirror of the values before this update (read here, not
+                xyo = f.xy[p];     // held across the staging wait: four fewer live registers)
+                yzo = f.yz[p];
+                f.xy[p + sy] = xyo;
+                f.yz[p + sy] = yzo;
+            }
             f.xy[p] = e0 + e1;
             f.yz[p] = h0 + h1;
             if (top) { put(AX_YZ0, (T)0); put(AX_YZ1, (T)0); }
