@@ -251,7 +251,7 @@ __global__ void __launch_bounds__(256) k_bint(const ModelDev* __restrict__ model
 }
 
 template <bool STRESS>
-__global__ void __launch_bounds__(PML_TILE, STRESS ? 3 : 4) k_bpml(const ModelDev* __restrict__ models,
+__global__ void __launch_bounds__(PML_TILE, 4) k_bpml(const ModelDev* __restrict__ models,
                                                       const Work* __restrict__ work, int b0,
                                                       const int* __restrict__ limit, const int* run_step,
                                                       int* gstatus) {
